@@ -1,0 +1,200 @@
+/*
+ * shearwave_b200 — C ABI of the B200 (sm_100a) implementation of the
+ * pinton-lab/shearwave hot path: the shear_fdtd time loop, the Helmholtz-Hodge
+ * force projection with its conjugate-gradient Poisson solve, and the strain
+ * post-pass.
+ *
+ * Conventions shared by every entry point
+ * ---------------------------------------
+ *  - Every pointer is a DEVICE pointer unless the comment says "host".  The
+ *    caller owns all memory (the Python layer allocates it through torch);
+ *    the library borrows pointers for the duration of a call and allocates
+ *    nothing itself.
+ *  - `stream` is a cudaStream_t (NULL = legacy default stream).  Work is
+ *    enqueued on it; calls that must read a device-side flag (the CG loop)
+ *    synchronise that stream and return when the work is complete.
+ *  - `dtype` is SW_F32 or SW_F64.
+ *  - Dense arrays are C-ordered (nx, ny, nz[, k]) like the reference's numpy
+ *    arrays.  Padded fields use a z pitch pz = sw_pitch(nz) (a multiple of 8)
+ *    and hold vector components as separate planes of ncell = nx*ny*pz
+ *    elements.  The one-voxel shell of every padded field is zero.
+ *  - Every entry point returns SW_OK (0) or an error code; sw_last_error()
+ *    gives a message for the last failure on the calling thread.
+ *
+ * Reference interfaces (paths within pinton-lab/shearwave):
+ *  src/shearwave/solver.py:27-243     shear_fdtd             -> sw_fdtd_*
+ *  src/shearwave/solver.py:246-566    shear_fdtd_jax extras  -> snaps / traces in sw_fdtd_desc
+ *  src/shearwave/solver.py:644-683    project_vector_field   -> sw_project
+ *  src/shearwave/solver.py:1010-1050  poisson_cg             -> sw_project (CG stage)
+ *  src/shearwave/solver.py:686-729    laplacian/divergence/gradient_center -> sw_laplacian, ...
+ *  src/shearwave/strain.py:16-135     compute_strain_tensor / _invariants -> sw_strain*
+ */
+#ifndef SHEARWAVE_B200_H
+#define SHEARWAVE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SW_ABI_VERSION 1
+
+enum sw_dtype { SW_F32 = 0, SW_F64 = 1 };
+
+enum sw_status {
+  SW_OK = 0,
+  SW_EINVAL = 1,      /* bad argument (null pointer, shape, size) */
+  SW_ECUDA = 2,       /* a CUDA runtime call or launch failed */
+  SW_ENONFINITE = 3,  /* non-finite values detected in the state */
+  SW_ERANGE = 4,      /* size above a compiled-in maximum */
+  SW_EWORKSPACE = 5   /* workspace smaller than the *_workspace_bytes query */
+};
+
+/* Why a CG solve stopped (solver.py:1033-1048 plus the early exit of 672-676). */
+enum sw_cg_reason {
+  SW_CG_RUNNING = 0,
+  SW_CG_CONVERGED = 1,  /* sqrt(r.r / rs0) < tol */
+  SW_CG_BREAKDOWN = 2,  /* p.Ap non-finite or <= 0 (x untouched that iteration) */
+  SW_CG_NONFINITE = 3,  /* r.r non-finite after the update */
+  SW_CG_MAXITERS = 4,   /* max_iters updates done */
+  SW_CG_EARLY_EXIT = 5  /* max|div f| < 1e-12: no solve, f returned masked */
+};
+
+enum sw_precision {
+  SW_PLAIN_F64 = 0, /* FP64 fields, reference arithmetic (the plain drop-in) */
+  SW_MIXED_F32 = 1  /* FP32 fields in increment form, Kahan-compensated u */
+};
+
+/* ---- library --------------------------------------------------------- */
+int sw_abi_version(void);
+const char* sw_last_error(void);
+/* Make `device` current for this thread's subsequent calls. */
+int sw_set_device(int device);
+/* Padded z pitch used for padded fields (nz rounded up to a multiple of 8). */
+int sw_pitch(int nz);
+/* sizeof(sw_fdtd_desc), so a binding can check its mirror of the struct. */
+size_t sw_fdtd_desc_size(void);
+
+/* ---- collocated FD operators on dense arrays (solver.py:686-729) ------- */
+/* laplacian_center: interior 7-point Laplacian, zero shell. */
+int sw_laplacian(int dtype, const void* f, void* out, int nx, int ny, int nz, double dX,
+                 double dY, double dZ, void* stream);
+/* divergence_center: interior 2h central divergence, zero shell. */
+int sw_divergence(int dtype, const void* fx, const void* fy, const void* fz, void* out, int nx,
+                  int ny, int nz, double dX, double dY, double dZ, void* stream);
+/* gradient_center: interior 2h central gradient, zero shell. */
+int sw_gradient(int dtype, const void* phi, void* gx, void* gy, void* gz, int nx, int ny, int nz,
+                double dX, double dY, double dZ, void* stream);
+
+/* ---- Helmholtz-Hodge projection (solver.py:644-683, 1010-1050) --------- */
+typedef struct sw_cg_stats {
+  int32_t iters;   /* completed CG updates */
+  int32_t reason;  /* enum sw_cg_reason */
+  double rel;      /* sqrt(r.r / rs0) at exit (NaN when no update ran) */
+  double max_div;  /* max |div_c f| of the masked input */
+} sw_cg_stats;
+
+/* Bytes of device workspace sw_project needs for an (nx, ny, nz) grid. */
+size_t sw_project_workspace_bytes(int nx, int ny, int nz);
+
+/* Project (fx, fy, fz) onto discretely divergence-free fields in FP64.
+ * Input: dtype `in_dtype`, element (x, y, z) at x*in_sx + y*in_sy + z*in_sz
+ * (elements; dense arrays: ny*nz, nz, 1).  A NULL component is zero.
+ * Output: `out` holds 3 padded FP64 components (pitch sw_pitch(nz)).
+ * The CG runs in FP64 with the reference's stopping rule; the call returns
+ * once the solve has finished (it synchronises `stream`).  `stats` is host. */
+int sw_project(int in_dtype, const void* fx, const void* fy, const void* fz, int64_t in_sx,
+               int64_t in_sy, int64_t in_sz, int nx, int ny, int nz, double dX, double dY,
+               double dZ, double tol, int max_iters, double* out, void* workspace,
+               size_t workspace_bytes, sw_cg_stats* stats, void* stream);
+
+/* dst = src * scale / rho (rho NULL: dst = src * scale) for `ncomp` padded FP64
+ * components into `dst` (dtype out_dtype, element (x,y,z) of component c at
+ * c*dst_cs + x*dst_sx + y*dst_sy + z*dst_sz).  rho is dense or strided like
+ * the input of sw_project (rho_sx, rho_sy, rho_sz). */
+int sw_convert(int ncomp, const double* src, int nx, int ny, int nz, int out_dtype, void* dst,
+               int64_t dst_cs, int64_t dst_sx, int64_t dst_sy, int64_t dst_sz, double scale,
+               int rho_dtype, const void* rho, int64_t rho_sx, int64_t rho_sy, int64_t rho_sz,
+               void* stream);
+
+/* ---- time loop (solver.py:27-243) --------------------------------------- */
+typedef struct sw_fdtd_desc {
+  int32_t precision;       /* enum sw_precision */
+  int32_t nx, ny, nz, pz;  /* pz must equal sw_pitch(nz) */
+  int32_t n_steps;         /* total steps of the solve (term table length) */
+  double dX, dY, dZ, dT, vel_damp;
+  /* SW_PLAIN_F64: state[0..2] are three rotating FP64 buffers of 3 padded
+   *   components (u_prev, u_curr, u_next).
+   * SW_MIXED_F32: state[0], state[1] are two FP32 buffers of 9 padded
+   *   components (u, d = u - u_prev, Kahan compensation c), ping-ponged. */
+  void* state[3];
+  /* Material coefficients, padded, written by sw_fdtd_materials:
+   *   F64: coef_m = mu/rho, coef_e = eta/rho (NULL: no viscosity), inv_rho = 1/rho.
+   *   F32: coef_m = dT^2 mu/rho, coef_e = dT eta/rho (NULL: none), inv_rho unused. */
+  void* coef_m;
+  void* coef_e;
+  void* inv_rho;
+  /* Projected force patterns, n_patterns x 3 padded components:
+   *   F64: f_S;  F32: dT^2 f_S / rho. */
+  const void* patterns;
+  int32_t n_patterns;
+  /* Force terms of step it: j in [term_off[it], term_off[it+1]) adds
+   * term_scale[j] * patterns[term_pat[j]] (term_off has n_steps+1 entries). */
+  const int32_t* term_off;
+  const int32_t* term_pat;
+  const double* term_scale;
+  int32_t kahan;          /* F32: 1 = compensated u update */
+  int32_t snap_stride;    /* > 0: write u after every snap_stride steps */
+  void* snaps;            /* dense (n_steps/snap_stride, nx, ny, nz, 3) of the field dtype */
+  int32_t n_traces;       /* > 0: record u_z at trace cells every step */
+  const int32_t* trace_cells; /* n_traces x (ix, iy, iz) */
+  void* traces;           /* dense (n_traces, n_steps) of the field dtype */
+  int32_t* flags;         /* device int, bit 0 set when a non-finite u appears (may be NULL) */
+  int32_t xchunk;         /* planes per tile along x (0 = automatic) */
+  int32_t steps_per_pass; /* F32: steps fused per HBM pass (0/1 = one) */
+} sw_fdtd_desc;
+
+/* Material coefficients from rho, mu, eta.  Each of rho/mu/eta is a dense
+ * (nx,ny,nz) array of `in_dtype`, or NULL to use the scalar.  eta_mode: 0 no
+ * viscosity, 1 use eta/eta_s. */
+int sw_fdtd_materials(const sw_fdtd_desc* d, int in_dtype, const void* rho, double rho_s,
+                      const void* mu, double mu_s, int eta_mode, const void* eta, double eta_s,
+                      void* stream);
+
+/* Initial state from initial_u / initial_v (dense (nx,ny,nz,3) of the field
+ * dtype, or NULL for zero), solver.py:157-171.  Zeroes all state buffers. */
+int sw_fdtd_init(const sw_fdtd_desc* d, const void* init_u, const void* init_v, void* stream);
+
+/* Advance steps it0 .. it0+nsteps-1 (0-based step indices). */
+int sw_fdtd_steps(const sw_fdtd_desc* d, int32_t it0, int32_t nsteps, void* stream);
+
+/* Write u and v = (u_curr - u_prev)/dT after `steps_done` steps as dense
+ * (nx,ny,nz,3) arrays of the field dtype (either may be NULL). */
+int sw_fdtd_finish(const sw_fdtd_desc* d, int32_t steps_done, void* u_out, void* v_out,
+                   void* stream);
+
+/* Project the state in place after `steps_done` steps (reproject_every,
+ * solver.py:236-239): u_curr and u_prev each go through sw_project. */
+int sw_fdtd_reproject(const sw_fdtd_desc* d, int32_t steps_done, double tol, int max_iters,
+                      double* tmp, void* workspace, size_t workspace_bytes, sw_cg_stats* stats,
+                      void* stream);
+
+/* ---- strain post-pass (strain.py:16-135) -------------------------------- */
+/* From displacement components (element (x,y,z) at x*sx + y*sy + z*sz) write
+ * any of: eps (dense (nx,ny,nz,6) Voigt, engineering shear), volumetric,
+ * deviatoric, max_shear (dense, dtype) and von_mises (dense, always FP64). */
+int sw_strain(int dtype, const void* ux, const void* uy, const void* uz, int64_t sx, int64_t sy,
+              int64_t sz, int nx, int ny, int nz, double dX, double dY, double dZ, void* eps,
+              void* vol, void* dev, void* max_shear, double* von_mises, void* stream);
+
+/* Invariants of n Voigt 6-vectors (dense (n, 6) of dtype). */
+int sw_strain_invariants(int dtype, const void* eps, int64_t n, void* vol, void* dev,
+                         void* max_shear, double* von_mises, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SHEARWAVE_B200_H */

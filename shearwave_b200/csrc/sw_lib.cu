@@ -1,0 +1,37 @@
+// Library-level entry points: version, error reporting, device selection.
+#include <stdarg.h>
+#include <stdio.h>
+
+#include "sw_common.cuh"
+
+namespace sw {
+
+static thread_local char g_err[512] = "";
+
+void set_error(const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof g_err, fmt, ap);
+  va_end(ap);
+}
+
+int cuda_status(cudaError_t e, const char* what) {
+  set_error("%s: %s (%s)", what, cudaGetErrorString(e), cudaGetErrorName(e));
+  return SW_ECUDA;
+}
+
+}  // namespace sw
+
+extern "C" int sw_abi_version(void) { return SW_ABI_VERSION; }
+
+extern "C" const char* sw_last_error(void) { return sw::g_err; }
+
+extern "C" int sw_set_device(int device) {
+  cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess) return sw::cuda_status(e, "cudaSetDevice");
+  return SW_OK;
+}
+
+extern "C" int sw_pitch(int nz) { return nz > 0 ? sw::pad_pitch(nz) : 0; }
+
+extern "C" size_t sw_fdtd_desc_size(void) { return sizeof(sw_fdtd_desc); }

@@ -1,0 +1,486 @@
+// Helmholtz-Hodge projection and its FP64 conjugate-gradient Poisson solve.
+//
+// Reference: project_vector_field (src/shearwave/solver.py:644-683) and
+// poisson_cg (src/shearwave/solver.py:1010-1050).
+//
+// The operator is A x = -div_c(grad_c x) with both 2h central differences
+// zero on the shell, so per axis an interior row reads x at i-2, i, i+2 and
+// drops the gradient term whose centre i+-1 lies on the shell.  One CG
+// iteration is two launches:
+//   cg_apply  : p_k = r + beta p_{k-1} (fused, written to the other p buffer),
+//               Ap = A p_k, partial p_k.Ap
+//   cg_update : x += alpha p_k, r -= alpha Ap, partial r.r
+// Each launch ends with a "last block" step: the block that takes the final
+// ticket of an instance sums that instance's per-tile partials in a fixed
+// order (deterministic) and advances the instance's scalar CG state, with the
+// reference's stopping rule.  No block ever waits for another one.
+// Every kernel works on a table of instances so that one launch can advance
+// many independent solves (the batched path) as well as a single one.
+#include <math.h>
+#include <stdio.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "sw_common.cuh"
+#include "sw_project.cuh"
+
+namespace sw {
+
+// ---------------------------------------------------------------------------
+// helpers
+// ---------------------------------------------------------------------------
+__device__ inline int find_inst(const CgInst* __restrict__ tab, int ninst, int t) {
+  int lo = 0, hi = ninst - 1;
+  while (lo < hi) {  // last instance with tile_base <= t
+    int mid = (lo + hi + 1) >> 1;
+    if (tab[mid].tile_base <= t) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Take a ticket for instance `in`; returns true in every thread of the block
+// that took the last ticket.  The caller has written its partial already.
+__device__ inline bool last_block(const CgInst& in, unsigned int* flag_smem) {
+  __syncthreads();
+  if (flat_tid() == 0) {
+    __threadfence();
+    unsigned int t = atomicAdd(&in.st->ticket, 1u);
+    *flag_smem = (t == (unsigned int)(in.ts.count - 1)) ? 1u : 0u;
+  }
+  __syncthreads();
+  bool last = *flag_smem != 0u;
+  if (last) __threadfence();
+  return last;
+}
+
+// Sum (and max) of this instance's per-tile partials, fixed order.
+__device__ inline double2 reduce_partials(const CgInst& in, double* red) {
+  double s = 0.0, m = 0.0;
+  const int tid = flat_tid(), nthr = blockDim.x * blockDim.y;
+  for (int i = tid; i < in.ts.count; i += nthr) {
+    double2 v = __ldcg(&in.partials[i]);
+    s += v.x;
+    m = fmax(m, v.y);
+  }
+  double2 out;
+  out.x = block_sum(s, red);
+  __syncthreads();
+  out.y = block_max(m, red);
+  return out;
+}
+
+template <typename T>
+__device__ inline double ld_masked(const T* __restrict__ f, const CgInst& in, const InStride& s,
+                                   int x, int y, int z) {
+  if (f == nullptr || !interior(in.g, x, y, z)) return 0.0;
+  return (double)f[(long long)x * s.sx + (long long)y * s.sy + (long long)z * s.sz];
+}
+
+// ---------------------------------------------------------------------------
+// prep: rhs = -div_c(mask f), r = p0 = rhs, rs0, max|div|
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(TILE_THREADS) cg_prep(const CgInst* __restrict__ tab, int ninst,
+                                                        int ntiles, const T* const* __restrict__ fin,
+                                                        const InStride* __restrict__ fstride) {
+  __shared__ double red[32];
+  __shared__ unsigned int lastflag;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const int ii = find_inst(tab, ninst, t);
+    const CgInst& in = tab[ii];
+    const Geom& g = in.g;
+    const T* fx = fin[3 * ii + 0];
+    const T* fy = fin[3 * ii + 1];
+    const T* fz = fin[3 * ii + 2];
+    const InStride s = fstride[ii];
+    const int local = t - in.tile_base;
+    const TileCoord tc = tile_coord(g, in.ts, local);
+    const int z = tc.z0 + threadIdx.x, y = tc.y0 + threadIdx.y;
+    double acc = 0.0, mx = 0.0;
+    for (int x = tc.x0; x < tc.x1; ++x) {
+      if (!interior(g, x, y, z)) continue;
+      double tx = (ld_masked(fx, in, s, x + 1, y, z) - ld_masked(fx, in, s, x - 1, y, z)) * in.c2x;
+      double ty = (ld_masked(fy, in, s, x, y + 1, z) - ld_masked(fy, in, s, x, y - 1, z)) * in.c2y;
+      double tz = (ld_masked(fz, in, s, x, y, z + 1) - ld_masked(fz, in, s, x, y, z - 1)) * in.c2z;
+      double div = (tx + ty) + tz;
+      double rhs = -div;
+      long long i = (long long)x * g.sxy + (long long)y * g.pz + z;
+      in.r[i] = rhs;
+      in.p0[i] = rhs;
+      acc += rhs * rhs;
+      mx = fmax(mx, fabs(div));
+    }
+    double bs = block_sum(acc, red);
+    __syncthreads();
+    double bm = block_max(mx, red);
+    if (flat_tid() == 0) in.partials[local] = make_double2(bs, bm);
+    if (last_block(in, &lastflag)) {
+      double2 tot = reduce_partials(in, red);
+      if (flat_tid() == 0) {
+        CgState* st = in.st;
+        st->ticket = 0u;
+        st->rs = tot.x;
+        st->rs0 = fmax(tot.x, 2.220446049250313e-16);
+        st->maxdiv = tot.y;
+        st->iters = 0;
+        st->k = 0;
+        st->rel = nan("");
+        if (tot.y < 1e-12) st->reason = SW_CG_EARLY_EXIT;
+        else if (st->max_iters <= 0) st->reason = SW_CG_MAXITERS;
+        else st->reason = SW_CG_RUNNING;
+        __threadfence();
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// apply: p_k (fused update), Ap = A p_k, partial p_k.Ap
+// ---------------------------------------------------------------------------
+struct PView {
+  const double* r;
+  const double* pold;
+  double beta;
+  bool first;
+  __device__ inline double operator()(long long i) const {
+    return first ? pold[i] : fma(beta, pold[i], r[i]);
+  }
+};
+
+__global__ void __launch_bounds__(TILE_THREADS) cg_apply(const CgInst* __restrict__ tab, int ninst,
+                                                         int ntiles) {
+  __shared__ double red[32];
+  __shared__ unsigned int lastflag;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const int ii = find_inst(tab, ninst, t);
+    const CgInst& in = tab[ii];
+    const CgState* st = in.st;
+    if (st->reason != SW_CG_RUNNING) continue;  // uniform across the block
+    const Geom& g = in.g;
+    const int k = st->k;
+    PView pv;
+    pv.first = (k == 0);
+    pv.r = in.r;
+    pv.beta = st->beta;
+    pv.pold = pv.first ? in.p0 : ((k - 1) & 1 ? in.p1 : in.p0);
+    double* pnew = (k & 1) ? in.p1 : in.p0;
+    const int local = t - in.tile_base;
+    const TileCoord tc = tile_coord(g, in.ts, local);
+    const int z = tc.z0 + threadIdx.x, y = tc.y0 + threadIdx.y;
+    double acc = 0.0;
+    for (int x = tc.x0; x < tc.x1; ++x) {
+      if (!interior(g, x, y, z)) continue;
+      const long long i = (long long)x * g.sxy + (long long)y * g.pz + z;
+      const double pc = pv(i);
+      double gp, gm, tx, ty, tz;
+      gp = (x + 1 <= g.nx - 2) ? (pv(i + 2 * g.sxy) - pc) * in.c2x : 0.0;
+      gm = (x - 1 >= 1) ? (pc - pv(i - 2 * g.sxy)) * in.c2x : 0.0;
+      tx = (gp - gm) * in.c2x;
+      gp = (y + 1 <= g.ny - 2) ? (pv(i + 2 * g.pz) - pc) * in.c2y : 0.0;
+      gm = (y - 1 >= 1) ? (pc - pv(i - 2 * g.pz)) * in.c2y : 0.0;
+      ty = (gp - gm) * in.c2y;
+      gp = (z + 1 <= g.nz - 2) ? (pv(i + 2) - pc) * in.c2z : 0.0;
+      gm = (z - 1 >= 1) ? (pc - pv(i - 2)) * in.c2z : 0.0;
+      tz = (gp - gm) * in.c2z;
+      const double ap = -((tx + ty) + tz);
+      in.ap[i] = ap;
+      if (!pv.first) pnew[i] = pc;
+      acc += pc * ap;
+    }
+    double bs = block_sum(acc, red);
+    if (flat_tid() == 0) in.partials[local] = make_double2(bs, 0.0);
+    if (last_block(in, &lastflag)) {
+      double2 tot = reduce_partials(in, red);
+      if (flat_tid() == 0) {
+        CgState* w = in.st;
+        w->ticket = 0u;
+        const double denom = tot.x;
+        if (!isfinite(denom) || denom <= 0.0) w->reason = SW_CG_BREAKDOWN;
+        else w->alpha = w->rs / denom;
+        __threadfence();
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// update: x += alpha p_k, r -= alpha Ap, partial r.r, stopping rule
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(TILE_THREADS) cg_update(const CgInst* __restrict__ tab, int ninst,
+                                                          int ntiles) {
+  __shared__ double red[32];
+  __shared__ unsigned int lastflag;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const int ii = find_inst(tab, ninst, t);
+    const CgInst& in = tab[ii];
+    const CgState* st = in.st;
+    if (st->reason != SW_CG_RUNNING) continue;
+    const Geom& g = in.g;
+    const int k = st->k;
+    const double alpha = st->alpha;
+    const double* pk = (k & 1) ? in.p1 : in.p0;
+    const int local = t - in.tile_base;
+    const TileCoord tc = tile_coord(g, in.ts, local);
+    const int z = tc.z0 + threadIdx.x, y = tc.y0 + threadIdx.y;
+    double acc = 0.0;
+    for (int x = tc.x0; x < tc.x1; ++x) {
+      if (!interior(g, x, y, z)) continue;
+      const long long i = (long long)x * g.sxy + (long long)y * g.pz + z;
+      in.x[i] = fma(alpha, pk[i], in.x[i]);
+      const double rn = fma(-alpha, in.ap[i], in.r[i]);
+      in.r[i] = rn;
+      acc += rn * rn;
+    }
+    double bs = block_sum(acc, red);
+    if (flat_tid() == 0) in.partials[local] = make_double2(bs, 0.0);
+    if (last_block(in, &lastflag)) {
+      double2 tot = reduce_partials(in, red);
+      if (flat_tid() == 0) {
+        CgState* w = in.st;
+        w->ticket = 0u;
+        const double rs_new = tot.x;
+        w->iters += 1;
+        if (!isfinite(rs_new)) {
+          w->reason = SW_CG_NONFINITE;
+        } else {
+          const double rel = sqrt(rs_new / w->rs0);
+          w->rel = rel;
+          if (rel < w->tol) {
+            w->reason = SW_CG_CONVERGED;
+          } else {
+            w->beta = rs_new / fmax(w->rs, 2.220446049250313e-16);
+            w->rs = rs_new;
+            w->k += 1;
+            if (w->iters >= w->max_iters) w->reason = SW_CG_MAXITERS;
+          }
+        }
+        __threadfence();
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// finish: out = (mask f - grad_c x), zero shell
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(TILE_THREADS) cg_finish(const CgInst* __restrict__ tab, int ninst,
+                                                          int ntiles, const T* const* __restrict__ fin,
+                                                          const InStride* __restrict__ fstride,
+                                                          double* const* __restrict__ outs) {
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const int ii = find_inst(tab, ninst, t);
+    const CgInst& in = tab[ii];
+    const Geom& g = in.g;
+    const InStride s = fstride[ii];
+    double* out = outs[ii];
+    const int local = t - in.tile_base;
+    const TileCoord tc = tile_coord(g, in.ts, local);
+    const int z = tc.z0 + threadIdx.x, y = tc.y0 + threadIdx.y;
+    for (int x = tc.x0; x < tc.x1; ++x) {
+      if (!interior(g, x, y, z)) continue;
+      const long long i = (long long)x * g.sxy + (long long)y * g.pz + z;
+      const double gx = (in.x[i + g.sxy] - in.x[i - g.sxy]) * in.c2x;
+      const double gy = (in.x[i + g.pz] - in.x[i - g.pz]) * in.c2y;
+      const double gz = (in.x[i + 1] - in.x[i - 1]) * in.c2z;
+      out[i] = ld_masked(fin[3 * ii + 0], in, s, x, y, z) - gx;
+      out[i + g.ncell] = ld_masked(fin[3 * ii + 1], in, s, x, y, z) - gy;
+      out[i + 2 * g.ncell] = ld_masked(fin[3 * ii + 2], in, s, x, y, z) - gz;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+size_t cg_workspace_bytes(const Geom& g, const TileSpace& ts) {
+  size_t vec = align_up((size_t)g.ncell * sizeof(double), 256);
+  size_t b = 5 * vec;                                            // x r p0 p1 ap
+  b += align_up((size_t)ts.count * sizeof(double2), 256);        // partials
+  b += align_up(sizeof(CgState), 256);                           // state
+  b += align_up(sizeof(CgInst), 256);                            // instance table
+  b += align_up(3 * sizeof(void*) + sizeof(InStride) + sizeof(double*), 256);
+  return b;
+}
+
+TileSpace cg_tiles(const Geom& g) { return make_tiles(g, choose_xchunk(g, 4 * 148)); }
+
+int cg_layout(const Geom& g, char* ws, size_t ws_bytes, CgInst* in, CgState** st,
+              char** tail) {
+  in->g = g;
+  in->ts = cg_tiles(g);
+  size_t need = cg_workspace_bytes(g, in->ts);
+  if (ws == nullptr || ws_bytes < need) {
+    set_error("workspace of %zu bytes is smaller than the %zu bytes required", ws_bytes, need);
+    return SW_EWORKSPACE;
+  }
+  size_t vec = align_up((size_t)g.ncell * sizeof(double), 256);
+  char* p = ws;
+  in->x = (double*)p;
+  p += vec;
+  in->r = (double*)p;
+  p += vec;
+  in->p0 = (double*)p;
+  p += vec;
+  in->p1 = (double*)p;
+  p += vec;
+  in->ap = (double*)p;
+  p += vec;
+  in->partials = (double2*)p;
+  p += align_up((size_t)in->ts.count * sizeof(double2), 256);
+  *st = (CgState*)p;
+  in->st = *st;
+  p += align_up(sizeof(CgState), 256);
+  *tail = p;
+  in->tile_base = 0;
+  return SW_OK;
+}
+
+int cg_run(const CgInst* d_tab, int ninst, int ntiles, CgState* const* states, int nst,
+           cudaStream_t s) {
+  // Launch CG iterations in growing batches; after each batch read the
+  // instances' exit reasons (one small D2H copy) and stop when all are done.
+  const int grid = std::max(1, std::min(ntiles, 148 * 8));
+  std::vector<int> reasons(nst, SW_CG_RUNNING);
+  int batch = 4;
+  for (;;) {
+    bool running = false;
+    for (int i = 0; i < nst; ++i) {
+      cudaError_t e = cudaMemcpyAsync(&reasons[i], &states[i]->reason, sizeof(int),
+                                      cudaMemcpyDeviceToHost, s);
+      if (e != cudaSuccess) return cuda_status(e, "cg reason readback");
+    }
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_status(e, "cg synchronize");
+    for (int i = 0; i < nst; ++i) running |= (reasons[i] == SW_CG_RUNNING);
+    if (!running) return SW_OK;
+    for (int b = 0; b < batch; ++b) {
+      cg_apply<<<grid, dim3(TILE_Z, TILE_Y), 0, s>>>(d_tab, ninst, ntiles);
+      cg_update<<<grid, dim3(TILE_Z, TILE_Y), 0, s>>>(d_tab, ninst, ntiles);
+    }
+    SW_CHECK_LAUNCH("cg iteration");
+    batch = std::min(batch * 2, 64);
+  }
+}
+
+template <typename T>
+int project_one(const void* fx, const void* fy, const void* fz, InStride fs, const Geom& g,
+                double dX, double dY, double dZ, double tol, int max_iters, double* out, void* ws,
+                size_t ws_bytes, sw_cg_stats* stats, cudaStream_t s) {
+  CgInst in{};
+  CgState* st = nullptr;
+  char* tail = nullptr;
+  int rc = cg_layout(g, (char*)ws, ws_bytes, &in, &st, &tail);
+  if (rc != SW_OK) return rc;
+  in.c2x = 1.0 / (2.0 * dX);
+  in.c2y = 1.0 / (2.0 * dY);
+  in.c2z = 1.0 / (2.0 * dZ);
+  CgInst* d_tab = (CgInst*)tail;
+  tail += align_up(sizeof(CgInst), 256);
+  const T** d_fin = (const T**)tail;
+  InStride* d_fs = (InStride*)(tail + 3 * sizeof(void*));
+  double** d_out = (double**)(tail + 3 * sizeof(void*) + sizeof(InStride));
+
+  struct {
+    const T* f[3];
+    InStride st;
+    double* out;
+  } hostargs;
+  hostargs.f[0] = (const T*)fx;
+  hostargs.f[1] = (const T*)fy;
+  hostargs.f[2] = (const T*)fz;
+  hostargs.st = fs;
+  hostargs.out = out;
+
+  CgState hst{};
+  hst.tol = tol;
+  hst.max_iters = max_iters;
+  hst.reason = SW_CG_RUNNING;
+  cudaError_t e;
+  // x r p0 p1 ap are consecutive 256-byte aligned vectors: zero all of them
+  const size_t vec = align_up((size_t)g.ncell * sizeof(double), 256);
+  e = cudaMemsetAsync(in.x, 0, 5 * vec, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(st, &hst, sizeof(hst), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d_tab, &in, sizeof(in), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(d_fin, hostargs.f, 3 * sizeof(void*), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d_fs, &fs, sizeof(fs), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d_out, &out, sizeof(out), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(out, 0, (size_t)g.ncell * 3 * sizeof(double), s);
+  if (e != cudaSuccess) return cuda_status(e, "projection setup");
+  const int ntiles = in.ts.count;
+  if (ntiles > 0) {
+    const int grid = std::max(1, std::min(ntiles, 148 * 8));
+    cg_prep<T><<<grid, dim3(TILE_Z, TILE_Y), 0, s>>>(d_tab, 1, ntiles, d_fin, d_fs);
+    SW_CHECK_LAUNCH("cg_prep");
+    rc = cg_run(d_tab, 1, ntiles, &st, 1, s);
+    if (rc != SW_OK) return rc;
+    cg_finish<T><<<grid, dim3(TILE_Z, TILE_Y), 0, s>>>(d_tab, 1, ntiles, d_fin, d_fs, d_out);
+    SW_CHECK_LAUNCH("cg_finish");
+  }
+  e = cudaMemcpyAsync(&hst, st, sizeof(hst), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return cuda_status(e, "projection readback");
+  if (stats) {
+    if (ntiles == 0) {
+      hst.iters = 0;
+      hst.reason = SW_CG_EARLY_EXIT;
+      hst.rel = nan("");
+      hst.maxdiv = 0.0;
+    }
+    stats->iters = hst.iters;
+    stats->reason = hst.reason;
+    stats->rel = hst.rel;
+    stats->max_div = hst.maxdiv;
+  }
+  return SW_OK;
+}
+
+int project_field(int dtype, const void* fx, const void* fy, const void* fz, InStride fs,
+                  const Geom& g, double dX, double dY, double dZ, double tol, int max_iters,
+                  double* out, void* ws, size_t ws_bytes, sw_cg_stats* stats, cudaStream_t s) {
+  if (dtype == SW_F32)
+    return project_one<float>(fx, fy, fz, fs, g, dX, dY, dZ, tol, max_iters, out, ws, ws_bytes,
+                              stats, s);
+  if (dtype == SW_F64)
+    return project_one<double>(fx, fy, fz, fs, g, dX, dY, dZ, tol, max_iters, out, ws, ws_bytes,
+                               stats, s);
+  set_error("projection: unknown dtype %d", dtype);
+  return SW_EINVAL;
+}
+
+}  // namespace sw
+
+using namespace sw;
+
+extern "C" size_t sw_project_workspace_bytes(int nx, int ny, int nz) {
+  if (nx <= 0 || ny <= 0 || nz <= 0) return 0;
+  Geom g = make_geom(nx, ny, nz, pad_pitch(nz));
+  return cg_workspace_bytes(g, cg_tiles(g));
+}
+
+extern "C" int sw_project(int in_dtype, const void* fx, const void* fy, const void* fz,
+                          int64_t in_sx, int64_t in_sy, int64_t in_sz, int nx, int ny, int nz,
+                          double dX, double dY, double dZ, double tol, int max_iters, double* out,
+                          void* workspace, size_t workspace_bytes, sw_cg_stats* stats,
+                          void* stream) {
+  if (nx <= 0 || ny <= 0 || nz <= 0 || out == nullptr) {
+    set_error("sw_project: bad grid or null output");
+    return SW_EINVAL;
+  }
+  if (!(dX > 0 && dY > 0 && dZ > 0)) {
+    set_error("sw_project: grid spacing must be positive");
+    return SW_EINVAL;
+  }
+  Geom g = make_geom(nx, ny, nz, pad_pitch(nz));
+  InStride fs{in_sx, in_sy, in_sz};
+  return project_field(in_dtype, fx, fy, fz, fs, g, dX, dY, dZ, tol, max_iters, out, workspace,
+                       workspace_bytes, stats, (cudaStream_t)stream);
+}

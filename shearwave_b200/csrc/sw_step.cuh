@@ -1,0 +1,35 @@
+// Internal interface of the time-loop stage (see sw_step.cu).
+#pragma once
+
+#include "sw_common.cuh"
+
+namespace sw {
+
+// Kernel-side view of an sw_fdtd_desc (passed by value as a grid constant).
+struct StepArgs {
+  Geom g;
+  TileSpace ts;
+  int precision;
+  void* state[3];
+  const void* coef_m;
+  const void* coef_e;
+  const void* inv_rho;
+  const void* patterns;
+  const int* term_off;
+  const int* term_pat;
+  const double* term_scale;
+  double ihx2, ihy2, ihz2;  // 1 / h^2
+  double dT, inv_dt, dt2, damp;
+  int use_damp, kahan, n_steps;
+  int snap_stride;
+  void* snaps;
+  int n_traces;
+  const int* trace_cells;
+  void* traces;
+  int* flags;
+};
+
+int make_step_args(const sw_fdtd_desc* d, StepArgs* a);
+int launch_steps(const StepArgs& a, int it0, int nsteps, cudaStream_t s);
+
+}  // namespace sw

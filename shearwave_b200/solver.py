@@ -1,0 +1,647 @@
+"""Drop-in ``shear_fdtd`` and projection / operator API on the B200 CUDA library.
+
+Mirrors the public solver functions of pinton-lab/shearwave
+(src/shearwave/solver.py): same argument order, array layout, opts keys,
+error messages and returned ``(u, v)``.  All arithmetic runs in the sm_100a
+kernels of ``libshearwave_b200.so``; this module validates arguments, moves
+arrays to the device (torch owns the memory) and sequences the C-ABI calls.
+
+Precision (``opts["precision"]``):
+
+* ``"mixed"`` (default): FP32 fields in increment form with a Kahan-
+  compensated displacement, FP64 CG projection; returns float32 like the
+  reference.
+* ``"fp64"``: the plain FP64 form, the reference's arithmetic in float64
+  (matches an FP64 run of the reference to relative L2 <= 1e-10); returns
+  float64.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import warnings
+
+import numpy as np
+import torch
+
+from . import _native
+from ._device import (
+    dtype_code,
+    is_tensor,
+    np_dtype,
+    ptr,
+    require_cuda,
+    stream_handle,
+    to_device,
+    to_host,
+)
+
+__all__ = [
+    "divergence_center",
+    "gradient_center",
+    "laplacian_center",
+    "project_body_force_to_shear",
+    "project_vector_field",
+    "shear_fdtd",
+    "shear_fdtd_jax",
+]
+
+_PRECISION = {
+    "mixed": _native.SW_MIXED_F32,
+    "fp32": _native.SW_MIXED_F32,
+    "float32": _native.SW_MIXED_F32,
+    "fp64": _native.SW_PLAIN_F64,
+    "plain": _native.SW_PLAIN_F64,
+    "float64": _native.SW_PLAIN_F64,
+}
+
+
+def _precision(opts: dict) -> int:
+    p = opts.get("precision", "mixed")
+    try:
+        return _PRECISION[str(p).lower()]
+    except KeyError:
+        raise ValueError(f"precision must be one of {sorted(_PRECISION)}, got {p!r}") from None
+
+
+def _field_dtype(prec: int) -> torch.dtype:
+    return torch.float64 if prec == _native.SW_PLAIN_F64 else torch.float32
+
+
+def _shape(a) -> tuple:
+    return tuple(a.shape)
+
+
+# ---------------------------------------------------------------------------
+# FD operators (solver.py:686-729)
+# ---------------------------------------------------------------------------
+def _op_dtype(a) -> torch.dtype:
+    dt = a.dtype if is_tensor(a) else np.asarray(a).dtype
+    if dt in (torch.float32, np.float32):
+        return torch.float32
+    return torch.float64
+
+
+def laplacian_center(field, dX, dY, dZ):
+    """Compact 7-point Laplacian at cell centres, zero on the shell (solver.py:686-695)."""
+    dev = require_cuda()
+    dt = _op_dtype(field)
+    f = to_device(field, dt, dev)
+    nx, ny, nz = _shape(f)
+    out = torch.empty_like(f)
+    _native.call("sw_laplacian", dtype_code(dt), ptr(f), ptr(out), nx, ny, nz, dX, dY, dZ,
+                 stream_handle())
+    return out if is_tensor(field) else out.cpu().numpy()
+
+
+def divergence_center(fx, fy, fz, dX, dY, dZ):
+    """2h central divergence at cell centres, zero on the shell (solver.py:708-717)."""
+    dev = require_cuda()
+    dt = torch.promote_types(torch.promote_types(_op_dtype(fx), _op_dtype(fy)), _op_dtype(fz))
+    a, b, c = (to_device(v, dt, dev) for v in (fx, fy, fz))
+    nx, ny, nz = _shape(a)
+    out = torch.empty_like(a)
+    _native.call("sw_divergence", dtype_code(dt), ptr(a), ptr(b), ptr(c), ptr(out), nx, ny, nz,
+                 dX, dY, dZ, stream_handle())
+    return out if is_tensor(fx) else out.cpu().numpy()
+
+
+def gradient_center(phi, dX, dY, dZ):
+    """2h central gradient at cell centres, zero on the shell (solver.py:720-729)."""
+    dev = require_cuda()
+    dt = _op_dtype(phi)
+    p = to_device(phi, dt, dev)
+    nx, ny, nz = _shape(p)
+    g = [torch.empty_like(p) for _ in range(3)]
+    _native.call("sw_gradient", dtype_code(dt), ptr(p), ptr(g[0]), ptr(g[1]), ptr(g[2]), nx, ny,
+                 nz, dX, dY, dZ, stream_handle())
+    return tuple(g) if is_tensor(phi) else tuple(t.cpu().numpy() for t in g)
+
+
+# ---------------------------------------------------------------------------
+# Projection (solver.py:644-683, 1010-1050)
+# ---------------------------------------------------------------------------
+class _Workspace:
+    """Device scratch of one grid for the projection (owned by torch)."""
+
+    def __init__(self, nx, ny, nz, dev):
+        lib = _native.load()
+        self.bytes = int(lib.sw_project_workspace_bytes(nx, ny, nz))
+        self.pz = int(lib.sw_pitch(nz))
+        self.ncell = nx * ny * self.pz
+        self.ws = torch.empty(self.bytes, dtype=torch.uint8, device=dev)
+        self.out = torch.empty((3, self.ncell), dtype=torch.float64, device=dev)
+
+
+def _project_raw(ws: _Workspace, dtype_c: int, comps, strides, shape, dX, dY, dZ, tol,
+                 max_iters) -> dict:
+    """Run sw_project on device components; the result is left in ws.out."""
+    nx, ny, nz = shape
+    st = _native.CGStats()
+    _native.call("sw_project", dtype_c, *[ptr(c) if c is not None else None for c in comps],
+                 *strides, nx, ny, nz, dX, dY, dZ, float(tol), int(max_iters), ptr(ws.out),
+                 ptr(ws.ws), ws.bytes, C.byref(st), stream_handle())
+    return st.as_dict()
+
+
+def _unpad(ws: _Workspace, shape, dt: torch.dtype, dev) -> list[torch.Tensor]:
+    nx, ny, nz = shape
+    outs = []
+    for c in range(3):
+        o = torch.empty((nx, ny, nz), dtype=dt, device=dev)
+        _native.call("sw_convert", 1, ws.out[c].data_ptr(), nx, ny, nz, dtype_code(dt), ptr(o), 0,
+                     ny * nz, nz, 1, 1.0, _native.SW_F32, None, 0, 0, 0, stream_handle())
+        outs.append(o)
+    return outs
+
+
+def project_vector_field(fx, fy, fz, dX, dY, dZ, tol, max_iters, *, info=None):
+    """Helmholtz-Hodge projection onto discretely divergence-free fields.
+
+    solver.py:644-683.  The CG (solver.py:1010-1050) runs in FP64 on the GPU
+    with the reference's stopping rule.  Returns three arrays in the input
+    dtype (float32 unless the inputs are float64).  ``info`` (dict) receives
+    the CG iteration count and exit reason.
+    """
+    dev = require_cuda()
+    dt = torch.promote_types(torch.promote_types(_op_dtype(fx), _op_dtype(fy)), _op_dtype(fz))
+    comps = [to_device(v, dt, dev) for v in (fx, fy, fz)]
+    shape = _shape(comps[0])
+    if any(_shape(c) != shape for c in comps) or len(shape) != 3:
+        raise ValueError("fx, fy, fz must be 3-D arrays of the same shape")
+    nx, ny, nz = shape
+    ws = _Workspace(nx, ny, nz, dev)
+    st = _project_raw(ws, dtype_code(dt), comps, (ny * nz, nz, 1), shape, dX, dY, dZ, tol,
+                      max_iters)
+    if info is not None:
+        info.update(st)
+    outs = _unpad(ws, shape, dt, dev)
+    if is_tensor(fx):
+        return tuple(outs)
+    return tuple(o.cpu().numpy() for o in outs)
+
+
+def project_body_force_to_shear(bz, dX, dY, dZ, tol=5e-5, max_iters=400):
+    """Project a z-only body force (solver.py:628-641)."""
+    z = np.zeros(_shape(bz), dtype=np.float32)
+    b = bz if is_tensor(bz) else np.asarray(bz, dtype=np.float32)
+    return project_vector_field(z, z, b, dX, dY, dZ, tol, max_iters)
+
+
+# ---------------------------------------------------------------------------
+# shear_fdtd (solver.py:27-243) and the shear_fdtd_jax extras (246-566)
+# ---------------------------------------------------------------------------
+def _check_jax_kwargs(n_steps, trace_indices, return_traces, snapshot_stride):
+    """Validation of solver.py:290-303 and 396-408."""
+    if return_traces and trace_indices is None:
+        raise ValueError("trace_indices must be provided when return_traces=True.")
+    if snapshot_stride is not None:
+        if not isinstance(snapshot_stride, (int, np.integer)) or int(snapshot_stride) <= 0:
+            raise ValueError("snapshot_stride must be a positive integer.")
+        snapshot_stride = int(snapshot_stride)
+        if n_steps % snapshot_stride != 0:
+            raise ValueError(
+                f"n_steps ({n_steps}) must be a multiple of snapshot_stride ({snapshot_stride})."
+            )
+        if return_traces:
+            raise ValueError("return_traces and snapshot_stride are not both supported in v1.")
+    cells = None
+    if trace_indices is not None:
+        if not isinstance(trace_indices, (tuple, list)) or len(trace_indices) != 3:
+            raise ValueError("trace_indices must be a 3-tuple: (ix, iy, iz).")
+        ix, iy, iz = (np.asarray(t, dtype=np.int32) for t in trace_indices)
+        if not (ix.shape == iy.shape == iz.shape):
+            raise ValueError("trace index arrays must share the same shape.")
+        if ix.ndim != 1:
+            raise ValueError("trace index arrays must be 1D.")
+        cells = np.stack([ix, iy, iz], axis=1)
+    return snapshot_stride, cells
+
+
+def _material(v, shape, dt, dev):
+    """(device array or None, scalar) for a material input (solver.py:1072-1079)."""
+    if np.isscalar(v):
+        return None, float(v)
+    if _shape(v) != shape:
+        raise ValueError("Material field has incompatible shape.")
+    return to_device(v, dt, dev), 0.0
+
+
+class _Forces:
+    """Force terms of one solve: projected patterns plus the per-step table."""
+
+    def __init__(self):
+        self.separable = []      # list of ((bx, by, bz) device 3-D or None, env np array)
+        self.stream4d = None     # (bx, by, bz) device 4-D or 3-D or None, for per-step projection
+        self.zero_steps = None   # bool per step (4-D mode): the force slice is identically zero
+
+
+def _gather_forces(bx, by, bz, opts, shape, n_steps, dt, dev, np_dt) -> _Forces:
+    fr = _Forces()
+    env_t = opts.get("env_t")
+
+    def dev3(b):
+        if b is None:
+            return None
+        if len(_shape(b)) != 3 or _shape(b) != shape:
+            raise ValueError("Body-force component has incompatible shape.")
+        return to_device(b, dt, dev)
+
+    if env_t is not None:
+        env = np.asarray(env_t.cpu() if is_tensor(env_t) else env_t, dtype=np_dt).ravel()
+        if env.shape[0] != n_steps:
+            raise ValueError(f"env_t length ({env.shape[0]}) must equal n_steps ({n_steps}).")
+        fr.separable.append(((dev3(bx), dev3(by), dev3(bz)), env))
+    else:
+        comps = []
+        any4 = False
+        for b in (bx, by, bz):
+            if b is None:
+                comps.append(None)
+                continue
+            s = _shape(b)
+            if len(s) == 3 and s == shape:
+                comps.append(b)
+            elif len(s) == 4 and s == (*shape, n_steps):
+                comps.append(b)
+                any4 = True
+            else:
+                raise ValueError("Body-force component has incompatible shape.")
+        if not any4:
+            # 3-D forces without env_t: the reference repeats them over every step
+            # and projects each identical slice; one projection with scale 1 is
+            # the same result.
+            fr.separable.append((tuple(dev3(b) for b in comps), np.ones(n_steps, dtype=np_dt)))
+        else:
+            zero = np.ones(n_steps, dtype=bool)
+            dcomps = []
+            for b in comps:
+                if b is None:
+                    dcomps.append(None)
+                    continue
+                if len(_shape(b)) == 4:
+                    if is_tensor(b):
+                        nz_t = (b.reshape(-1, n_steps) != 0).any(0).cpu().numpy()
+                    else:
+                        nz_t = np.any(np.asarray(b).reshape(-1, n_steps) != 0, axis=0)
+                    zero &= ~nz_t
+                else:
+                    zero &= not bool(np.any(np.asarray(b.cpu() if is_tensor(b) else b) != 0))
+                dcomps.append(to_device(b, dt, dev))
+            fr.stream4d = dcomps
+            fr.zero_steps = zero
+    for term in opts.get("force_terms") or ():
+        if isinstance(term, dict):
+            tb = (term.get("bx"), term.get("by"), term.get("bz"))
+            tenv = term["env"]
+        else:
+            (tb, tenv) = term
+        env = np.asarray(tenv.cpu() if is_tensor(tenv) else tenv, dtype=np_dt).ravel()
+        if env.shape[0] != n_steps:
+            raise ValueError(f"env_t length ({env.shape[0]}) must equal n_steps ({n_steps}).")
+        fr.separable.append((tuple(dev3(b) for b in tb), env))
+    return fr
+
+
+class _Run:
+    """Device state of one shear_fdtd solve."""
+
+    def __init__(self, shape, spacing, dT, n_steps, prec, kahan, dev):
+        lib = _native.load()
+        self.dev = dev
+        self.shape = shape
+        self.nx, self.ny, self.nz = shape
+        self.pz = int(lib.sw_pitch(self.nz))
+        self.ncell = self.nx * self.ny * self.pz
+        self.prec = prec
+        self.dt = _field_dtype(prec)
+        d = _native.FdtdDesc()
+        d.precision = prec
+        d.nx, d.ny, d.nz, d.pz = self.nx, self.ny, self.nz, self.pz
+        d.n_steps = n_steps
+        d.dX, d.dY, d.dZ = spacing
+        d.dT = dT
+        d.kahan = 1 if kahan else 0
+        self.desc = d
+        nbuf, ncomp = (3, 3) if prec == _native.SW_PLAIN_F64 else (2, 9)
+        self.state = torch.empty((nbuf, ncomp, self.ncell), dtype=self.dt, device=dev)
+        for i in range(nbuf):
+            d.state[i] = self.state[i].data_ptr()
+        self.coef_m = torch.zeros(self.ncell, dtype=self.dt, device=dev)
+        d.coef_m = self.coef_m.data_ptr()
+        self.coef_e = None
+        self.inv_rho = None
+        if prec == _native.SW_PLAIN_F64:
+            self.inv_rho = torch.zeros(self.ncell, dtype=self.dt, device=dev)
+            d.inv_rho = self.inv_rho.data_ptr()
+        self.flags = torch.zeros(1, dtype=torch.int32, device=dev)
+        d.flags = self.flags.data_ptr()
+        self.keep = []  # tensors referenced by the descriptor
+
+    def p(self):
+        return C.byref(self.desc)
+
+    def materials(self, rho, mu, eta, in_dt):
+        dev = self.dev
+        r, rs = _material(rho, self.shape, in_dt, dev)
+        m, ms = _material(mu, self.shape, in_dt, dev)
+        eta_mode, e, es = 0, None, 0.0
+        if eta is not None:
+            eta_mode = 1
+            e, es = _material(eta, self.shape, in_dt, dev)
+            self.coef_e = torch.zeros(self.ncell, dtype=self.dt, device=dev)
+            self.desc.coef_e = self.coef_e.data_ptr()
+        _native.call("sw_fdtd_materials", self.p(), dtype_code(in_dt), ptr(r), rs, ptr(m), ms,
+                     eta_mode, ptr(e), es, stream_handle())
+        self.rho_dev, self.rho_s = r, rs
+        self.keep += [r, m, e]
+
+    def set_patterns(self, pats: torch.Tensor, term_off, term_pat, term_scale):
+        self.patterns = pats
+        self.term_off = torch.as_tensor(np.asarray(term_off, np.int32), device=self.dev)
+        self.term_pat = torch.as_tensor(np.asarray(term_pat, np.int32), device=self.dev)
+        self.term_scale = torch.as_tensor(np.asarray(term_scale, np.float64), device=self.dev)
+        d = self.desc
+        d.patterns = pats.data_ptr()
+        d.n_patterns = int(pats.shape[0])
+        d.term_off = self.term_off.data_ptr()
+        d.term_pat = self.term_pat.data_ptr() if len(term_pat) else self.term_off.data_ptr()
+        d.term_scale = self.term_scale.data_ptr() if len(term_scale) else None
+        if not len(term_scale):
+            self.term_scale = torch.zeros(1, dtype=torch.float64, device=self.dev)
+            d.term_scale = self.term_scale.data_ptr()
+
+    def pattern_from(self, ws: _Workspace, dst: torch.Tensor, spacing_dt2: float):
+        """Store the projected force (ws.out) as a pattern of this form."""
+        if self.prec == _native.SW_PLAIN_F64:
+            dst.copy_(ws.out)  # FP64 f_S as is
+        else:
+            # dT^2 f_S / rho in FP32
+            r = self.rho_dev
+            if r is None:
+                scale, rptr, rs = spacing_dt2 / self.rho_s, None, (0, 0, 0)
+                rdt = _native.SW_F32
+            else:
+                scale, rptr, rs = spacing_dt2, ptr(r), (self.ny * self.nz, self.nz, 1)
+                rdt = dtype_code(r.dtype)
+            _native.call("sw_convert", 3, ws.out.data_ptr(), self.nx, self.ny, self.nz,
+                         _native.SW_F32, dst.data_ptr(), self.ncell, self.ny * self.pz, self.pz,
+                         1, scale, rdt, rptr, *rs, stream_handle())
+
+
+def validate_inputs(bx, by, bz, rho, mu, eta, opts, shape, n_steps) -> None:
+    """Every shape / length check of solver.py:88-171, 1060-1079 on the host.
+
+    Raises the reference's ValueError messages before any device work.
+    """
+    env_t = opts.get("env_t")
+    for b in (bx, by, bz):
+        if b is None:
+            continue
+        s = _shape(b)
+        ok = s == shape if env_t is not None else (s == shape or s == (*shape, n_steps))
+        if not ok:
+            raise ValueError("Body-force component has incompatible shape.")
+    if env_t is not None:
+        n_env = int(np.asarray(env_t.cpu() if is_tensor(env_t) else env_t).size)
+        if n_env != n_steps:
+            raise ValueError(f"env_t length ({n_env}) must equal n_steps ({n_steps}).")
+    for term in opts.get("force_terms") or ():
+        tb, tenv = ((term.get("bx"), term.get("by"), term.get("bz")), term["env"]) \
+            if isinstance(term, dict) else term
+        for b in tb:
+            if b is not None and _shape(b) != shape:
+                raise ValueError("Body-force component has incompatible shape.")
+        n_env = int(np.asarray(tenv.cpu() if is_tensor(tenv) else tenv).size)
+        if n_env != n_steps:
+            raise ValueError(f"env_t length ({n_env}) must equal n_steps ({n_steps}).")
+    for m in (rho, mu) + (() if eta is None else (eta,)):
+        if not np.isscalar(m) and _shape(m) != shape:
+            raise ValueError("Material field has incompatible shape.")
+    for key in ("initial_u", "initial_v"):
+        a = opts.get(key)
+        if a is not None and _shape(a) != (*shape, 3):
+            raise ValueError(f"{key} must match shape (nx,ny,nz,3)")
+
+
+def _prepare_opts(opts):
+    opts = dict(opts or {})
+    reproject_every = int(opts.get("reproject_every", 0) or 0)
+    if reproject_every < 0:
+        raise ValueError("reproject_every must be a non-negative integer.")
+    return opts, reproject_every
+
+
+def shear_fdtd(  # noqa: PLR0912, PLR0915
+    bx,
+    by,
+    bz,
+    rho,
+    mu,
+    dX,
+    dY,
+    dZ,
+    dT,
+    n_steps,
+    opts=None,
+    callback=None,
+    *,
+    trace_indices=None,
+    return_traces=False,
+    return_device=False,
+    snapshot_stride=None,
+):
+    """3-D collocated cell-centred shear FDTD solver on a B200 (drop-in).
+
+    Same contract as the reference ``shear_fdtd`` (solver.py:27-243): forces
+    ``(nx,ny,nz)`` (with ``opts["env_t"]``) or ``(nx,ny,nz,n_steps)``,
+    scalar or ``(nx,ny,nz)`` materials, the same opts keys (``vel_damp``,
+    ``eta``, ``env_t``, ``poisson_tol``, ``poisson_max_iters``,
+    ``reproject_every``, ``verbose``, ``progress_every``, ``initial_u``,
+    ``initial_v``) and returns ``(u, v)`` of shape ``(nx, ny, nz, 3)``.
+
+    Also accepts the ``shear_fdtd_jax`` keywords (solver.py:259-262):
+    ``snapshot_stride`` (adds ``u`` snapshots after every k steps as a third
+    return value), ``trace_indices`` / ``return_traces`` (z-displacement
+    traces ``(n_traces, n_steps)``) and ``return_device`` (torch CUDA tensors
+    instead of numpy arrays).
+
+    Additional opts: ``precision`` ("mixed" default, or "fp64"), ``kahan``
+    (True), ``force_terms`` (extra separable terms: list of
+    ``((bx, by, bz), env)``), ``snapshot_stride`` (alias of the keyword),
+    ``info`` (dict filled with CG statistics and a non-finite flag).
+
+    ``callback(it, u)`` is called after every step with a host copy of the new
+    displacement (the reference passes its live buffer; writing into the copy
+    does not feed back into the solve).
+    """
+    ref = bx if bx is not None else (by if by is not None else bz)
+    if ref is None:
+        raise ValueError("At least one body-force component must be provided.")
+    opts, reproject_every = _prepare_opts(opts)
+    if snapshot_stride is None:
+        snapshot_stride = opts.get("snapshot_stride")
+    snapshot_stride, trace_cells = _check_jax_kwargs(n_steps, trace_indices, return_traces,
+                                                     snapshot_stride)
+    n_steps = int(n_steps)
+    vel_damp = float(opts.get("vel_damp", 0.0))
+    tol = opts.get("poisson_tol", 1e-5)
+    max_iters = opts.get("poisson_max_iters", 200)
+    verbose = opts.get("verbose", False)
+    progress_every = opts.get("progress_every", max(1, n_steps // 10))
+    info = opts.get("info")
+    prec = _precision(opts)
+    dt = _field_dtype(prec)
+    np_dt = np_dtype(dt)
+
+    shape = tuple(int(s) for s in _shape(ref)[:3])
+    nx, ny, nz = shape
+    if trace_cells is not None and trace_cells.size:
+        if np.any(trace_cells < 0) or np.any(trace_cells >= np.asarray(shape)):
+            raise ValueError("trace_indices outside the grid.")
+    eta = opts.get("eta", 0.0)
+    if np.isscalar(eta):
+        eta = float(eta) if float(eta) != 0.0 else None
+    validate_inputs(bx, by, bz, rho, mu, eta, opts, shape, n_steps)
+    dev = require_cuda()
+    forces = _gather_forces(bx, by, bz, opts, shape, n_steps, dt, dev, np_dt)
+
+    run = _Run(shape, (dX, dY, dZ), dT, n_steps, prec, opts.get("kahan", True), dev)
+    run.desc.vel_damp = vel_damp
+    run.materials(rho, mu, eta, dt)
+
+    init_u = opts.get("initial_u")
+    init_v = opts.get("initial_v")
+    iu = iv = None
+    if init_u is not None:
+        if _shape(init_u) != (*shape, 3):
+            raise ValueError("initial_u must match shape (nx,ny,nz,3)")
+        iu = to_device(init_u, dt, dev)
+    if init_v is not None:
+        if _shape(init_v) != (*shape, 3):
+            raise ValueError("initial_v must match shape (nx,ny,nz,3)")
+        iv = to_device(init_v, dt, dev)
+    _native.call("sw_fdtd_init", run.p(), ptr(iu), ptr(iv), stream_handle())
+
+    # ---- forces: project the separable patterns once (solver.py:188-192) ----
+    ws = _Workspace(nx, ny, nz, dev)
+    cg_log = []
+    n_sep = len(forces.separable)
+    n_pat = n_sep + (1 if forces.stream4d is not None else 0)
+    pats = torch.zeros((max(n_pat, 1), 3, run.ncell), dtype=dt, device=dev)
+    if verbose and n_sep:
+        print("Pre-computing Helmholtz projection (separable force)...")
+    for k, (comps, _env) in enumerate(forces.separable):
+        st = _project_raw(ws, dtype_code(dt), comps, (ny * nz, nz, 1), shape, dX, dY, dZ, tol,
+                          max_iters)
+        cg_log.append(st)
+        run.pattern_from(ws, pats[k], dT * dT)
+    term_off, term_pat, term_scale = [0], [], []
+    for it in range(n_steps):
+        for k, (_c, env) in enumerate(forces.separable):
+            s = float(env[it])
+            if s != 0.0:
+                term_pat.append(k)
+                term_scale.append(s)
+        if forces.stream4d is not None and not forces.zero_steps[it]:
+            term_pat.append(n_sep)
+            term_scale.append(1.0)
+        term_off.append(len(term_pat))
+    run.set_patterns(pats, term_off, term_pat, term_scale)
+
+    # ---- outputs written by the step kernels ----
+    snaps = None
+    if snapshot_stride:
+        snaps = torch.zeros((n_steps // snapshot_stride, nx, ny, nz, 3), dtype=dt, device=dev)
+        run.desc.snap_stride = snapshot_stride
+        run.desc.snaps = snaps.data_ptr()
+    traces = None
+    if trace_cells is not None and return_traces:
+        tc = torch.as_tensor(trace_cells.reshape(-1), dtype=torch.int32, device=dev)
+        traces = torch.zeros((trace_cells.shape[0], n_steps), dtype=dt, device=dev)
+        run.keep.append(tc)
+        run.desc.n_traces = int(trace_cells.shape[0])
+        run.desc.trace_cells = tc.data_ptr()
+        run.desc.traces = traces.data_ptr()
+
+    # ---- time loop (solver.py:194-239) ----
+    per_step = callback is not None or forces.stream4d is not None
+    events = set()
+    if reproject_every:
+        events.update(range(reproject_every, n_steps + 1, reproject_every))
+    if verbose:
+        events.update(range(progress_every, n_steps + 1, progress_every))
+    u_cb = torch.empty((nx, ny, nz, 3), dtype=dt, device=dev) if callback is not None else None
+    tmp_sep = None
+    it = 0
+    strm = stream_handle()
+    while it < n_steps:
+        if per_step:
+            end = it + 1
+        else:
+            later = [e for e in events if e > it]
+            end = min(later) if later else n_steps
+        if forces.stream4d is not None and not forces.zero_steps[it]:
+            # per-step projection of b[..., it] (solver.py:198-199)
+            comps = [None if b is None else (b[..., it] if b.dim() == 4 else b).contiguous()
+                     for b in forces.stream4d]
+            st = _project_raw(ws, dtype_code(dt), comps, (ny * nz, nz, 1), shape, dX, dY, dZ,
+                              tol, max_iters)
+            cg_log.append(st)
+            if tmp_sep is None:
+                tmp_sep = pats[n_sep]
+            run.pattern_from(ws, tmp_sep, dT * dT)
+        _native.call("sw_fdtd_steps", run.p(), it, end - it, strm)
+        if callback is not None:
+            _native.call("sw_fdtd_finish", run.p(), end, ptr(u_cb), None, strm)
+            callback(end - 1, u_cb.cpu().numpy())
+        if verbose and end % progress_every == 0:
+            print(f"FDTD it={end}/{n_steps}")
+        if reproject_every and end % reproject_every == 0:
+            stats = (_native.CGStats * 2)()
+            _native.call("sw_fdtd_reproject", run.p(), end, float(tol), int(max_iters),
+                         ws.out.data_ptr(), ptr(ws.ws), ws.bytes, stats, strm)
+            cg_log += [stats[0].as_dict(), stats[1].as_dict()]
+        it = end
+
+    u = torch.empty((nx, ny, nz, 3), dtype=dt, device=dev)
+    v = torch.empty((nx, ny, nz, 3), dtype=dt, device=dev)
+    _native.call("sw_fdtd_finish", run.p(), n_steps, ptr(u), ptr(v), strm)
+    nonfinite = bool(run.flags.item())
+    if info is not None:
+        info.update(cg=cg_log, nonfinite=nonfinite,
+                    precision="fp64" if prec == _native.SW_PLAIN_F64 else "mixed")
+    if nonfinite:
+        warnings.warn("shear_fdtd: non-finite displacement encountered (unstable dT?)",
+                      RuntimeWarning, stacklevel=2)
+    out = [to_host(u, return_device), to_host(v, return_device)]
+    if snaps is not None:
+        out.append(to_host(snaps, return_device))
+    elif traces is not None:
+        out.append(to_host(traces, return_device))
+    return tuple(out)
+
+
+def shear_fdtd_jax(bx, by, bz, rho, mu, dX, dY, dZ, dT, n_steps, opts=None, callback=None,
+                   trace_indices=None, return_traces=False, return_device=False,
+                   snapshot_stride=None):
+    """``shear_fdtd_jax`` contract (solver.py:246-566) on the CUDA path.
+
+    Same errors as the reference's JAX solver: no callback, no
+    ``reproject_every``; device outputs are torch CUDA tensors.
+    """
+    ref = bx if bx is not None else (by if by is not None else bz)
+    if ref is None:
+        raise ValueError("At least one body-force component must be provided.")
+    if callback is not None:
+        raise ValueError("callback is not supported in shear_fdtd_jax.")
+    _check_jax_kwargs(n_steps, trace_indices, return_traces, snapshot_stride)
+    opts = dict(opts or {})
+    if opts.get("reproject_every"):
+        raise NotImplementedError(
+            "reproject_every is only implemented in the NumPy solver (shear_fdtd)."
+        )
+    opts.pop("jit", None)
+    return shear_fdtd(bx, by, bz, rho, mu, dX, dY, dZ, dT, n_steps, opts,
+                      trace_indices=trace_indices, return_traces=return_traces,
+                      return_device=return_device, snapshot_stride=snapshot_stride)

@@ -1,0 +1,117 @@
+"""Host-side argument handling of the drop-in API (no GPU needed).
+
+Every check below raises before the first device call, with the reference's
+messages (src/shearwave/solver.py:88-171, 287-308, 396-408, 1060-1079;
+src/shearwave/strain.py:98-100, 138-159).
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import shearwave_b200 as sw
+
+Z = np.zeros((6, 5, 4), np.float32)
+
+
+def _call(**kw):
+    args = dict(bx=None, by=None, bz=Z, rho=1000.0, mu=2000.0, dX=1e-3, dY=1e-3, dZ=1e-3,
+                dT=1e-6, n_steps=4, opts=None)
+    args.update(kw)
+    return sw.shear_fdtd(**args)
+
+
+def test_requires_a_force_component():
+    with pytest.raises(ValueError, match="At least one body-force component"):
+        _call(bz=None)
+
+
+def test_negative_reproject_every():
+    with pytest.raises(ValueError, match="reproject_every"):
+        _call(opts={"env_t": np.ones(4), "reproject_every": -1})
+
+
+def test_env_t_length():
+    with pytest.raises(ValueError, match=r"env_t length \(3\) must equal n_steps \(4\)"):
+        _call(opts={"env_t": np.ones(3)})
+
+
+def test_body_force_shape():
+    with pytest.raises(ValueError, match="Body-force component has incompatible shape"):
+        _call(bx=np.zeros((6, 5, 3), np.float32))
+    with pytest.raises(ValueError, match="Body-force component has incompatible shape"):
+        _call(bz=np.zeros((6, 5, 4, 3), np.float32))
+
+
+def test_material_shape():
+    with pytest.raises(ValueError, match="Material field has incompatible shape"):
+        _call(rho=np.ones((6, 5, 3)))
+    with pytest.raises(ValueError, match="Material field has incompatible shape"):
+        _call(opts={"eta": np.ones((2, 2, 2))})
+
+
+def test_initial_state_shape():
+    with pytest.raises(ValueError, match=r"initial_u must match shape"):
+        _call(opts={"initial_u": np.zeros((6, 5, 4))})
+    with pytest.raises(ValueError, match=r"initial_v must match shape"):
+        _call(opts={"initial_v": np.zeros((6, 5, 4, 2))})
+
+
+def test_snapshot_stride_errors():
+    with pytest.raises(ValueError, match="positive integer"):
+        _call(snapshot_stride=0)
+    with pytest.raises(ValueError, match="multiple of snapshot_stride"):
+        _call(snapshot_stride=3)
+    with pytest.raises(ValueError, match="not both supported"):
+        _call(snapshot_stride=2, return_traces=True, trace_indices=([0], [0], [0]))
+
+
+def test_trace_errors():
+    with pytest.raises(ValueError, match="trace_indices must be provided"):
+        _call(return_traces=True)
+    with pytest.raises(ValueError, match="3-tuple"):
+        _call(trace_indices=([0], [0]))
+    with pytest.raises(ValueError, match="same shape"):
+        _call(trace_indices=([0], [0, 1], [0]))
+    with pytest.raises(ValueError, match="1D"):
+        _call(trace_indices=([[0]], [[0]], [[0]]))
+    with pytest.raises(ValueError, match="outside the grid"):
+        _call(trace_indices=([6], [0], [0]), return_traces=True)
+
+
+def test_jax_entry_point_errors():
+    with pytest.raises(ValueError, match="callback is not supported"):
+        sw.shear_fdtd_jax(None, None, Z, 1000.0, 2000.0, 1e-3, 1e-3, 1e-3, 1e-6, 4,
+                          callback=lambda it, u: None)
+    with pytest.raises(NotImplementedError, match="reproject_every"):
+        sw.shear_fdtd_jax(None, None, Z, 1000.0, 2000.0, 1e-3, 1e-3, 1e-3, 1e-6, 4,
+                          opts={"reproject_every": 5})
+
+
+def test_unknown_precision():
+    with pytest.raises(ValueError, match="precision"):
+        _call(opts={"precision": "bf16"})
+
+
+def test_strain_validation():
+    with pytest.raises(ValueError, match="same shape"):
+        sw.compute_strain_tensor(np.zeros((4, 4, 4)), np.zeros((4, 4, 5)), np.zeros((4, 4, 4)),
+                                 1e-3, 1e-3, 1e-3)
+    with pytest.raises(ValueError, match="positive"):
+        sw.compute_strain_tensor(Z, Z, Z, -1e-3, 1e-3, 1e-3)
+    with pytest.raises(ValueError, match="3-D"):
+        sw.compute_strain_tensor(np.zeros((4, 4)), np.zeros((4, 4)), np.zeros((4, 4)),
+                                 1e-3, 1e-3, 1e-3)
+    with pytest.raises(ValueError, match="Voigt"):
+        sw.compute_strain_invariants(np.zeros((5, 5, 5, 3)))
+
+
+def test_no_cpu_fallback_without_a_gpu():
+    """With valid arguments and no CUDA device the call fails loudly."""
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    with pytest.raises(RuntimeError, match="CUDA device"):
+        _call(opts={"env_t": np.ones(4)})

@@ -1,0 +1,443 @@
+"""Benchmark of the shear_fdtd hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c1] [--impl ours|reference]
+
+One bench step is one full solve of the workload (force projection, the whole
+time loop, outputs) on seeded synthetic inputs with the config's shapes.
+Prints ONE JSON line (rank 0).  Multi-GPU runs are launched by torchrun, one
+rank per GPU; the solves are independent replicas (weak scaling, no
+collective on the data path) and the time is the max over ranks.
+
+value   Gcell-steps/s with inputs resident in HBM (device-timed, CUDA events)
+e2e     the same through the public API with numpy inputs and outputs
+        (host<->device copies inside the timed region, wall clock)
+roofline  the fused step kernel: algorithmic bytes per launch / mean launch
+        time, against the measured HBM copy bandwidth
+cpu_baseline  the FP32 CPU port of the reference time loop on a bounded
+        sample of the same workload, on this host's cores
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "Gcell-steps/s mixed+batched vs plain FP64 GPU @relL2≤1e-4; HBM %; p99 lat"
+UNIT = "Gcell-steps/s"
+FALLBACK_HBM_GBS = 6650.0
+# algorithmic bytes per cell-step of the fused step kernel (FP32 mixed form):
+# read u_c, u_p and write u_n (9 x 4 B) + mu/rho, eta/rho (2 x 4 B); push
+# steps read the projected force (3 x 4 B) in addition
+BYTES_CELL_STEP = {"mixed": 44.0, "fp64": 88.0}
+BYTES_PUSH = {"mixed": 12.0, "fp64": 24.0}
+
+
+# ---------------------------------------------------------------------------
+# helpers
+# ---------------------------------------------------------------------------
+def rank_info():
+    r = int(os.environ.get("RANK", "0"))
+    w = int(os.environ.get("WORLD_SIZE", "1"))
+    lr = int(os.environ.get("LOCAL_RANK", str(r)))
+    return r, w, lr
+
+
+def measured_hbm():
+    p = ROOT / "MEASURED_PEAKS.json"
+    try:
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def ncu_traffic(kernel: str, workload: str):
+    """dram bytes per launch recorded from an ncu capture (profiles/traffic.txt)."""
+    p = ROOT / "profiles" / "traffic.txt"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        parts = line.split()
+        if len(parts) >= 3 and parts[0] == kernel and parts[1] == workload:
+            try:
+                return float(parts[2])
+            except ValueError:
+                return None
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(self.gpu)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.out = ""
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=5)
+            except Exception:
+                self.proc.kill()
+                self.out = ""
+
+    def summary(self):
+        rows = []
+        for line in (self.out or "").splitlines():
+            p = [x.strip() for x in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                rows.append((float(p[1]), float(p[2]), p[5:9]))
+            except ValueError:
+                continue
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for _, _, r in rows for i, v in enumerate(r)
+                          if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": rows[0][1],
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------
+# workloads
+# ---------------------------------------------------------------------------
+def make_workload(name: str, rank: int, grid=None, nsteps=None):
+    from shearwave_b200 import workloads as W
+
+    if name == "c1":
+        shape = (grid, grid, grid) if grid else (192, 192, 192)
+        return [W.problem_c1(seed=rank, shape=shape, n_steps=nsteps or 2000)]
+    if name == "c0":
+        return [W.problem_c0()]
+    if name == "c3":
+        return W.batch_c3(seed=rank)
+    raise SystemExit(f"unknown workload {name}")
+
+
+def describe(name: str, probs) -> dict:
+    cs = sum(_cell_steps(p) for p in probs)
+    if name == "c1" and (_shape(probs[0]) != (192, 192, 192) or probs[0]["n_steps"] != 2000):
+        name = "c1"  # overridden size: grid / n_steps below say which
+    desc = {"workload": {"c0": "config-0 64^3 homogeneous, nT=500, snapshots every 10",
+                         "c1": "config-1 192^3 heterogeneous (12 inclusions), nT=2000, "
+                               "snapshots every 10, dT viscous clamp",
+                         "c3": "config-3 batch of 48 seeded solves 64^3..160x160x224, "
+                               "nT 500..3000"}[name],
+            "instances": len(probs), "cell_steps_per_rank": cs,
+            "grid": list(_shape(probs[0])) if len(probs) == 1 else "varied",
+            "n_steps": probs[0]["n_steps"] if len(probs) == 1 else "varied",
+            "dX_m": probs[0]["dX"], "precision": "mixed (FP32 fields, Kahan u, FP64 CG)",
+            "l2_flush": "none needed: per-solve state is larger than the 126 MB L2",
+            "data": "seeded synthetic inputs with the config shapes"}
+    return desc
+
+
+def _shape(p):
+    ref = p["bx"] if p["bx"] is not None else (p["by"] if p["by"] is not None else p["bz"])
+    return tuple(ref.shape[:3])
+
+
+def _cell_steps(p):
+    nx, ny, nz = _shape(p)
+    return nx * ny * nz * p["n_steps"]
+
+
+def _to_dev(obj, dev):
+    import torch
+
+    if isinstance(obj, np.ndarray):
+        return torch.from_numpy(obj).to(dev)
+    if isinstance(obj, dict):
+        return {k: _to_dev(v, dev) for k, v in obj.items()}
+    if isinstance(obj, (list, tuple)):
+        return type(obj)(_to_dev(v, dev) for v in obj)
+    return obj
+
+
+def _solve(p, precision, device_io, info=None):
+    import shearwave_b200 as sw
+
+    opts = dict(p["opts"], precision=precision)
+    if info is not None:
+        opts["info"] = info
+    return sw.shear_fdtd(p["bx"], p["by"], p["bz"], p["rho"], p["mu"], p["dX"], p["dY"], p["dZ"],
+                         p["dT"], p["n_steps"], opts, snapshot_stride=p.get("snapshot_stride"),
+                         return_device=device_io)
+
+
+def _nbytes(obj) -> int:
+    if isinstance(obj, np.ndarray):
+        return obj.nbytes
+    if isinstance(obj, dict):
+        return sum(_nbytes(v) for v in obj.values())
+    if isinstance(obj, (list, tuple)):
+        return sum(_nbytes(v) for v in obj)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the FP32 port of the reference time loop (oracle) on a sample
+# ---------------------------------------------------------------------------
+def _cpu_sample(p, budget_s: float):
+    from oracle import shearwave_oracle as O
+
+    shape = _shape(p)
+    rng = np.random.default_rng(0)
+    iu = (1e-6 * rng.standard_normal((*shape, 3))).astype(np.float32)
+    opts = dict(p["opts"])
+    opts.pop("force_terms", None)
+    opts["initial_u"] = iu
+    zero = np.zeros(shape, np.float32)
+    def timed(steps):
+        o = dict(opts, env_t=np.zeros(steps, np.float32))
+        t0 = time.perf_counter()
+        O.shear_fdtd(None, None, zero, p["rho"], p["mu"], p["dX"], p["dY"], p["dZ"], p["dT"],
+                     steps, opts=o, dtype=np.float32)
+        return time.perf_counter() - t0
+
+    t1 = timed(1)  # one step sizes the sample
+    steps = max(2, min(4096, int(budget_s / max(t1, 1e-4))))
+    t = timed(steps)
+    n = shape[0] * shape[1] * shape[2]
+    return n * steps / t / 1e9, steps, shape
+
+
+def cpu_baseline(probs, budget_s=12.0):
+    p = max(probs, key=_cell_steps)
+    v, steps, shape = _cpu_sample(p, budget_s)
+    return {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"FP32 CPU port of the reference time loop (oracle/shearwave_oracle.py), "
+                      f"{steps} steps on the {shape[0]}x{shape[1]}x{shape[2]} grid of this "
+                      f"workload, projection excluded, numpy single-threaded"}
+
+
+def _ref_worker(args):
+    p, budget = args
+    return _cpu_sample(p, budget)
+
+
+def run_reference(a, rank, world):
+    """Reference arm: the CPU port of the reference on the host's cores."""
+    if rank != 0:
+        return 0
+    probs = make_workload(a.workload, 0, a.grid, a.nsteps)
+    ncpu = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    procs = ncpu if len(probs) > 1 else 1
+    budget = 2.0
+    import multiprocessing as mp
+
+    ctx = mp.get_context("spawn")
+    samples = []
+    with ctx.Pool(procs) as pool:
+        for i in range(a.warmup + a.steps):
+            work = [(probs[(i * procs + j) % len(probs)], budget) for j in range(procs)]
+            t0 = time.perf_counter()
+            res = pool.map(_ref_worker, work)
+            el = time.perf_counter() - t0
+            cells = sum(r[1] * r[2][0] * r[2][1] * r[2][2] for r in res)
+            if i >= a.warmup:
+                samples.append((cells / el / 1e9, el))
+    val = statistics.median(s[0] for s in samples)
+    line = {
+        "metric": METRIC, "value": val, "unit": UNIT, "impl": "reference", "n_gpus": a.gpus,
+        "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": 1e3 * statistics.median(s[1] for s in samples),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic", "config": describe(a.workload, probs),
+        "cpu_baseline": {"value": val, "unit": UNIT, "cores": procs, "kind": "port",
+                         "sample": f"{procs} process(es) x ~{budget:.0f} s of the FP32 CPU port "
+                                   "of the reference time loop on this workload's grids"},
+        "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--workload", default="c1", choices=["c0", "c1", "c3"])
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--grid", type=int, default=None, help="c1 only: cubic grid override")
+    ap.add_argument("--nsteps", type=int, default=None, help="c1 only: nT override")
+    a = ap.parse_args(argv)
+    rank, world, local = rank_info()
+    if a.impl == "reference":
+        return run_reference(a, rank, world)
+
+    import torch
+    import torch.distributed as dist
+
+    import shearwave_b200._native as native
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        return float(t.item())
+
+    probs = make_workload(a.workload, rank, a.grid, a.nsteps)
+    dprobs = [_to_dev(p, dev) for p in probs]
+    cs_rank = sum(_cell_steps(p) for p in probs)
+
+    # ---- device-resident timing -------------------------------------------
+    for _ in range(a.warmup):
+        for p in dprobs:
+            _solve(p, "mixed", True)
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    infos = []
+    n0 = native.launch_count()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        start.record()
+        for _ in range(a.steps):
+            infos = []
+            outs = []
+            for p in dprobs:
+                info = {}
+                outs.append(_solve(p, "mixed", True, info))
+                infos.append(info)
+        end.record()
+        torch.cuda.synchronize()
+    barrier()
+    launches = native.launch_count() - n0
+    t_dev = max_over_ranks(start.elapsed_time(end) / 1e3)
+    value = sum_over_ranks(cs_rank) * a.steps / t_dev / 1e9
+
+    # roofline of the fused step kernel (the dominant kernel)
+    step_ms = sum(i["t_steps_ms"] for i in infos)
+    launches_step = sum(p["n_steps"] for p in probs)
+    alg_bytes = 0.0
+    for p, i in zip(probs, infos):
+        nx, ny, nz = _shape(p)
+        alg_bytes += nx * ny * nz * (BYTES_CELL_STEP["mixed"] * p["n_steps"]
+                                     + BYTES_PUSH["mixed"] * i["n_push_steps"])
+    per_launch_ms = step_ms / launches_step
+    achieved = alg_bytes / launches_step / (per_launch_ms / 1e3) / 1e9
+    peak, peak_kind = measured_hbm()
+    traffic = ncu_traffic("step_f32", a.workload)
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
+            "kernel": "step_f32 (fused KV step, mixed form)",
+            "mean_launch_us": per_launch_ms * 1e3,
+            "alg_bytes_per_launch": alg_bytes / launches_step,
+            "step_only_gcell_steps_s": cs_rank / (step_ms / 1e3) / 1e9}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": 1e3 * t_dev / a.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": describe(a.workload, probs), "roofline": roof,
+        "clocks": clk.summary(), "gpu_launches": int(launches),
+        "cg_iters": [c["iters"] for i in infos for c in i["cg"]],
+    }
+
+    # ---- plain FP64 GPU drop-in on the same workload ----------------------
+    if not a.no_fp64:
+        _solve(dprobs[0], "fp64", True)  # warm
+        torch.cuda.synchronize()
+        barrier()
+        s2, e2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s2.record()
+        o64 = [_solve(p, "fp64", True) for p in dprobs]
+        e2.record()
+        torch.cuda.synchronize()
+        t64 = max_over_ranks(s2.elapsed_time(e2) / 1e3)
+        v64 = sum_over_ranks(cs_rank) / t64 / 1e9
+        rl = []
+        for (u32, v32, *_), (u64, v64_, *_) in zip(outs, o64):
+            du = torch.linalg.vector_norm(u32.double() - u64) / torch.linalg.vector_norm(u64)
+            dv = torch.linalg.vector_norm(v32.double() - v64_) / torch.linalg.vector_norm(v64_)
+            rl.append((float(du), float(dv)))
+        line["vs_plain_fp64"] = {"value": v64, "unit": UNIT, "ratio": value / v64,
+                                 "rel_l2_u": max(r[0] for r in rl),
+                                 "rel_l2_v": max(r[1] for r in rl)}
+
+    # ---- end to end through the public API with host arrays ---------------
+    if not a.no_e2e:
+        h2d = sum(_nbytes({k: p[k] for k in ("bx", "by", "bz", "rho", "mu", "opts")})
+                  for p in probs)
+        _solve(probs[0], "mixed", False)
+        barrier()
+        t0 = time.perf_counter()
+        d2h = 0
+        for p in probs:
+            out = _solve(p, "mixed", False)
+            d2h += sum(o.nbytes for o in out)
+        torch.cuda.synchronize()
+        te = max_over_ranks(time.perf_counter() - t0)
+        line["e2e"] = {"value": sum_over_ranks(cs_rank) / te / 1e9, "unit": UNIT,
+                       "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                       "note": "numpy inputs/outputs through shear_fdtd, wall clock, one step"}
+
+    if rank == 0 and world == 1 and not a.no_cpu:
+        line["cpu_baseline"] = cpu_baseline(probs)
+
+    if world > 1:
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -76,6 +76,8 @@ int sw_set_device(int device);
 int sw_pitch(int nz);
 /* sizeof(sw_fdtd_desc), so a binding can check its mirror of the struct. */
 size_t sw_fdtd_desc_size(void);
+/* Number of kernels this library has launched in the process so far. */
+uint64_t sw_launch_count(void);
 
 /* ---- collocated FD operators on dense arrays (solver.py:686-729) ------- */
 /* laplacian_center: interior 7-point Laplacian, zero shell. */

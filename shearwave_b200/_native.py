@@ -65,6 +65,7 @@ _SIGNATURES = {
     "sw_set_device": ([C.c_int], C.c_int),
     "sw_pitch": ([C.c_int], C.c_int),
     "sw_fdtd_desc_size": ([], _sz),
+    "sw_launch_count": ([], C.c_uint64),
     "sw_laplacian": ([C.c_int, _vp, _vp, C.c_int, C.c_int, C.c_int, _f64, _f64, _f64, _vp],
                      C.c_int),
     "sw_divergence": ([C.c_int, _vp, _vp, _vp, _vp, C.c_int, C.c_int, C.c_int, _f64, _f64, _f64,
@@ -137,3 +138,8 @@ def call(name: str, *args) -> None:
     if rc != SW_OK:
         msg = lib.sw_last_error()
         raise NativeError(name, rc, msg.decode() if msg else "")
+
+
+def launch_count() -> int:
+    """Kernels launched by the library in this process so far."""
+    return int(load().sw_launch_count())

@@ -156,6 +156,8 @@ __device__ inline bool interior(const Geom& g, int x, int y, int z) {
 // ---------------------------------------------------------------------------
 void set_error(const char* fmt, ...);
 int cuda_status(cudaError_t e, const char* what);
+// Count kernel launches issued by this library (exported as sw_launch_count).
+void count_launches(unsigned long long n);
 
 #define SW_CHECK_LAUNCH(what)                                   \
   do {                                                          \

@@ -2,6 +2,8 @@
 #include <stdarg.h>
 #include <stdio.h>
 
+#include <atomic>
+
 #include "sw_common.cuh"
 
 namespace sw {
@@ -14,6 +16,10 @@ void set_error(const char* fmt, ...) {
   vsnprintf(g_err, sizeof g_err, fmt, ap);
   va_end(ap);
 }
+
+static std::atomic<unsigned long long> g_launches{0};
+
+void count_launches(unsigned long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
 int cuda_status(cudaError_t e, const char* what) {
   set_error("%s: %s (%s)", what, cudaGetErrorString(e), cudaGetErrorName(e));
@@ -35,3 +41,5 @@ extern "C" int sw_set_device(int device) {
 extern "C" int sw_pitch(int nz) { return nz > 0 ? sw::pad_pitch(nz) : 0; }
 
 extern "C" size_t sw_fdtd_desc_size(void) { return sizeof(sw_fdtd_desc); }
+
+extern "C" uint64_t sw_launch_count(void) { return sw::g_launches.load(); }

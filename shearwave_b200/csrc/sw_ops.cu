@@ -233,6 +233,7 @@ extern "C" int sw_laplacian(int dtype, const void* f, void* out, int nx, int ny,
     set_error("sw_laplacian: unknown dtype");
     return SW_EINVAL;
   }
+  count_launches(1);
   SW_CHECK_LAUNCH("laplacian");
   return SW_OK;
 }
@@ -259,6 +260,7 @@ extern "C" int sw_divergence(int dtype, const void* fx, const void* fy, const vo
     set_error("sw_divergence: unknown dtype");
     return SW_EINVAL;
   }
+  count_launches(1);
   SW_CHECK_LAUNCH("divergence");
   return SW_OK;
 }
@@ -286,6 +288,7 @@ extern "C" int sw_gradient(int dtype, const void* phi, void* gx, void* gy, void*
     set_error("sw_gradient: unknown dtype");
     return SW_EINVAL;
   }
+  count_launches(1);
   SW_CHECK_LAUNCH("gradient");
   return SW_OK;
 }
@@ -319,6 +322,7 @@ extern "C" int sw_strain(int dtype, const void* ux, const void* uy, const void* 
     set_error("sw_strain: unknown dtype");
     return SW_EINVAL;
   }
+  count_launches(1);
   SW_CHECK_LAUNCH("strain");
   return SW_OK;
 }
@@ -343,6 +347,7 @@ extern "C" int sw_strain_invariants(int dtype, const void* eps, int64_t n, void*
     set_error("sw_strain_invariants: unknown dtype");
     return SW_EINVAL;
   }
+  count_launches(1);
   SW_CHECK_LAUNCH("strain invariants");
   return SW_OK;
 }

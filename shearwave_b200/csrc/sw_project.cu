@@ -365,6 +365,7 @@ int cg_run(const CgInst* d_tab, int ninst, int ntiles, CgState* const* states, i
       cg_apply<<<grid, dim3(TILE_Z, TILE_Y), 0, s>>>(d_tab, ninst, ntiles);
       cg_update<<<grid, dim3(TILE_Z, TILE_Y), 0, s>>>(d_tab, ninst, ntiles);
     }
+    count_launches(2ull * batch);
     SW_CHECK_LAUNCH("cg iteration");
     batch = std::min(batch * 2, 64);
   }
@@ -419,10 +420,12 @@ int project_one(const void* fx, const void* fy, const void* fz, InStride fs, con
   if (ntiles > 0) {
     const int grid = std::max(1, std::min(ntiles, 148 * 8));
     cg_prep<T><<<grid, dim3(TILE_Z, TILE_Y), 0, s>>>(d_tab, 1, ntiles, d_fin, d_fs);
+    count_launches(1);
     SW_CHECK_LAUNCH("cg_prep");
     rc = cg_run(d_tab, 1, ntiles, &st, 1, s);
     if (rc != SW_OK) return rc;
     cg_finish<T><<<grid, dim3(TILE_Z, TILE_Y), 0, s>>>(d_tab, 1, ntiles, d_fin, d_fs, d_out);
+    count_launches(1);
     SW_CHECK_LAUNCH("cg_finish");
   }
   e = cudaMemcpyAsync(&hst, st, sizeof(hst), cudaMemcpyDeviceToHost, s);

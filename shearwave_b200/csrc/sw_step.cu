@@ -395,6 +395,7 @@ int launch_steps(const StepArgs& a, int it0, int nsteps, cudaStream_t s) {
       step_f32<<<grid, dim3(TILE_Z, TILE_Y), 0, s>>>(a, it);
     if (a.n_traces > 0) trace_kernel<<<(a.n_traces + 127) / 128, 128, 0, s>>>(a, it);
   }
+  count_launches((unsigned long long)nsteps * (a.n_traces > 0 ? 2 : 1));
   SW_CHECK_LAUNCH("step");
   return SW_OK;
 }
@@ -427,6 +428,7 @@ extern "C" int sw_fdtd_materials(const sw_fdtd_desc* d, int in_dtype, const void
     set_error("sw_fdtd_materials: unknown dtype %d", in_dtype);
     return SW_EINVAL;
   }
+  count_launches(1);
   SW_CHECK_LAUNCH("materials");
   return SW_OK;
 }
@@ -442,6 +444,7 @@ extern "C" int sw_fdtd_init(const sw_fdtd_desc* d, const void* init_u, const voi
     init_kernel<double><<<grid, 256, 0, s>>>(a, (const double*)init_u, (const double*)init_v);
   else
     init_kernel<float><<<grid, 256, 0, s>>>(a, (const float*)init_u, (const float*)init_v);
+  count_launches(1);
   SW_CHECK_LAUNCH("init");
   return SW_OK;
 }
@@ -465,6 +468,7 @@ extern "C" int sw_fdtd_finish(const sw_fdtd_desc* d, int32_t steps_done, void* u
   const long long n = (long long)a.g.nx * a.g.ny * a.g.nz;
   finish_kernel<<<grid_blocks(n, 256, 148 * 32), 256, 0, (cudaStream_t)stream>>>(a, steps_done,
                                                                                   u_out, v_out);
+  count_launches(1);
   SW_CHECK_LAUNCH("finish");
   return SW_OK;
 }
@@ -493,6 +497,7 @@ extern "C" int sw_fdtd_reproject(const sw_fdtd_desc* d, int32_t steps_done, doub
                          s);
       if (rc != SW_OK) return rc;
       write_back_kernel<<<grid, 256, 0, s>>>(tmp, g, b, 0, 0);
+      count_launches(1);
       SW_CHECK_LAUNCH("reproject write-back");
     }
   } else {
@@ -505,9 +510,11 @@ extern "C" int sw_fdtd_reproject(const sw_fdtd_desc* d, int32_t steps_done, doub
                          s);
       if (rc != SW_OK) return rc;
       write_back_kernel<<<grid, 256, 0, s>>>(tmp, g, S, 1, 3 * k);
+      count_launches(1);
       SW_CHECK_LAUNCH("reproject write-back");
     }
     zero_comp_kernel<<<grid, 256, 0, s>>>(S, g, 6, 3);
+    count_launches(1);
     SW_CHECK_LAUNCH("reproject reset");
   }
   return SW_OK;
@@ -538,6 +545,7 @@ extern "C" int sw_convert(int ncomp, const double* src, int nx, int ny, int nz, 
     return SW_EINVAL;
   }
 #undef SW_CONV
+  count_launches(1);
   SW_CHECK_LAUNCH("convert");
   return SW_OK;
 }

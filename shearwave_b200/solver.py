@@ -506,6 +506,10 @@ def shear_fdtd(  # noqa: PLR0912, PLR0915
     dev = require_cuda()
     forces = _gather_forces(bx, by, bz, opts, shape, n_steps, dt, dev, np_dt)
 
+    events = None
+    if info is not None:
+        events = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        events[0].record()
     run = _Run(shape, (dX, dY, dZ), dT, n_steps, prec, opts.get("kahan", True), dev)
     run.desc.vel_damp = vel_damp
     run.materials(rho, mu, eta, dt)
@@ -572,6 +576,8 @@ def shear_fdtd(  # noqa: PLR0912, PLR0915
     if verbose:
         events.update(range(progress_every, n_steps + 1, progress_every))
     u_cb = torch.empty((nx, ny, nz, 3), dtype=dt, device=dev) if callback is not None else None
+    if events is not None:
+        events[1].record()
     tmp_sep = None
     it = 0
     strm = stream_handle()
@@ -604,13 +610,22 @@ def shear_fdtd(  # noqa: PLR0912, PLR0915
             cg_log += [stats[0].as_dict(), stats[1].as_dict()]
         it = end
 
+    if events is not None:
+        events[2].record()
     u = torch.empty((nx, ny, nz, 3), dtype=dt, device=dev)
     v = torch.empty((nx, ny, nz, 3), dtype=dt, device=dev)
     _native.call("sw_fdtd_finish", run.p(), n_steps, ptr(u), ptr(v), strm)
     nonfinite = bool(run.flags.item())
     if info is not None:
+        events[3].record()
+        events[3].synchronize()
         info.update(cg=cg_log, nonfinite=nonfinite,
-                    precision="fp64" if prec == _native.SW_PLAIN_F64 else "mixed")
+                    precision="fp64" if prec == _native.SW_PLAIN_F64 else "mixed",
+                    t_setup_ms=events[0].elapsed_time(events[1]),
+                    t_steps_ms=events[1].elapsed_time(events[2]),
+                    t_finish_ms=events[2].elapsed_time(events[3]),
+                    n_push_steps=int(sum(1 for i in range(n_steps)
+                                         if term_off[i + 1] > term_off[i])))
     if nonfinite:
         warnings.warn("shear_fdtd: non-finite displacement encountered (unstable dT?)",
                       RuntimeWarning, stacklevel=2)

@@ -56,6 +56,7 @@ class FdtdDesc(C.Structure):
         ("flags", C.c_void_p),
         ("xchunk", C.c_int32),
         ("steps_per_pass", C.c_int32),
+        ("kernel", C.c_int32),
     ]
 
 

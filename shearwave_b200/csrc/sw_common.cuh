@@ -84,6 +84,34 @@ __host__ __device__ inline TileCoord tile_coord(const Geom& g, const TileSpace& 
   return c;
 }
 
+// Tile space / coordinates for an arbitrary (tz, ty) output tile.
+__host__ __device__ inline TileSpace make_tiles_t(const Geom& g, int xc, int tz, int ty) {
+  TileSpace t;
+  t.ntz = (g.nz + tz - 1) / tz;
+  t.nty = (g.ny + ty - 1) / ty;
+  int nxi = g.nx > 2 ? g.nx - 2 : 0;
+  t.xc = xc < 1 ? 1 : xc;
+  t.nxc = nxi > 0 ? (nxi + t.xc - 1) / t.xc : 0;
+  t.count = t.ntz * t.nty * t.nxc;
+  return t;
+}
+
+__host__ __device__ inline TileCoord tile_coord_t(const Geom& g, const TileSpace& t, int local,
+                                                  int tz, int ty) {
+  TileCoord c;
+  int zt = local % t.ntz;
+  int rest = local / t.ntz;
+  int yt = rest % t.nty;
+  int xt = rest / t.nty;
+  c.z0 = zt * tz;
+  c.y0 = yt * ty;
+  c.x0 = 1 + xt * t.xc;
+  int xe = c.x0 + t.xc;
+  int xl = g.nx - 1;
+  c.x1 = xe < xl ? xe : xl;
+  return c;
+}
+
 // Chunk length along x so that a launch over one grid has roughly `want`
 // tiles (at least one plane per chunk, at most the whole interior).
 inline int choose_xchunk(const Geom& g, long long want) {

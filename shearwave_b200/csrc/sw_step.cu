@@ -27,6 +27,7 @@
 #include "sw_common.cuh"
 #include "sw_project.cuh"
 #include "sw_step.cuh"
+#include "sw_step_tma.cuh"
 
 namespace sw {
 
@@ -80,6 +81,8 @@ int make_step_args(const sw_fdtd_desc* d, StepArgs* a) {
   a->trace_cells = d->trace_cells;
   a->traces = d->traces;
   a->flags = d->flags;
+  a->kernel = d->kernel;
+  a->xchunk = d->xchunk;
   const int nbuf = d->precision == SW_PLAIN_F64 ? 3 : 2;
   for (int i = 0; i < nbuf; ++i)
     if (a->state[i] == nullptr) {
@@ -387,6 +390,17 @@ __global__ void zero_comp_kernel(float* dst, Geom g, long long comp0, int ncomp)
 
 int launch_steps(const StepArgs& a, int it0, int nsteps, cudaStream_t s) {
   if (a.ts.count == 0) return SW_OK;
+  if (a.kernel == 0 && a.n_traces == 0) return launch_steps_tma(a, a.xchunk, it0, nsteps, s);
+  if (a.kernel == 0) {  // TMA steps one at a time, with the trace gather after each
+    for (int it = it0; it < it0 + nsteps; ++it) {
+      int rc = launch_steps_tma(a, a.xchunk, it, 1, s);
+      if (rc != SW_OK) return rc;
+      trace_kernel<<<(a.n_traces + 127) / 128, 128, 0, s>>>(a, it);
+      count_launches(1);
+    }
+    SW_CHECK_LAUNCH("trace");
+    return SW_OK;
+  }
   const int grid = std::min(a.ts.count, 148 * 16);
   for (int it = it0; it < it0 + nsteps; ++it) {
     if (a.precision == SW_PLAIN_F64)

@@ -27,6 +27,8 @@ struct StepArgs {
   const int* trace_cells;
   void* traces;
   int* flags;
+  int kernel;  // 0 TMA-staged, 1 direct loads
+  int xchunk;  // requested planes per tile (0 automatic)
 };
 
 int make_step_args(const sw_fdtd_desc* d, StepArgs* a);

@@ -467,7 +467,8 @@ def shear_fdtd(  # noqa: PLR0912, PLR0915
     instead of numpy arrays).
 
     Additional opts: ``precision`` ("mixed" default, or "fp64"), ``kahan``
-    (True), ``force_terms`` (extra separable terms: list of
+    (True), ``step_kernel`` ("tma" default, or "direct"), ``xchunk`` (planes
+    per tile along x, 0 = automatic), ``force_terms`` (extra separable terms: list of
     ``((bx, by, bz), env)``), ``snapshot_stride`` (alias of the keyword),
     ``info`` (dict filled with CG statistics and a non-finite flag).
 
@@ -506,12 +507,17 @@ def shear_fdtd(  # noqa: PLR0912, PLR0915
     dev = require_cuda()
     forces = _gather_forces(bx, by, bz, opts, shape, n_steps, dt, dev, np_dt)
 
-    events = None
+    tev = None  # CUDA events: start, steps begin, steps end, done
     if info is not None:
-        events = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
-        events[0].record()
+        tev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        tev[0].record()
     run = _Run(shape, (dX, dY, dZ), dT, n_steps, prec, opts.get("kahan", True), dev)
     run.desc.vel_damp = vel_damp
+    kern = opts.get("step_kernel", "tma")
+    if kern not in ("tma", "direct"):
+        raise ValueError("step_kernel must be 'tma' or 'direct'")
+    run.desc.kernel = 0 if kern == "tma" else 1
+    run.desc.xchunk = int(opts.get("xchunk", 0) or 0)
     run.materials(rho, mu, eta, dt)
 
     init_u = opts.get("initial_u")
@@ -576,8 +582,8 @@ def shear_fdtd(  # noqa: PLR0912, PLR0915
     if verbose:
         events.update(range(progress_every, n_steps + 1, progress_every))
     u_cb = torch.empty((nx, ny, nz, 3), dtype=dt, device=dev) if callback is not None else None
-    if events is not None:
-        events[1].record()
+    if tev is not None:
+        tev[1].record()
     tmp_sep = None
     it = 0
     strm = stream_handle()
@@ -610,20 +616,20 @@ def shear_fdtd(  # noqa: PLR0912, PLR0915
             cg_log += [stats[0].as_dict(), stats[1].as_dict()]
         it = end
 
-    if events is not None:
-        events[2].record()
+    if tev is not None:
+        tev[2].record()
     u = torch.empty((nx, ny, nz, 3), dtype=dt, device=dev)
     v = torch.empty((nx, ny, nz, 3), dtype=dt, device=dev)
     _native.call("sw_fdtd_finish", run.p(), n_steps, ptr(u), ptr(v), strm)
     nonfinite = bool(run.flags.item())
     if info is not None:
-        events[3].record()
-        events[3].synchronize()
+        tev[3].record()
+        tev[3].synchronize()
         info.update(cg=cg_log, nonfinite=nonfinite,
                     precision="fp64" if prec == _native.SW_PLAIN_F64 else "mixed",
-                    t_setup_ms=events[0].elapsed_time(events[1]),
-                    t_steps_ms=events[1].elapsed_time(events[2]),
-                    t_finish_ms=events[2].elapsed_time(events[3]),
+                    t_setup_ms=tev[0].elapsed_time(tev[1]),
+                    t_steps_ms=tev[1].elapsed_time(tev[2]),
+                    t_finish_ms=tev[2].elapsed_time(tev[3]),
                     n_push_steps=int(sum(1 for i in range(n_steps)
                                          if term_off[i + 1] > term_off[i])))
     if nonfinite:

@@ -1,0 +1,84 @@
+"""Step kernels against each other and against the FP64 oracle on awkward grids.
+
+Grids are chosen to hit tile edges (z tiles of 64 / 32 cells, y tiles of 8
+rows), short and long x chunks, non-multiple-of-8 z pitches and grids with
+a single interior plane.  Tolerances: the TMA-staged and direct-load kernels
+compute the same expression per cell, so they agree to FP rounding (rel L2
+<= 1e-12 in FP64, <= 1e-6 in FP32); the FP64 form matches the oracle to
+rel L2 <= 1e-10 and the mixed form to <= 1e-4.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+GRIDS = [(5, 7, 9), (17, 13, 11), (3, 20, 70), (40, 9, 133), (12, 33, 65)]
+
+
+def _problem(shape, seed, n_steps=24):
+    rng = np.random.default_rng(seed)
+    h = (0.5e-3, 0.6e-3, 0.45e-3)
+    rho = (1000.0 * (1 + 0.05 * rng.uniform(-1, 1, shape))).astype(np.float32)
+    mu = (3e3 * np.exp(rng.uniform(-1, 1, shape))).astype(np.float32)
+    eta = rng.uniform(0.2, 1.0, shape).astype(np.float32)
+    ax = [(np.arange(n) - (n - 1) / 2.0) * hh for n, hh in zip(shape, h)]
+    x, y, z = np.meshgrid(*ax, indexing="ij")
+    bz = (1e3 * np.exp(-(x**2 + y**2) / (2 * 1e-3**2) - z**2 / (2 * 2e-3**2))).astype(np.float32)
+    bx = (200 * np.exp(-((x - 5e-4) ** 2 + y**2 + z**2) / (2 * 1e-3**2))).astype(np.float32)
+    env = np.zeros(n_steps, np.float32)
+    env[:6] = np.linspace(1.0, 0.5, 6)
+    iu = (1e-7 * rng.standard_normal((*shape, 3))).astype(np.float32)
+    opts = {"eta": eta, "env_t": env, "vel_damp": 0.01, "poisson_tol": 1e-10,
+            "poisson_max_iters": 4 * max(shape), "initial_u": iu}
+    return dict(bx=bx, by=None, bz=bz, rho=rho, mu=mu, dX=h[0], dY=h[1], dZ=h[2], dT=4e-6,
+                n_steps=n_steps), opts
+
+
+def _run(p, opts, **kw):
+    import shearwave_b200 as sw
+
+    o = dict(opts, **kw)
+    return sw.shear_fdtd(p["bx"], p["by"], p["bz"], p["rho"], p["mu"], p["dX"], p["dY"], p["dZ"],
+                         p["dT"], p["n_steps"], o, snapshot_stride=6)
+
+
+@pytest.mark.parametrize("shape", GRIDS)
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_tma_matches_direct_kernel(cuda, shape, precision):
+    p, opts = _problem(shape, seed=sum(shape))
+    a = _run(p, opts, precision=precision, step_kernel="tma")
+    b = _run(p, opts, precision=precision, step_kernel="direct")
+    tol = 1e-12 if precision == "fp64" else 1e-6
+    for x, y in zip(a, b):
+        assert rel_l2(x, y) <= tol
+
+
+@pytest.mark.parametrize("xchunk", [1, 2, 7, 1000])
+def test_xchunk_does_not_change_results(cuda, xchunk):
+    p, opts = _problem((30, 18, 70), seed=3)
+    ref = _run(p, opts, precision="fp64", xchunk=0)
+    got = _run(p, opts, precision="fp64", xchunk=xchunk)
+    for x, y in zip(ref, got):
+        assert np.array_equal(x, y)
+
+
+@pytest.mark.parametrize("shape", GRIDS[:4])
+def test_against_oracle(cuda, shape):
+    from oracle import shearwave_oracle as O
+
+    p, opts = _problem(shape, seed=7 + shape[0])
+    o64 = {k: (v.astype(np.float64) if isinstance(v, np.ndarray) else v) for k, v in opts.items()}
+    ref = O.shear_fdtd(p["bx"].astype(np.float64), None, p["bz"].astype(np.float64),
+                       p["rho"].astype(np.float64), p["mu"].astype(np.float64), p["dX"], p["dY"],
+                       p["dZ"], p["dT"], p["n_steps"], opts=o64, dtype=np.float64,
+                       snapshot_stride=6)
+    g64 = _run(p, opts, precision="fp64")
+    g32 = _run(p, opts, precision="mixed")
+    for r, a, b in zip(ref, g64, g32):
+        assert rel_l2(a, r) <= 1e-10
+        assert rel_l2(b, r) <= 1e-4

@@ -92,8 +92,9 @@ __device__ inline bool ring_wait(Ring& r, int stage) {
 // ---------------------------------------------------------------------------
 __device__ inline void tile_f32(const TmaF32& in, int local, int lit, float* sm, Ring& ring,
                                 int* abort_flag) {
-  constexpr int W = TmaF32::W, H = TmaF32::H, NST = TmaF32::NST, PL = TmaF32::PLANE;
-  constexpr uint32_t BYTES = PL * sizeof(float);
+  constexpr int W = TmaF32::W, H = TmaF32::H, NST = TmaF32::NST, PL = TmaF32::STAGE;
+  constexpr uint32_t BYTES = TmaF32::PLANE * sizeof(float);
+  static_assert((PL * sizeof(float)) % 128 == 0, "TMA destinations must be 128-byte aligned");
   const Geom& g = in.g;
   const TileCoord tc = tile_coord_t(g, in.ts, local, TmaF32::TZ, TmaF32::TY);
   const CUtensorMap* tm = &in.tm[lit & 1];
@@ -200,9 +201,10 @@ __device__ inline void tile_f32(const TmaF32& in, int local, int lit, float* sm,
 // ---------------------------------------------------------------------------
 __device__ inline void tile_f64(const TmaF64& in, int local, int lit, double* sm, Ring& ring,
                                 int* abort_flag) {
-  constexpr int W = TmaF64::W, H = TmaF64::H, NST = TmaF64::NST, PL = TmaF64::PLANE;
-  constexpr int HALF = PL / 2;
-  constexpr uint32_t BYTES = PL * sizeof(double);
+  constexpr int W = TmaF64::W, H = TmaF64::H, NST = TmaF64::NST, PL = TmaF64::STAGE;
+  constexpr int HALF = TmaF64::HALF;
+  constexpr uint32_t BYTES = TmaF64::PLANE * sizeof(double);
+  static_assert((HALF * sizeof(double)) % 128 == 0, "TMA destinations must be 128-byte aligned");
   const Geom& g = in.g;
   const TileCoord tc = tile_coord_t(g, in.ts, local, TmaF64::TZ, TmaF64::TY);
   const CUtensorMap* tmp = &in.tm[lit % 3];
@@ -326,10 +328,17 @@ template <bool BATCH>
 __global__ void __launch_bounds__(256, 3)
     step_f32_tma(const __grid_constant__ TmaF32 one, const TmaF32* __restrict__ tab, int ninst,
                  int ntiles, int it) {
-  extern __shared__ __align__(128) unsigned char smem_raw[];
-  uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw);
-  float* sm = reinterpret_cast<float*>(smem_raw + 128);
-  __shared__ int abort_flag;
+  extern __shared__ unsigned char smem_raw[];
+  // 128-byte aligned header (mbarriers, abort flag) followed by the stages
+  unsigned char* base = smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(base);
+  int& abort_flag = *reinterpret_cast<int*>(base + 64);
+  float* sm = reinterpret_cast<float*>(base + 128);
+  if ((smem_addr(sm) & 127u) != 0u) {  // never issue a TMA to a misaligned destination
+    int* fl = BATCH ? (ninst > 0 ? tab[0].flags : nullptr) : one.flags;
+    if (threadIdx.x == 0 && fl) atomicOr(fl, 4);
+    return;
+  }
   if (threadIdx.x == 0) {
     for (int s = 0; s < TmaF32::NST; ++s) mbar_init(&bars[s], 1);
     mbar_fence_init();
@@ -363,10 +372,17 @@ template <bool BATCH>
 __global__ void __launch_bounds__(256, 3)
     step_f64_tma(const __grid_constant__ TmaF64 one, const TmaF64* __restrict__ tab, int ninst,
                  int ntiles, int it) {
-  extern __shared__ __align__(128) unsigned char smem_raw[];
-  uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw);
-  double* sm = reinterpret_cast<double*>(smem_raw + 128);
-  __shared__ int abort_flag;
+  extern __shared__ unsigned char smem_raw[];
+  // 128-byte aligned header (mbarriers, abort flag) followed by the stages
+  unsigned char* base = smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(base);
+  int& abort_flag = *reinterpret_cast<int*>(base + 64);
+  double* sm = reinterpret_cast<double*>(base + 128);
+  if ((smem_addr(sm) & 127u) != 0u) {  // never issue a TMA to a misaligned destination
+    int* fl = BATCH ? (ninst > 0 ? tab[0].flags : nullptr) : one.flags;
+    if (threadIdx.x == 0 && fl) atomicOr(fl, 4);
+    return;
+  }
   if (threadIdx.x == 0) {
     for (int s = 0; s < TmaF64::NST; ++s) mbar_init(&bars[s], 1);
     mbar_fence_init();
@@ -399,9 +415,10 @@ __global__ void __launch_bounds__(256, 3)
 // ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
+// dynamic shared memory: alignment slack + header + stages
 size_t tma_smem_bytes(int precision) {
-  return precision == SW_PLAIN_F64 ? 128 + (size_t)TmaF64::NST * TmaF64::PLANE * sizeof(double)
-                                   : 128 + (size_t)TmaF32::NST * TmaF32::PLANE * sizeof(float);
+  return precision == SW_PLAIN_F64 ? 256 + (size_t)TmaF64::NST * TmaF64::STAGE * sizeof(double)
+                                   : 256 + (size_t)TmaF32::NST * TmaF32::STAGE * sizeof(float);
 }
 
 static int set_smem_attr(int precision) {

@@ -16,7 +16,8 @@ struct TmaF32 {
   static constexpr int H = TY + 2;         // box height: 1 row of halo each side in y
   static constexpr int NF = 6;             // halo'd components per plane: u, d
   static constexpr int NST = 4;            // plane stages in the ring
-  static constexpr int PLANE = W * H * NF; // floats per stage
+  static constexpr int PLANE = W * H * NF; // floats per stage (box of the one TMA load)
+  static constexpr int STAGE = ((PLANE * 4 + 127) / 128) * 128 / 4;  // 128-byte aligned stride
   CUtensorMap tm[2];
   Geom g;
   TileSpace ts;
@@ -43,7 +44,10 @@ struct TmaF64 {
   static constexpr int H = TY + 2;
   static constexpr int NF = 6;      // u_prev (3) then u_curr (3)
   static constexpr int NST = 4;
-  static constexpr int PLANE = W * H * NF;
+  static constexpr int PLANE = W * H * NF;  // doubles of the two boxes
+  // each box lands on a 128-byte boundary (TMA destination alignment)
+  static constexpr int HALF = ((W * H * 3 * 8 + 127) / 128) * 128 / 8;
+  static constexpr int STAGE = 2 * HALF;
   CUtensorMap tm[3];
   Geom g;
   TileSpace ts;

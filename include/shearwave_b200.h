@@ -112,6 +112,30 @@ int sw_project(int in_dtype, const void* fx, const void* fy, const void* fz, int
                double dZ, double tol, int max_iters, double* out, void* workspace,
                size_t workspace_bytes, sw_cg_stats* stats, void* stream);
 
+/* One solve of a batched projection (fields as for sw_project). */
+typedef struct sw_project_job {
+  int32_t in_dtype;
+  const void* fx;
+  const void* fy;
+  const void* fz;
+  int64_t sx, sy, sz;
+  int32_t nx, ny, nz;
+  double dX, dY, dZ, tol;
+  int32_t max_iters;
+  double* out;            /* 3 padded FP64 components */
+  void* workspace;        /* sw_project_workspace_bytes(nx, ny, nz) bytes */
+  size_t workspace_bytes;
+} sw_project_job;
+
+/* Device bytes of the instance table sw_project_batch needs for n jobs. */
+size_t sw_project_batch_table_bytes(int n);
+
+/* Project n independent fields together: every CG launch advances all
+ * unfinished solves (same dtype for all jobs); each solve keeps its own
+ * stopping rule and iteration count.  `stats` (host) receives n entries. */
+int sw_project_batch(const sw_project_job* jobs, int n, void* table, size_t table_bytes,
+                     sw_cg_stats* stats, void* stream);
+
 /* dst = src * scale / rho (rho NULL: dst = src * scale) for `ncomp` padded FP64
  * components into `dst` (dtype out_dtype, element (x,y,z) of component c at
  * c*dst_cs + x*dst_sx + y*dst_sy + z*dst_sz).  rho is dense or strided like
@@ -134,7 +158,8 @@ typedef struct sw_fdtd_desc {
   void* state[3];
   /* Material coefficients, padded, written by sw_fdtd_materials:
    *   F64: coef_m = mu/rho, coef_e = eta/rho (NULL: no viscosity), inv_rho = 1/rho.
-   *   F32: coef_m = dT^2 mu/rho, coef_e = dT eta/rho (NULL: none), inv_rho unused. */
+   *   F32: coef_m = dT^2 mu/rho, coef_e = dT eta/rho (NULL: none), inv_rho unused.
+   * The TMA kernels (kernel == 0) need coef_e == coef_m + ncell elements. */
   void* coef_m;
   void* coef_e;
   void* inv_rho;
@@ -177,6 +202,18 @@ int sw_fdtd_steps(const sw_fdtd_desc* d, int32_t it0, int32_t nsteps, void* stre
  * (nx,ny,nz,3) arrays of the field dtype (either may be NULL). */
 int sw_fdtd_finish(const sw_fdtd_desc* d, int32_t steps_done, void* u_out, void* v_out,
                    void* stream);
+
+/* Device bytes of the instance table sw_fdtd_batch_steps needs for n solves. */
+size_t sw_fdtd_batch_table_bytes(int n);
+
+/* Advance a batch of independent solves (same precision, TMA kernels, no
+ * traces).  Solve i runs its local step it - begins[i] at global step it
+ * when 0 <= it - begins[i] < n_steps (begins NULL: all start at 0).  One
+ * launch per global step covers the tiles of every running solve, so small
+ * and large grids share the GPU.  `table`: 64-byte aligned device memory of
+ * sw_fdtd_batch_table_bytes(n) bytes. */
+int sw_fdtd_batch_steps(const sw_fdtd_desc* descs, const int32_t* begins, int n, int32_t it0,
+                        int32_t nsteps, void* table, size_t table_bytes, void* stream);
 
 /* Project the state in place after `steps_done` steps (reproject_every,
  * solver.py:236-239): u_curr and u_prev each go through sw_project. */

@@ -14,6 +14,7 @@ from .solver import (
     project_body_force_to_shear,
     project_vector_field,
     shear_fdtd,
+    shear_fdtd_batch,
     shear_fdtd_jax,
 )
 from .strain import compute_strain_fields, compute_strain_invariants, compute_strain_tensor
@@ -31,5 +32,6 @@ __all__ = [
     "project_body_force_to_shear",
     "project_vector_field",
     "shear_fdtd",
+    "shear_fdtd_batch",
     "shear_fdtd_jax",
 ]

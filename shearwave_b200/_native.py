@@ -33,6 +33,22 @@ class CGStats(C.Structure):
                 "rel": float(self.rel), "max_div": float(self.max_div)}
 
 
+class ProjectJob(C.Structure):
+    """sw_project_job."""
+
+    _fields_ = [
+        ("in_dtype", C.c_int32),
+        ("fx", C.c_void_p), ("fy", C.c_void_p), ("fz", C.c_void_p),
+        ("sx", C.c_int64), ("sy", C.c_int64), ("sz", C.c_int64),
+        ("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32),
+        ("dX", C.c_double), ("dY", C.c_double), ("dZ", C.c_double), ("tol", C.c_double),
+        ("max_iters", C.c_int32),
+        ("out", C.c_void_p),
+        ("workspace", C.c_void_p),
+        ("workspace_bytes", C.c_size_t),
+    ]
+
+
 class FdtdDesc(C.Structure):
     """sw_fdtd_desc (field order and types must match the header)."""
 
@@ -76,6 +92,12 @@ _SIGNATURES = {
     "sw_project_workspace_bytes": ([C.c_int, C.c_int, C.c_int], _sz),
     "sw_project": ([C.c_int, _vp, _vp, _vp, _i64, _i64, _i64, C.c_int, C.c_int, C.c_int, _f64,
                     _f64, _f64, _f64, C.c_int, _vp, _vp, _sz, C.POINTER(CGStats), _vp], C.c_int),
+    "sw_project_batch_table_bytes": ([C.c_int], _sz),
+    "sw_project_batch": ([C.POINTER(ProjectJob), C.c_int, _vp, _sz, C.POINTER(CGStats), _vp],
+                         C.c_int),
+    "sw_fdtd_batch_table_bytes": ([C.c_int], _sz),
+    "sw_fdtd_batch_steps": ([C.POINTER(FdtdDesc), C.POINTER(C.c_int32), C.c_int, _i32, _i32, _vp,
+                             _sz, _vp], C.c_int),
     "sw_convert": ([C.c_int, _vp, C.c_int, C.c_int, C.c_int, C.c_int, _vp, _i64, _i64, _i64,
                     _i64, _f64, C.c_int, _vp, _i64, _i64, _i64, _vp], C.c_int),
     "sw_fdtd_materials": ([C.POINTER(FdtdDesc), C.c_int, _vp, _f64, _vp, _f64, C.c_int, _vp,

@@ -343,23 +343,21 @@ int cg_layout(const Geom& g, char* ws, size_t ws_bytes, CgInst* in, CgState** st
   return SW_OK;
 }
 
-int cg_run(const CgInst* d_tab, int ninst, int ntiles, CgState* const* states, int nst,
+int cg_run(const CgInst* d_tab, int ninst, int ntiles, CgState* d_states, int nst,
            cudaStream_t s) {
-  // Launch CG iterations in growing batches; after each batch read the
-  // instances' exit reasons (one small D2H copy) and stop when all are done.
+  // Launch CG iterations in growing batches; after each batch read every
+  // instance's exit reason (one small D2H copy of the contiguous state
+  // array) and stop when all are done.
   const int grid = std::max(1, std::min(ntiles, 148 * 8));
-  std::vector<int> reasons(nst, SW_CG_RUNNING);
+  std::vector<CgState> h(nst);
   int batch = 4;
   for (;;) {
+    cudaError_t e = cudaMemcpyAsync(h.data(), d_states, nst * sizeof(CgState),
+                                    cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_status(e, "cg state readback");
     bool running = false;
-    for (int i = 0; i < nst; ++i) {
-      cudaError_t e = cudaMemcpyAsync(&reasons[i], &states[i]->reason, sizeof(int),
-                                      cudaMemcpyDeviceToHost, s);
-      if (e != cudaSuccess) return cuda_status(e, "cg reason readback");
-    }
-    cudaError_t e = cudaStreamSynchronize(s);
-    if (e != cudaSuccess) return cuda_status(e, "cg synchronize");
-    for (int i = 0; i < nst; ++i) running |= (reasons[i] == SW_CG_RUNNING);
+    for (int i = 0; i < nst; ++i) running |= (h[i].reason == SW_CG_RUNNING);
     if (!running) return SW_OK;
     for (int b = 0; b < batch; ++b) {
       cg_apply<<<grid, dim3(TILE_Z, TILE_Y), 0, s>>>(d_tab, ninst, ntiles);
@@ -422,7 +420,7 @@ int project_one(const void* fx, const void* fy, const void* fz, InStride fs, con
     cg_prep<T><<<grid, dim3(TILE_Z, TILE_Y), 0, s>>>(d_tab, 1, ntiles, d_fin, d_fs);
     count_launches(1);
     SW_CHECK_LAUNCH("cg_prep");
-    rc = cg_run(d_tab, 1, ntiles, &st, 1, s);
+    rc = cg_run(d_tab, 1, ntiles, st, 1, s);
     if (rc != SW_OK) return rc;
     cg_finish<T><<<grid, dim3(TILE_Z, TILE_Y), 0, s>>>(d_tab, 1, ntiles, d_fin, d_fs, d_out);
     count_launches(1);
@@ -486,4 +484,142 @@ extern "C" int sw_project(int in_dtype, const void* fx, const void* fy, const vo
   InStride fs{in_sx, in_sy, in_sz};
   return project_field(in_dtype, fx, fy, fz, fs, g, dX, dY, dZ, tol, max_iters, out, workspace,
                        workspace_bytes, stats, (cudaStream_t)stream);
+}
+
+// ---------------------------------------------------------------------------
+// batched projection: many independent solves advance together, one launch
+// per CG phase over all their tiles
+// ---------------------------------------------------------------------------
+namespace {
+struct BatchTableLayout {
+  size_t inst, state, fin, strides, outs, total;
+};
+BatchTableLayout batch_layout(int n) {
+  BatchTableLayout L;
+  size_t off = 0;
+  L.inst = off;
+  off += align_up((size_t)n * sizeof(CgInst), 256);
+  L.state = off;
+  off += align_up((size_t)n * sizeof(CgState), 256);
+  L.fin = off;
+  off += align_up((size_t)3 * n * sizeof(void*), 256);
+  L.strides = off;
+  off += align_up((size_t)n * sizeof(InStride), 256);
+  L.outs = off;
+  off += align_up((size_t)n * sizeof(double*), 256);
+  L.total = off;
+  return L;
+}
+
+template <typename T>
+int project_batch_t(const sw_project_job* jobs, int n, char* table, sw_cg_stats* stats,
+                    cudaStream_t s) {
+  const BatchTableLayout L = batch_layout(n);
+  std::vector<CgInst> insts(n);
+  std::vector<CgState> hst(n);
+  std::vector<const void*> fin(3 * (size_t)n);
+  std::vector<InStride> strides(n);
+  std::vector<double*> outs(n);
+  CgState* d_states = (CgState*)(table + L.state);
+  int ntiles = 0;
+  cudaError_t e = cudaSuccess;
+  for (int i = 0; i < n; ++i) {
+    const sw_project_job& j = jobs[i];
+    Geom g = make_geom(j.nx, j.ny, j.nz, pad_pitch(j.nz));
+    CgState* st_unused = nullptr;
+    char* tail = nullptr;
+    int rc = cg_layout(g, (char*)j.workspace, j.workspace_bytes, &insts[i], &st_unused, &tail);
+    if (rc != SW_OK) return rc;
+    insts[i].st = d_states + i;
+    insts[i].c2x = 1.0 / (2.0 * j.dX);
+    insts[i].c2y = 1.0 / (2.0 * j.dY);
+    insts[i].c2z = 1.0 / (2.0 * j.dZ);
+    insts[i].tile_base = ntiles;
+    ntiles += insts[i].ts.count;
+    hst[i] = CgState{};
+    hst[i].tol = j.tol;
+    hst[i].max_iters = j.max_iters;
+    hst[i].reason = insts[i].ts.count > 0 ? SW_CG_RUNNING : SW_CG_EARLY_EXIT;
+    fin[3 * i + 0] = j.fx;
+    fin[3 * i + 1] = j.fy;
+    fin[3 * i + 2] = j.fz;
+    strides[i] = InStride{j.sx, j.sy, j.sz};
+    outs[i] = j.out;
+    const size_t vec = align_up((size_t)g.ncell * sizeof(double), 256);
+    if (e == cudaSuccess) e = cudaMemsetAsync(insts[i].x, 0, 5 * vec, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(j.out, 0, (size_t)g.ncell * 3 * sizeof(double), s);
+  }
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(table + L.inst, insts.data(), n * sizeof(CgInst), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(d_states, hst.data(), n * sizeof(CgState), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(table + L.fin, fin.data(), fin.size() * sizeof(void*),
+                        cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(table + L.strides, strides.data(), n * sizeof(InStride),
+                        cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(table + L.outs, outs.data(), n * sizeof(double*), cudaMemcpyHostToDevice,
+                        s);
+  if (e != cudaSuccess) return cuda_status(e, "batched projection setup");
+  const CgInst* d_tab = (const CgInst*)(table + L.inst);
+  if (ntiles > 0) {
+    const int grid = std::max(1, std::min(ntiles, 148 * 8));
+    cg_prep<T><<<grid, dim3(TILE_Z, TILE_Y), 0, s>>>(d_tab, n, ntiles, (const T* const*)(table + L.fin),
+                                                     (const InStride*)(table + L.strides));
+    count_launches(1);
+    SW_CHECK_LAUNCH("cg_prep (batch)");
+    int rc = cg_run(d_tab, n, ntiles, d_states, n, s);
+    if (rc != SW_OK) return rc;
+    cg_finish<T><<<grid, dim3(TILE_Z, TILE_Y), 0, s>>>(d_tab, n, ntiles,
+                                                       (const T* const*)(table + L.fin),
+                                                       (const InStride*)(table + L.strides),
+                                                       (double* const*)(table + L.outs));
+    count_launches(1);
+    SW_CHECK_LAUNCH("cg_finish (batch)");
+  }
+  e = cudaMemcpyAsync(hst.data(), d_states, n * sizeof(CgState), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return cuda_status(e, "batched projection readback");
+  if (stats)
+    for (int i = 0; i < n; ++i) {
+      stats[i].iters = hst[i].iters;
+      stats[i].reason = hst[i].reason;
+      stats[i].rel = hst[i].rel;
+      stats[i].max_div = hst[i].maxdiv;
+    }
+  return SW_OK;
+}
+}  // namespace
+
+extern "C" size_t sw_project_batch_table_bytes(int n) {
+  return n > 0 ? batch_layout(n).total : 0;
+}
+
+extern "C" int sw_project_batch(const sw_project_job* jobs, int n, void* table,
+                                size_t table_bytes, sw_cg_stats* stats, void* stream) {
+  if (n <= 0 || jobs == nullptr || table == nullptr) {
+    set_error("sw_project_batch: bad arguments");
+    return SW_EINVAL;
+  }
+  if (table_bytes < batch_layout(n).total) {
+    set_error("sw_project_batch: table of %zu bytes, %zu required", table_bytes,
+              batch_layout(n).total);
+    return SW_EWORKSPACE;
+  }
+  const int dt = jobs[0].in_dtype;
+  for (int i = 0; i < n; ++i) {
+    const sw_project_job& j = jobs[i];
+    if (j.in_dtype != dt || j.nx <= 0 || j.ny <= 0 || j.nz <= 0 || j.out == nullptr ||
+        !(j.dX > 0 && j.dY > 0 && j.dZ > 0)) {
+      set_error("sw_project_batch: job %d is invalid (dtype, grid, output or spacing)", i);
+      return SW_EINVAL;
+    }
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  if (dt == SW_F32) return project_batch_t<float>(jobs, n, (char*)table, stats, s);
+  if (dt == SW_F64) return project_batch_t<double>(jobs, n, (char*)table, stats, s);
+  set_error("sw_project_batch: unknown dtype %d", dt);
+  return SW_EINVAL;
 }

@@ -21,6 +21,7 @@
 #include <math.h>
 
 #include <algorithm>
+#include <vector>
 
 #include "sw_common.cuh"
 #include "sw_step.cuh"
@@ -72,342 +73,414 @@ int encode_tmap_4d(CUtensorMap* map, CUtensorMapDataType dt, void* base, const u
 }
 
 // ---------------------------------------------------------------------------
-// shared pipeline helpers
+// pipeline helpers
 // ---------------------------------------------------------------------------
-struct Ring {
-  uint64_t* bars;   // NST mbarriers
-  uint32_t phases;  // parity bit per stage (uniform across the block)
+// mbarrier arrive (no transaction), used by consumer warps to free a stage.
+__device__ inline void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
+// Shared-memory header of the warp-specialised kernels (first 128 bytes).
+struct WsHeader {
+  uint64_t fullA[4], emptyA[4], fullB[4], emptyB[4];  // 128 bytes
 };
 
-// Wait for the next completion of `stage`; false when the bounded wait ran out.
-__device__ inline bool ring_wait(Ring& r, int stage) {
-  const uint32_t par = (r.phases >> stage) & 1u;
-  const bool ok = mbar_wait_bounded(&r.bars[stage], par);
-  r.phases ^= (1u << stage);
-  return ok;
+// A bounded wait that also gives up as soon as another thread has aborted.
+__device__ inline bool ws_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const long long t0 = clock64();
+  while (!mbar_try_wait(bar, parity)) {
+    if (*abort_flag) return false;
+    if (clock64() - t0 > 4000000000LL) {
+      *abort_flag = 1;
+      return false;
+    }
+  }
+  return true;
+}
+
+// Resolve the tile's instance and local step; false if the tile is idle.
+template <typename Inst, bool BATCH>
+__device__ inline bool resolve_tile(const Inst& one, const Inst* __restrict__ tab, int ninst,
+                                    int t, int it, const Inst*& in, int& local, int& lit) {
+  if (BATCH) {
+    int lo = 0, hi = ninst - 1;
+    while (lo < hi) {
+      int mid = (lo + hi + 1) >> 1;
+      if (tab[mid].tile_base <= t) lo = mid;
+      else hi = mid - 1;
+    }
+    in = &tab[lo];
+    local = t - in->tile_base;
+  } else {
+    in = &one;
+    local = t;
+  }
+  lit = it - in->it_begin;
+  return lit >= 0 && lit < in->n_steps;
 }
 
 // ---------------------------------------------------------------------------
-// mixed FP32 step, one tile
+// mixed FP32 step: warp-specialised TMA pipeline
 // ---------------------------------------------------------------------------
-__device__ inline void tile_f32(const TmaF32& in, int local, int lit, float* sm, Ring& ring,
-                                int* abort_flag) {
-  constexpr int W = TmaF32::W, H = TmaF32::H, NST = TmaF32::NST, PL = TmaF32::STAGE;
-  constexpr uint32_t BYTES = TmaF32::PLANE * sizeof(float);
-  static_assert((PL * sizeof(float)) % 128 == 0, "TMA destinations must be 128-byte aligned");
-  const Geom& g = in.g;
-  const TileCoord tc = tile_coord_t(g, in.ts, local, TmaF32::TZ, TmaF32::TY);
-  const CUtensorMap* tm = &in.tm[lit & 1];
-  const float* __restrict__ S = in.state[lit & 1];
-  float* __restrict__ D = in.state[(lit + 1) & 1];
-  const int pfirst = tc.x0 - 1, plast = tc.x1;
-  const int tid = threadIdx.x;
-  if (tid == 0) {
-    for (int k = 0; k < NST && pfirst + k <= plast; ++k) {
-      fence_proxy_async_smem();
-      mbar_arrive_expect_tx(&ring.bars[k], BYTES);
-      tma_load_4d(sm + k * PL, tm, &ring.bars[k], tc.z0 - 4, tc.y0 - 1, pfirst + k, 0);
-    }
-  }
-  const int ly = tid >> 5, lane = tid & 31;
-  const int y = tc.y0 + ly;
-  const bool yin = (y >= 1 && y <= g.ny - 2);
-  const int zc[2] = {tc.z0 + lane, tc.z0 + lane + 32};
-  const bool act[2] = {yin && zc[0] >= 1 && zc[0] <= g.nz - 2,
-                       yin && zc[1] >= 1 && zc[1] <= g.nz - 2};
-  const int j0 = in.term_off ? in.term_off[lit] : 0;
-  const int j1 = in.term_off ? in.term_off[lit + 1] : 0;
-  const bool snap = in.snap_stride > 0 && in.snaps != nullptr && ((lit + 1) % in.snap_stride) == 0;
-  const int slot = snap ? (lit + 1) / in.snap_stride - 1 : 0;
-  const long long nc = g.ncell;
-  for (int x = tc.x0; x < tc.x1; ++x) {
-    bool ok = true;
-    if (x == tc.x0) {
-      ok &= ring_wait(ring, 0);
-      ok &= ring_wait(ring, 1 % NST);
-    }
-    const int rel = x - pfirst;  // plane x-1 has rel-1
-    const int sp = (rel - 1) % NST, sc = rel % NST, sn = (rel + 1) % NST;
-    ok &= ring_wait(ring, sn);
-    if (__syncthreads_or(!ok)) {  // block-uniform decision
-      if (tid == 0) *abort_flag = 1;
-      __syncthreads();
-      return;
-    }
-    const float* Pp = sm + sp * PL;
-    const float* Pc = sm + sc * PL;
-    const float* Pn = sm + sn * PL;
-#pragma unroll
-    for (int k = 0; k < 2; ++k) {
-      if (!act[k]) continue;
-      const int z = zc[k];
-      const long long i = (long long)x * g.sxy + (long long)y * g.pz + z;
-      const float m = in.m[i];
-      const float e = in.e ? in.e[i] : 0.0f;
-      const int row = ly + 1, col = lane + 32 * k + 4;
-      bool bad = false;
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        const int o = (c * H + row) * W + col;
-        const int od = o + 3 * H * W;
-        const float u0 = Pc[o], d0 = Pc[od];
-        const float lu = ((Pn[o] + Pp[o]) - 2.0f * u0) * in.hx +
-                         ((Pc[o + W] + Pc[o - W]) - 2.0f * u0) * in.hy +
-                         ((Pc[o + 1] + Pc[o - 1]) - 2.0f * u0) * in.hz;
-        float inc = d0 + m * lu;
-        if (in.e) {
-          const float ld = ((Pn[od] + Pp[od]) - 2.0f * d0) * in.hx +
-                           ((Pc[od + W] + Pc[od - W]) - 2.0f * d0) * in.hy +
-                           ((Pc[od + 1] + Pc[od - 1]) - 2.0f * d0) * in.hz;
-          inc += e * ld;
-        }
-        for (int j = j0; j < j1; ++j)
-          inc += in.pat[((long long)in.term_pat[j] * 3 + c) * nc + i] * (float)in.term_scale[j];
-        if (in.use_damp) inc *= in.damp;
-        float unew, cnew;
-        if (in.kahan) {
-          const float cc = S[(6 + c) * nc + i];
-          const float yk = inc - cc;
-          unew = u0 + yk;
-          cnew = (unew - u0) - yk;
-        } else {
-          unew = u0 + inc;
-          cnew = 0.0f;
-        }
-        D[c * nc + i] = unew;
-        D[(3 + c) * nc + i] = inc;
-        D[(6 + c) * nc + i] = cnew;
-        bad |= !isfinite(unew);
-        if (snap)
-          in.snaps[((((long long)slot * g.nx + x) * g.ny + y) * g.nz + z) * 3 + c] = unew;
-      }
-      if (bad && in.flags) atomicOr(in.flags, 1);
-    }
-    __syncthreads();  // every thread is done with plane x-1's stage
-    if (tid == 0) {
-      const int p = x - 1 + NST;
-      if (p <= plast) {
-        fence_proxy_async_smem();
-        mbar_arrive_expect_tx(&ring.bars[sp], BYTES);
-        tma_load_4d(sm + sp * PL, tm, &ring.bars[sp], tc.z0 - 4, tc.y0 - 1, p, 0);
-      }
-    }
-  }
-  __syncthreads();
-}
-
-// ---------------------------------------------------------------------------
-// plain FP64 step, one tile
-// ---------------------------------------------------------------------------
-__device__ inline void tile_f64(const TmaF64& in, int local, int lit, double* sm, Ring& ring,
-                                int* abort_flag) {
-  constexpr int W = TmaF64::W, H = TmaF64::H, NST = TmaF64::NST, PL = TmaF64::STAGE;
-  constexpr int HALF = TmaF64::HALF;
-  constexpr uint32_t BYTES = TmaF64::PLANE * sizeof(double);
-  static_assert((HALF * sizeof(double)) % 128 == 0, "TMA destinations must be 128-byte aligned");
-  const Geom& g = in.g;
-  const TileCoord tc = tile_coord_t(g, in.ts, local, TmaF64::TZ, TmaF64::TY);
-  const CUtensorMap* tmp = &in.tm[lit % 3];
-  const CUtensorMap* tmc = &in.tm[(lit + 1) % 3];
-  double* __restrict__ un = in.state[(lit + 2) % 3];
-  const int pfirst = tc.x0 - 1, plast = tc.x1;
-  const int tid = threadIdx.x;
-  if (tid == 0) {
-    for (int k = 0; k < NST && pfirst + k <= plast; ++k) {
-      fence_proxy_async_smem();
-      mbar_arrive_expect_tx(&ring.bars[k], BYTES);
-      tma_load_4d(sm + k * PL, tmp, &ring.bars[k], tc.z0 - 2, tc.y0 - 1, pfirst + k, 0);
-      tma_load_4d(sm + k * PL + HALF, tmc, &ring.bars[k], tc.z0 - 2, tc.y0 - 1, pfirst + k, 0);
-    }
-  }
-  const int ly = tid >> 5, lane = tid & 31;
-  const int y = tc.y0 + ly, z = tc.z0 + lane;
-  const bool act = (y >= 1 && y <= g.ny - 2 && z >= 1 && z <= g.nz - 2);
-  const int j0 = in.term_off ? in.term_off[lit] : 0;
-  const int j1 = in.term_off ? in.term_off[lit + 1] : 0;
-  const bool snap = in.snap_stride > 0 && in.snaps != nullptr && ((lit + 1) % in.snap_stride) == 0;
-  const int slot = snap ? (lit + 1) / in.snap_stride - 1 : 0;
-  const long long nc = g.ncell;
-  const double ihx2 = in.ihx2, ihy2 = in.ihy2, ihz2 = in.ihz2, inv_dt = in.inv_dt;
-  for (int x = tc.x0; x < tc.x1; ++x) {
-    bool ok = true;
-    if (x == tc.x0) {
-      ok &= ring_wait(ring, 0);
-      ok &= ring_wait(ring, 1 % NST);
-    }
-    const int rel = x - pfirst;
-    const int sp = (rel - 1) % NST, sc = rel % NST, sn = (rel + 1) % NST;
-    ok &= ring_wait(ring, sn);
-    if (__syncthreads_or(!ok)) {  // block-uniform decision
-      if (tid == 0) *abort_flag = 1;
-      __syncthreads();
-      return;
-    }
-    if (act) {
-      const double* Pp = sm + sp * PL;
-      const double* Pc = sm + sc * PL;
-      const double* Pn = sm + sn * PL;
-      const long long i = (long long)x * g.sxy + (long long)y * g.pz + z;
-      const double m = in.m[i];
-      const double e = in.e ? in.e[i] : 0.0;
-      const double rinv = (j1 > j0) ? in.ir[i] : 0.0;
-      const int row = ly + 1, col = lane + 2;
-      bool bad = false;
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        const int op = (c * H + row) * W + col;  // u_prev component c
-        const int oc = op + HALF;                // u_curr component c
-        const double ucc = Pc[oc];
-        const double lap_u = ((Pn[oc] - 2.0 * ucc) + Pp[oc]) * ihx2 +
-                             ((Pc[oc + W] - 2.0 * ucc) + Pc[oc - W]) * ihy2 +
-                             ((Pc[oc + 1] - 2.0 * ucc) + Pc[oc - 1]) * ihz2;
-        double f = 0.0;
-        for (int j = j0; j < j1; ++j) {
-          const double fj = in.pat[((long long)in.term_pat[j] * 3 + c) * nc + i] * in.term_scale[j];
-          f = (j == j0) ? fj : f + fj;
-        }
-        double acc = m * lap_u + f * rinv;
-        const double upc = Pc[op];
-        if (in.e) {
-          const double vc = (ucc - upc) * inv_dt;
-          const double lap_v =
-              (((Pn[oc] - Pn[op]) * inv_dt - 2.0 * vc) + (Pp[oc] - Pp[op]) * inv_dt) * ihx2 +
-              (((Pc[oc + W] - Pc[op + W]) * inv_dt - 2.0 * vc) + (Pc[oc - W] - Pc[op - W]) * inv_dt) *
-                  ihy2 +
-              (((Pc[oc + 1] - Pc[op + 1]) * inv_dt - 2.0 * vc) + (Pc[oc - 1] - Pc[op - 1]) * inv_dt) *
-                  ihz2;
-          acc += e * lap_v;
-        }
-        double unew = (2.0 * ucc - upc) + in.dt2 * acc;
-        if (in.use_damp) unew = ucc + in.damp * (unew - ucc);
-        un[c * nc + i] = unew;
-        bad |= !isfinite(unew);
-        if (snap)
-          in.snaps[((((long long)slot * g.nx + x) * g.ny + y) * g.nz + z) * 3 + c] = unew;
-      }
-      if (bad && in.flags) atomicOr(in.flags, 1);
-    }
-    __syncthreads();
-    if (tid == 0) {
-      const int p = x - 1 + NST;
-      if (p <= plast) {
-        fence_proxy_async_smem();
-        mbar_arrive_expect_tx(&ring.bars[sp], BYTES);
-        tma_load_4d(sm + sp * PL, tmp, &ring.bars[sp], tc.z0 - 2, tc.y0 - 1, p, 0);
-        tma_load_4d(sm + sp * PL + HALF, tmc, &ring.bars[sp], tc.z0 - 2, tc.y0 - 1, p, 0);
-      }
-    }
-  }
-  __syncthreads();
-}
-
-// ---------------------------------------------------------------------------
-// kernels
-// ---------------------------------------------------------------------------
-template <typename Inst>
-__device__ inline int find_tma_inst(const Inst* __restrict__ tab, int ninst, int t) {
-  int lo = 0, hi = ninst - 1;
-  while (lo < hi) {
-    int mid = (lo + hi + 1) >> 1;
-    if (tab[mid].tile_base <= t) lo = mid;
-    else hi = mid - 1;
-  }
-  return lo;
-}
-
-// Drain: wait (bounded) until every stage with an outstanding load has
-// completed, so no copy is still writing this CTA's shared memory.
-template <int NST>
-__device__ inline void ring_drain(Ring& ring, int outstanding_mask) {
-  if (threadIdx.x != 0) return;
-  for (int s = 0; s < NST; ++s)
-    if (outstanding_mask & (1 << s)) mbar_wait_bounded(&ring.bars[s], (ring.phases >> s) & 1u);
-}
-
 template <bool BATCH>
-__global__ void __launch_bounds__(256, 3)
+__global__ void __launch_bounds__(TmaF32::THREADS, 2)
     step_f32_tma(const __grid_constant__ TmaF32 one, const TmaF32* __restrict__ tab, int ninst,
                  int ntiles, int it) {
+  constexpr int NA = TmaF32::NA, NB = TmaF32::NB, W = TmaF32::W, H = TmaF32::H;
+  constexpr int TZ = TmaF32::TZ, TY = TmaF32::TY;
+  constexpr int AF = TmaF32::A_STAGE / 4, BF = TmaF32::B_STAGE / 4;  // floats per stage
+  constexpr int CF = round128(TmaF32::C_BYTES) / 4;                  // offset of coefficients
   extern __shared__ unsigned char smem_raw[];
-  // 128-byte aligned header (mbarriers, abort flag) followed by the stages
   unsigned char* base = smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u);
-  uint64_t* bars = reinterpret_cast<uint64_t*>(base);
-  int& abort_flag = *reinterpret_cast<int*>(base + 64);
-  float* sm = reinterpret_cast<float*>(base + 128);
-  if ((smem_addr(sm) & 127u) != 0u) {  // never issue a TMA to a misaligned destination
+  WsHeader* hd = reinterpret_cast<WsHeader*>(base);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(base + 128);
+  float* ringA = reinterpret_cast<float*>(base + 256);
+  float* ringB = ringA + NA * AF;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if ((smem_addr(ringA) & 127u) != 0u) {  // never issue a TMA to a misaligned destination
     int* fl = BATCH ? (ninst > 0 ? tab[0].flags : nullptr) : one.flags;
     if (threadIdx.x == 0 && fl) atomicOr(fl, 4);
     return;
   }
   if (threadIdx.x == 0) {
-    for (int s = 0; s < TmaF32::NST; ++s) mbar_init(&bars[s], 1);
+    for (int s = 0; s < NA; ++s) {
+      mbar_init(&hd->fullA[s], 1);
+      mbar_init(&hd->emptyA[s], TmaF32::CONSUMER_WARPS);
+    }
+    for (int s = 0; s < NB; ++s) {
+      mbar_init(&hd->fullB[s], 1);
+      mbar_init(&hd->emptyB[s], TmaF32::CONSUMER_WARPS);
+    }
+    *abort_flag = 0;
     mbar_fence_init();
-    abort_flag = 0;
   }
   __syncthreads();
-  Ring ring{bars, 0u};
-  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-    const TmaF32* in;
-    int local;
-    if (BATCH) {
-      const int ii = find_tma_inst(tab, ninst, t);
-      in = &tab[ii];
-      local = t - in->tile_base;
-    } else {
-      in = &one;
-      local = t;
+
+  if (warp == TmaF32::CONSUMER_WARPS) {
+    // ------------------------------- producer -----------------------------
+    if (lane == 0) {
+      uint32_t pa = 0, pb = 0;  // loads issued into ring A / ring B
+      for (int t = blockIdx.x; t < ntiles && !*abort_flag; t += gridDim.x) {
+        const TmaF32* in;
+        int local, lit;
+        if (!resolve_tile<TmaF32, BATCH>(one, tab, ninst, t, it, in, local, lit)) continue;
+        const TileCoord tc = tile_coord_t(in->g, in->ts, local, TZ, TY);
+        const CUtensorMap* tma = &in->tm[lit & 1];
+        const CUtensorMap* tmc = &in->tmc[lit & 1];
+        const uint32_t bbytes = (in->kahan ? TmaF32::C_BYTES : 0) + TZ * TY * 4 * in->ncoef;
+        for (int p = tc.x0 - 1; p <= tc.x1 && !*abort_flag; ++p) {
+          const int sa = pa % NA;
+          if (!ws_wait(&hd->emptyA[sa], ((pa / NA) & 1u) ^ 1u, abort_flag)) break;
+          fence_proxy_async_smem();
+          mbar_arrive_expect_tx(&hd->fullA[sa], TmaF32::A_BYTES);
+          tma_load_4d(ringA + sa * AF, tma, &hd->fullA[sa], tc.z0 - 4, tc.y0 - 1, p, 0);
+          ++pa;
+          if (p >= tc.x0 && p < tc.x1) {
+            const int sb = pb % NB;
+            if (!ws_wait(&hd->emptyB[sb], ((pb / NB) & 1u) ^ 1u, abort_flag)) break;
+            fence_proxy_async_smem();
+            mbar_arrive_expect_tx(&hd->fullB[sb], bbytes);
+            if (in->kahan) tma_load_4d(ringB + sb * BF, tmc, &hd->fullB[sb], tc.z0, tc.y0, p, 6);
+            tma_load_4d(ringB + sb * BF + CF, &in->tmm, &hd->fullB[sb], tc.z0, tc.y0, p, 0);
+            ++pb;
+          }
+        }
+      }
     }
-    const int lit = it - in->it_begin;
-    if (lit < 0 || lit >= in->n_steps) continue;
-    tile_f32(*in, local, lit, sm, ring, &abort_flag);
-    if (abort_flag) {
-      if (threadIdx.x == 0 && in->flags) atomicOr(in->flags, 2);
-      ring_drain<TmaF32::NST>(ring, (1 << TmaF32::NST) - 1);
-      return;
+  } else {
+    // ------------------------------- consumers ----------------------------
+    const int ly = warp;
+    uint32_t ca = 0, cb = 0;  // planes consumed from ring A / ring B
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+      const TmaF32* in;
+      int local, lit;
+      if (!resolve_tile<TmaF32, BATCH>(one, tab, ninst, t, it, in, local, lit)) continue;
+      const Geom& g = in->g;
+      const TileCoord tc = tile_coord_t(g, in->ts, local, TZ, TY);
+      const float* __restrict__ S = in->state[lit & 1];
+      float* __restrict__ D = in->state[(lit + 1) & 1];
+      const int y = tc.y0 + ly;
+      const bool yin = (y >= 1 && y <= g.ny - 2);
+      const int z0 = tc.z0 + lane, z1 = z0 + 32;
+      const bool act0 = yin && z0 >= 1 && z0 <= g.nz - 2;
+      const bool act1 = yin && z1 >= 1 && z1 <= g.nz - 2;
+      const int j0 = in->term_off ? in->term_off[lit] : 0;
+      const int j1 = in->term_off ? in->term_off[lit + 1] : 0;
+      const bool snap =
+          in->snap_stride > 0 && in->snaps != nullptr && ((lit + 1) % in->snap_stride) == 0;
+      const int slot = snap ? (lit + 1) / in->snap_stride - 1 : 0;
+      const long long nc = g.ncell;
+      const bool visc = in->ncoef > 1;
+      const float hx = in->hx, hy = in->hy, hz = in->hz;
+      int s_prev, s_cur, s_next;  // ring A stages of planes x-1, x, x+1
+      bool ok = true;
+      s_prev = ca % NA;
+      ok &= ws_wait(&hd->fullA[s_prev], (ca / NA) & 1u, abort_flag);
+      ++ca;
+      s_cur = ca % NA;
+      ok &= ws_wait(&hd->fullA[s_cur], (ca / NA) & 1u, abort_flag);
+      ++ca;
+      long long irow = (long long)tc.x0 * g.sxy + (long long)y * g.pz;
+      for (int x = tc.x0; x < tc.x1 && ok; ++x, irow += g.sxy) {
+        s_next = ca % NA;
+        ok &= ws_wait(&hd->fullA[s_next], (ca / NA) & 1u, abort_flag);
+        ++ca;
+        const int sb = cb % NB;
+        ok &= ws_wait(&hd->fullB[sb], (cb / NB) & 1u, abort_flag);
+        ++cb;
+        if (!ok) break;
+        const float* Pp = ringA + s_prev * AF;
+        const float* Pc = ringA + s_cur * AF;
+        const float* Pn = ringA + s_next * AF;
+        const float* Bc = ringB + sb * BF;
+        const float* Bm = Bc + CF;
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+          if (!(k == 0 ? act0 : act1)) continue;
+          const int lz = lane + 32 * k;
+          const int z = tc.z0 + lz;
+          const long long i = irow + z;
+          const float m = Bm[ly * TZ + lz];
+          const float e = visc ? Bm[(TY + ly) * TZ + lz] : 0.0f;
+          bool bad = false;
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            const int o = (c * H + ly + 1) * W + lz + 4;
+            const int od = o + 3 * H * W;
+            const float u0 = Pc[o], d0 = Pc[od];
+            const float lu = ((Pn[o] + Pp[o]) - 2.0f * u0) * hx +
+                             ((Pc[o + W] + Pc[o - W]) - 2.0f * u0) * hy +
+                             ((Pc[o + 1] + Pc[o - 1]) - 2.0f * u0) * hz;
+            float inc = d0 + m * lu;
+            if (visc) {
+              const float ld = ((Pn[od] + Pp[od]) - 2.0f * d0) * hx +
+                               ((Pc[od + W] + Pc[od - W]) - 2.0f * d0) * hy +
+                               ((Pc[od + 1] + Pc[od - 1]) - 2.0f * d0) * hz;
+              inc += e * ld;
+            }
+            for (int j = j0; j < j1; ++j)
+              inc += in->pat[((long long)in->term_pat[j] * 3 + c) * nc + i] *
+                     (float)in->term_scale[j];
+            if (in->use_damp) inc *= in->damp;
+            float unew, cnew;
+            if (in->kahan) {
+              const float cc = Bc[(c * TY + ly) * TZ + lz];
+              const float yk = inc - cc;
+              unew = u0 + yk;
+              cnew = (unew - u0) - yk;
+            } else {
+              unew = u0 + inc;
+              cnew = 0.0f;
+            }
+            D[c * nc + i] = unew;
+            D[(3 + c) * nc + i] = inc;
+            D[(6 + c) * nc + i] = cnew;
+            bad |= !isfinite(unew);
+            if (snap)
+              in->snaps[((((long long)slot * g.nx + x) * g.ny + y) * g.nz + z) * 3 + c] = unew;
+          }
+          if (bad && in->flags) atomicOr(in->flags, 1);
+        }
+        (void)S;
+        __syncwarp();
+        if (lane == 0) {
+          mbar_arrive(&hd->emptyA[s_prev]);  // plane x-1 is done
+          mbar_arrive(&hd->emptyB[sb]);
+        }
+        s_prev = s_cur;
+        s_cur = s_next;
+      }
+      if (!ok) break;
+      __syncwarp();
+      if (lane == 0) {  // planes x1-1 and x1 are done too
+        mbar_arrive(&hd->emptyA[s_prev]);
+        mbar_arrive(&hd->emptyA[s_cur]);
+      }
+    }
+  }
+  __syncthreads();
+  if (*abort_flag && threadIdx.x == 0) {
+    int* fl = BATCH ? (ninst > 0 ? tab[0].flags : nullptr) : one.flags;
+    if (fl) atomicOr(fl, 2);
+    // bounded drain: let any copy still in flight land before the CTA exits
+    const long long t0 = clock64();
+    while (clock64() - t0 < 200000000LL) {
     }
   }
 }
 
+// ---------------------------------------------------------------------------
+// plain FP64 step: warp-specialised TMA pipeline
+// ---------------------------------------------------------------------------
 template <bool BATCH>
-__global__ void __launch_bounds__(256, 3)
+__global__ void __launch_bounds__(TmaF64::THREADS, 2)
     step_f64_tma(const __grid_constant__ TmaF64 one, const TmaF64* __restrict__ tab, int ninst,
                  int ntiles, int it) {
+  constexpr int NA = TmaF64::NA, NB = TmaF64::NB, W = TmaF64::W, H = TmaF64::H;
+  constexpr int TZ = TmaF64::TZ, TY = TmaF64::TY;
+  constexpr int AD = TmaF64::A_STAGE / 8, BD = TmaF64::B_STAGE / 8, HALF = TmaF64::HALF / 8;
   extern __shared__ unsigned char smem_raw[];
-  // 128-byte aligned header (mbarriers, abort flag) followed by the stages
   unsigned char* base = smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u);
-  uint64_t* bars = reinterpret_cast<uint64_t*>(base);
-  int& abort_flag = *reinterpret_cast<int*>(base + 64);
-  double* sm = reinterpret_cast<double*>(base + 128);
-  if ((smem_addr(sm) & 127u) != 0u) {  // never issue a TMA to a misaligned destination
+  WsHeader* hd = reinterpret_cast<WsHeader*>(base);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(base + 128);
+  double* ringA = reinterpret_cast<double*>(base + 256);
+  double* ringB = ringA + NA * AD;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if ((smem_addr(ringA) & 127u) != 0u) {
     int* fl = BATCH ? (ninst > 0 ? tab[0].flags : nullptr) : one.flags;
     if (threadIdx.x == 0 && fl) atomicOr(fl, 4);
     return;
   }
   if (threadIdx.x == 0) {
-    for (int s = 0; s < TmaF64::NST; ++s) mbar_init(&bars[s], 1);
+    for (int s = 0; s < NA; ++s) {
+      mbar_init(&hd->fullA[s], 1);
+      mbar_init(&hd->emptyA[s], TmaF64::CONSUMER_WARPS);
+    }
+    for (int s = 0; s < NB; ++s) {
+      mbar_init(&hd->fullB[s], 1);
+      mbar_init(&hd->emptyB[s], TmaF64::CONSUMER_WARPS);
+    }
+    *abort_flag = 0;
     mbar_fence_init();
-    abort_flag = 0;
   }
   __syncthreads();
-  Ring ring{bars, 0u};
-  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-    const TmaF64* in;
-    int local;
-    if (BATCH) {
-      const int ii = find_tma_inst(tab, ninst, t);
-      in = &tab[ii];
-      local = t - in->tile_base;
-    } else {
-      in = &one;
-      local = t;
+
+  if (warp == TmaF64::CONSUMER_WARPS) {
+    if (lane == 0) {
+      uint32_t pa = 0, pb = 0;
+      for (int t = blockIdx.x; t < ntiles && !*abort_flag; t += gridDim.x) {
+        const TmaF64* in;
+        int local, lit;
+        if (!resolve_tile<TmaF64, BATCH>(one, tab, ninst, t, it, in, local, lit)) continue;
+        const TileCoord tc = tile_coord_t(in->g, in->ts, local, TZ, TY);
+        const CUtensorMap* tmp = &in->tm[lit % 3];
+        const CUtensorMap* tmc = &in->tm[(lit + 1) % 3];
+        const uint32_t bbytes = TZ * TY * 8 * in->ncoef;
+        for (int p = tc.x0 - 1; p <= tc.x1 && !*abort_flag; ++p) {
+          const int sa = pa % NA;
+          if (!ws_wait(&hd->emptyA[sa], ((pa / NA) & 1u) ^ 1u, abort_flag)) break;
+          fence_proxy_async_smem();
+          mbar_arrive_expect_tx(&hd->fullA[sa], 2 * TmaF64::BOX_BYTES);
+          tma_load_4d(ringA + sa * AD, tmp, &hd->fullA[sa], tc.z0 - 2, tc.y0 - 1, p, 0);
+          tma_load_4d(ringA + sa * AD + HALF, tmc, &hd->fullA[sa], tc.z0 - 2, tc.y0 - 1, p, 0);
+          ++pa;
+          if (p >= tc.x0 && p < tc.x1) {
+            const int sb = pb % NB;
+            if (!ws_wait(&hd->emptyB[sb], ((pb / NB) & 1u) ^ 1u, abort_flag)) break;
+            fence_proxy_async_smem();
+            mbar_arrive_expect_tx(&hd->fullB[sb], bbytes);
+            tma_load_4d(ringB + sb * BD, &in->tmm, &hd->fullB[sb], tc.z0, tc.y0, p, 0);
+            ++pb;
+          }
+        }
+      }
     }
-    const int lit = it - in->it_begin;
-    if (lit < 0 || lit >= in->n_steps) continue;
-    tile_f64(*in, local, lit, sm, ring, &abort_flag);
-    if (abort_flag) {
-      if (threadIdx.x == 0 && in->flags) atomicOr(in->flags, 2);
-      ring_drain<TmaF64::NST>(ring, (1 << TmaF64::NST) - 1);
-      return;
+  } else {
+    const int ly = warp;
+    uint32_t ca = 0, cb = 0;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+      const TmaF64* in;
+      int local, lit;
+      if (!resolve_tile<TmaF64, BATCH>(one, tab, ninst, t, it, in, local, lit)) continue;
+      const Geom& g = in->g;
+      const TileCoord tc = tile_coord_t(g, in->ts, local, TZ, TY);
+      double* __restrict__ un = in->state[(lit + 2) % 3];
+      const int y = tc.y0 + ly, z = tc.z0 + lane;
+      const bool act = (y >= 1 && y <= g.ny - 2 && z >= 1 && z <= g.nz - 2);
+      const int j0 = in->term_off ? in->term_off[lit] : 0;
+      const int j1 = in->term_off ? in->term_off[lit + 1] : 0;
+      const bool snap =
+          in->snap_stride > 0 && in->snaps != nullptr && ((lit + 1) % in->snap_stride) == 0;
+      const int slot = snap ? (lit + 1) / in->snap_stride - 1 : 0;
+      const long long nc = g.ncell;
+      const bool visc = in->ncoef > 1;
+      const double ihx2 = in->ihx2, ihy2 = in->ihy2, ihz2 = in->ihz2, inv_dt = in->inv_dt;
+      int s_prev, s_cur, s_next;
+      bool ok = true;
+      s_prev = ca % NA;
+      ok &= ws_wait(&hd->fullA[s_prev], (ca / NA) & 1u, abort_flag);
+      ++ca;
+      s_cur = ca % NA;
+      ok &= ws_wait(&hd->fullA[s_cur], (ca / NA) & 1u, abort_flag);
+      ++ca;
+      long long i = (long long)tc.x0 * g.sxy + (long long)y * g.pz + z;
+      for (int x = tc.x0; x < tc.x1 && ok; ++x, i += g.sxy) {
+        s_next = ca % NA;
+        ok &= ws_wait(&hd->fullA[s_next], (ca / NA) & 1u, abort_flag);
+        ++ca;
+        const int sb = cb % NB;
+        ok &= ws_wait(&hd->fullB[sb], (cb / NB) & 1u, abort_flag);
+        ++cb;
+        if (!ok) break;
+        if (act) {
+          const double* Pp = ringA + s_prev * AD;
+          const double* Pc = ringA + s_cur * AD;
+          const double* Pn = ringA + s_next * AD;
+          const double* Bm = ringB + sb * BD;
+          const double m = Bm[ly * TZ + lane];
+          const double e = visc ? Bm[(TY + ly) * TZ + lane] : 0.0;
+          const double rinv = (j1 > j0) ? in->ir[i] : 0.0;
+          bool bad = false;
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            const int op = (c * H + ly + 1) * W + lane + 2;  // u_prev component c
+            const int oc = op + HALF;                        // u_curr component c
+            const double ucc = Pc[oc];
+            const double lap_u = ((Pn[oc] - 2.0 * ucc) + Pp[oc]) * ihx2 +
+                                 ((Pc[oc + W] - 2.0 * ucc) + Pc[oc - W]) * ihy2 +
+                                 ((Pc[oc + 1] - 2.0 * ucc) + Pc[oc - 1]) * ihz2;
+            double f = 0.0;
+            for (int j = j0; j < j1; ++j) {
+              const double fj =
+                  in->pat[((long long)in->term_pat[j] * 3 + c) * nc + i] * in->term_scale[j];
+              f = (j == j0) ? fj : f + fj;
+            }
+            double acc = m * lap_u + f * rinv;
+            const double upc = Pc[op];
+            if (visc) {
+              const double vc = (ucc - upc) * inv_dt;
+              const double lap_v =
+                  (((Pn[oc] - Pn[op]) * inv_dt - 2.0 * vc) + (Pp[oc] - Pp[op]) * inv_dt) * ihx2 +
+                  (((Pc[oc + W] - Pc[op + W]) * inv_dt - 2.0 * vc) +
+                   (Pc[oc - W] - Pc[op - W]) * inv_dt) *
+                      ihy2 +
+                  (((Pc[oc + 1] - Pc[op + 1]) * inv_dt - 2.0 * vc) +
+                   (Pc[oc - 1] - Pc[op - 1]) * inv_dt) *
+                      ihz2;
+              acc += e * lap_v;
+            }
+            double unew = (2.0 * ucc - upc) + in->dt2 * acc;
+            if (in->use_damp) unew = ucc + in->damp * (unew - ucc);
+            un[c * nc + i] = unew;
+            bad |= !isfinite(unew);
+            if (snap)
+              in->snaps[((((long long)slot * g.nx + x) * g.ny + y) * g.nz + z) * 3 + c] = unew;
+          }
+          if (bad && in->flags) atomicOr(in->flags, 1);
+        }
+        __syncwarp();
+        if (lane == 0) {
+          mbar_arrive(&hd->emptyA[s_prev]);
+          mbar_arrive(&hd->emptyB[sb]);
+        }
+        s_prev = s_cur;
+        s_cur = s_next;
+      }
+      if (!ok) break;
+      __syncwarp();
+      if (lane == 0) {
+        mbar_arrive(&hd->emptyA[s_prev]);
+        mbar_arrive(&hd->emptyA[s_cur]);
+      }
+    }
+  }
+  __syncthreads();
+  if (*abort_flag && threadIdx.x == 0) {
+    int* fl = BATCH ? (ninst > 0 ? tab[0].flags : nullptr) : one.flags;
+    if (fl) atomicOr(fl, 2);
+    const long long t0 = clock64();
+    while (clock64() - t0 < 200000000LL) {
     }
   }
 }
@@ -415,10 +488,11 @@ __global__ void __launch_bounds__(256, 3)
 // ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
-// dynamic shared memory: alignment slack + header + stages
+// dynamic shared memory: alignment slack + header + ring A + ring B
 size_t tma_smem_bytes(int precision) {
-  return precision == SW_PLAIN_F64 ? 256 + (size_t)TmaF64::NST * TmaF64::STAGE * sizeof(double)
-                                   : 256 + (size_t)TmaF32::NST * TmaF32::STAGE * sizeof(float);
+  if (precision == SW_PLAIN_F64)
+    return 128 + 256 + (size_t)TmaF64::NA * TmaF64::A_STAGE + (size_t)TmaF64::NB * TmaF64::B_STAGE;
+  return 128 + 256 + (size_t)TmaF32::NA * TmaF32::A_STAGE + (size_t)TmaF32::NB * TmaF32::B_STAGE;
 }
 
 static int set_smem_attr(int precision) {
@@ -445,33 +519,70 @@ static int set_smem_attr(int precision) {
   return SW_OK;
 }
 
-int tma_xchunk(const Geom& g, int tz, int ty, long long want_tiles) {
-  long long ntz = (g.nz + tz - 1) / tz, nty = (g.ny + ty - 1) / ty;
-  long long nxi = g.nx > 2 ? g.nx - 2 : 0;
+// Planes per x chunk for a launch over one grid with `slots` resident CTAs:
+// minimise (waves of tiles) x (planes a CTA loads per tile, including the
+// two halo planes every chunk starts with).
+int tma_xchunk(const Geom& g, int tz, int ty, long long slots) {
+  const long long ntz = (g.nz + tz - 1) / tz, nty = (g.ny + ty - 1) / ty;
+  const long long nxi = g.nx > 2 ? g.nx - 2 : 0;
   if (nxi == 0) return 1;
-  long long cols = ntz * nty;
-  long long nchunks = std::max(1LL, (want_tiles + cols - 1) / cols);
-  long long xc = std::max(8LL, (nxi + nchunks - 1) / nchunks);
-  return (int)std::min(xc, nxi);
+  const long long cols = ntz * nty;
+  long long best_nc = 1, best_cost = -1;
+  for (long long nc = 1; nc <= nxi; ++nc) {
+    const long long xc = (nxi + nc - 1) / nc;
+    const long long nchunks = (nxi + xc - 1) / xc;
+    const long long waves = (cols * nchunks + slots - 1) / slots;
+    const long long cost = waves * (xc + 2);
+    if (best_cost < 0 || cost < best_cost) {
+      best_cost = cost;
+      best_nc = nc;
+    }
+  }
+  return (int)((nxi + best_nc - 1) / best_nc);
+}
+
+// Material coefficients must be one allocation: component 0 = mu term,
+// component 1 (optional) = eta term, ncell elements apart.
+static int coef_components(const StepArgs& a, size_t es, int* ncoef) {
+  if (a.coef_e == nullptr) {
+    *ncoef = 1;
+    return SW_OK;
+  }
+  if ((const char*)a.coef_e != (const char*)a.coef_m + a.g.ncell * es) {
+    set_error("TMA step kernels need coef_e == coef_m + ncell (one 2-component allocation)");
+    return SW_EINVAL;
+  }
+  *ncoef = 2;
+  return SW_OK;
 }
 
 int make_tma_f32(const StepArgs& a, int xchunk, TmaF32* t) {
   *t = TmaF32{};
   t->g = a.g;
-  const int xc = xchunk > 0 ? xchunk : tma_xchunk(a.g, TmaF32::TZ, TmaF32::TY, 3 * 148);
+  const int xc = xchunk > 0 ? xchunk : tma_xchunk(a.g, TmaF32::TZ, TmaF32::TY, 2 * 148);
   t->ts = make_tiles_t(a.g, xc, TmaF32::TZ, TmaF32::TY);
+  int rc = coef_components(a, 4, &t->ncoef);
+  if (rc != SW_OK) return rc;
   const uint64_t dims[4] = {(uint64_t)a.g.pz, (uint64_t)a.g.ny, (uint64_t)a.g.nx, 9};
   const uint64_t strides[3] = {(uint64_t)a.g.pz * 4, (uint64_t)a.g.sxy * 4,
                                (uint64_t)a.g.ncell * 4};
-  const uint32_t box[4] = {TmaF32::W, TmaF32::H, 1, 6};
+  const uint32_t box_halo[4] = {TmaF32::W, TmaF32::H, 1, 6};
+  const uint32_t box_pt[4] = {TmaF32::TZ, TmaF32::TY, 1, 3};
   for (int b = 0; b < 2; ++b) {
     t->state[b] = (float*)a.state[b];
-    int rc = encode_tmap_4d(&t->tm[b], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, a.state[b], dims, strides,
-                            box);
+    rc = encode_tmap_4d(&t->tm[b], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, a.state[b], dims, strides,
+                        box_halo);
+    if (rc == SW_OK)
+      rc = encode_tmap_4d(&t->tmc[b], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, a.state[b], dims, strides,
+                          box_pt);
     if (rc != SW_OK) return rc;
   }
-  t->m = (const float*)a.coef_m;
-  t->e = (const float*)a.coef_e;
+  const uint64_t mdims[4] = {(uint64_t)a.g.pz, (uint64_t)a.g.ny, (uint64_t)a.g.nx,
+                             (uint64_t)t->ncoef};
+  const uint32_t box_m[4] = {TmaF32::TZ, TmaF32::TY, 1, (uint32_t)t->ncoef};
+  rc = encode_tmap_4d(&t->tmm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, (void*)a.coef_m, mdims, strides,
+                      box_m);
+  if (rc != SW_OK) return rc;
   t->pat = (const float*)a.patterns;
   t->term_off = a.term_off;
   t->term_pat = a.term_pat;
@@ -494,20 +605,26 @@ int make_tma_f32(const StepArgs& a, int xchunk, TmaF32* t) {
 int make_tma_f64(const StepArgs& a, int xchunk, TmaF64* t) {
   *t = TmaF64{};
   t->g = a.g;
-  const int xc = xchunk > 0 ? xchunk : tma_xchunk(a.g, TmaF64::TZ, TmaF64::TY, 3 * 148);
+  const int xc = xchunk > 0 ? xchunk : tma_xchunk(a.g, TmaF64::TZ, TmaF64::TY, 2 * 148);
   t->ts = make_tiles_t(a.g, xc, TmaF64::TZ, TmaF64::TY);
+  int rc = coef_components(a, 8, &t->ncoef);
+  if (rc != SW_OK) return rc;
   const uint64_t dims[4] = {(uint64_t)a.g.pz, (uint64_t)a.g.ny, (uint64_t)a.g.nx, 3};
   const uint64_t strides[3] = {(uint64_t)a.g.pz * 8, (uint64_t)a.g.sxy * 8,
                                (uint64_t)a.g.ncell * 8};
   const uint32_t box[4] = {TmaF64::W, TmaF64::H, 1, 3};
   for (int b = 0; b < 3; ++b) {
     t->state[b] = (double*)a.state[b];
-    int rc = encode_tmap_4d(&t->tm[b], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, a.state[b], dims, strides,
-                            box);
+    rc = encode_tmap_4d(&t->tm[b], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, a.state[b], dims, strides,
+                        box);
     if (rc != SW_OK) return rc;
   }
-  t->m = (const double*)a.coef_m;
-  t->e = (const double*)a.coef_e;
+  const uint64_t mdims[4] = {(uint64_t)a.g.pz, (uint64_t)a.g.ny, (uint64_t)a.g.nx,
+                             (uint64_t)t->ncoef};
+  const uint32_t box_m[4] = {TmaF64::TZ, TmaF64::TY, 1, (uint32_t)t->ncoef};
+  rc = encode_tmap_4d(&t->tmm, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, (void*)a.coef_m, mdims, strides,
+                      box_m);
+  if (rc != SW_OK) return rc;
   t->ir = (const double*)a.inv_rho;
   t->pat = (const double*)a.patterns;
   t->term_off = a.term_off;
@@ -538,17 +655,17 @@ int launch_steps_tma(const StepArgs& a, int xchunk, int it0, int nsteps, cudaStr
     rc = make_tma_f64(a, xchunk, &t);
     if (rc != SW_OK) return rc;
     if (t.ts.count == 0) return SW_OK;
-    const int grid = std::min(t.ts.count, 148 * 3);
+    const int grid = std::min(t.ts.count, 148 * 2);
     for (int it = it0; it < it0 + nsteps; ++it)
-      step_f64_tma<false><<<grid, 256, smem, s>>>(t, nullptr, 1, t.ts.count, it);
+      step_f64_tma<false><<<grid, TmaF64::THREADS, smem, s>>>(t, nullptr, 1, t.ts.count, it);
   } else {
     TmaF32 t;
     rc = make_tma_f32(a, xchunk, &t);
     if (rc != SW_OK) return rc;
     if (t.ts.count == 0) return SW_OK;
-    const int grid = std::min(t.ts.count, 148 * 3);
+    const int grid = std::min(t.ts.count, 148 * 2);
     for (int it = it0; it < it0 + nsteps; ++it)
-      step_f32_tma<false><<<grid, 256, smem, s>>>(t, nullptr, 1, t.ts.count, it);
+      step_f32_tma<false><<<grid, TmaF32::THREADS, smem, s>>>(t, nullptr, 1, t.ts.count, it);
   }
   count_launches((unsigned long long)nsteps);
   SW_CHECK_LAUNCH("step (tma)");
@@ -561,13 +678,15 @@ int launch_steps_tma_batch(int precision, const void* d_tab, int ninst, int ntil
   if (rc != SW_OK) return rc;
   if (ntiles == 0) return SW_OK;
   const size_t smem = tma_smem_bytes(precision);
-  const int grid = std::min(ntiles, 148 * 3);
+  const int grid = std::min(ntiles, 148 * 2);
   if (precision == SW_PLAIN_F64) {
     TmaF64 dummy{};
-    step_f64_tma<true><<<grid, 256, smem, s>>>(dummy, (const TmaF64*)d_tab, ninst, ntiles, it);
+    step_f64_tma<true><<<grid, TmaF64::THREADS, smem, s>>>(dummy, (const TmaF64*)d_tab, ninst,
+                                                          ntiles, it);
   } else {
     TmaF32 dummy{};
-    step_f32_tma<true><<<grid, 256, smem, s>>>(dummy, (const TmaF32*)d_tab, ninst, ntiles, it);
+    step_f32_tma<true><<<grid, TmaF32::THREADS, smem, s>>>(dummy, (const TmaF32*)d_tab, ninst,
+                                                          ntiles, it);
   }
   count_launches(1);
   SW_CHECK_LAUNCH("step (tma, batch)");
@@ -575,3 +694,131 @@ int launch_steps_tma_batch(int precision, const void* d_tab, int ninst, int ntil
 }
 
 }  // namespace sw
+
+// ---------------------------------------------------------------------------
+// batched time loop: one launch per global step over every active solve
+// ---------------------------------------------------------------------------
+namespace sw {
+namespace {
+
+template <typename Inst>
+int build_batch(const sw_fdtd_desc* descs, const int32_t* begins, int n, int it,
+                std::vector<Inst>& tab, int* ntiles);
+
+template <>
+int build_batch<TmaF32>(const sw_fdtd_desc* descs, const int32_t* begins, int n, int it,
+                        std::vector<TmaF32>& tab, int* ntiles) {
+  tab.clear();
+  int nt = 0;
+  for (int i = 0; i < n; ++i) {
+    const int lit = it - (begins ? begins[i] : 0);
+    if (lit < 0 || lit >= descs[i].n_steps) continue;
+    StepArgs a;
+    int rc = make_step_args(&descs[i], &a);
+    if (rc != SW_OK) return rc;
+    TmaF32 t;
+    rc = make_tma_f32(a, descs[i].xchunk > 0 ? descs[i].xchunk : 16, &t);
+    if (rc != SW_OK) return rc;
+    t.it_begin = begins ? begins[i] : 0;
+    t.tile_base = nt;
+    nt += t.ts.count;
+    tab.push_back(t);
+  }
+  *ntiles = nt;
+  return SW_OK;
+}
+
+template <>
+int build_batch<TmaF64>(const sw_fdtd_desc* descs, const int32_t* begins, int n, int it,
+                        std::vector<TmaF64>& tab, int* ntiles) {
+  tab.clear();
+  int nt = 0;
+  for (int i = 0; i < n; ++i) {
+    const int lit = it - (begins ? begins[i] : 0);
+    if (lit < 0 || lit >= descs[i].n_steps) continue;
+    StepArgs a;
+    int rc = make_step_args(&descs[i], &a);
+    if (rc != SW_OK) return rc;
+    TmaF64 t;
+    rc = make_tma_f64(a, descs[i].xchunk > 0 ? descs[i].xchunk : 16, &t);
+    if (rc != SW_OK) return rc;
+    t.it_begin = begins ? begins[i] : 0;
+    t.tile_base = nt;
+    nt += t.ts.count;
+    tab.push_back(t);
+  }
+  *ntiles = nt;
+  return SW_OK;
+}
+
+template <typename Inst>
+int batch_steps(int precision, const sw_fdtd_desc* descs, const int32_t* begins, int n, int it0,
+                int nsteps, void* table, cudaStream_t s) {
+  std::vector<Inst> tab;
+  std::vector<int> active(n, -1);
+  int ntiles = 0;
+  bool have = false;
+  for (int it = it0; it < it0 + nsteps; ++it) {
+    // rebuild the table only when the set of running solves changes
+    bool changed = !have;
+    for (int i = 0; i < n && !changed; ++i) {
+      const int lit = it - (begins ? begins[i] : 0);
+      const int act = (lit >= 0 && lit < descs[i].n_steps) ? 1 : 0;
+      changed = (act != active[i]);
+    }
+    if (changed) {
+      for (int i = 0; i < n; ++i) {
+        const int lit = it - (begins ? begins[i] : 0);
+        active[i] = (lit >= 0 && lit < descs[i].n_steps) ? 1 : 0;
+      }
+      int rc = build_batch<Inst>(descs, begins, n, it, tab, &ntiles);
+      if (rc != SW_OK) return rc;
+      if (!tab.empty()) {
+        cudaError_t e = cudaMemcpyAsync(table, tab.data(), tab.size() * sizeof(Inst),
+                                        cudaMemcpyHostToDevice, s);
+        if (e != cudaSuccess) return cuda_status(e, "batch table upload");
+      }
+      have = true;
+    }
+    if (tab.empty()) continue;
+    int rc = launch_steps_tma_batch(precision, table, (int)tab.size(), ntiles, it, s);
+    if (rc != SW_OK) return rc;
+  }
+  return SW_OK;
+}
+
+}  // namespace
+}  // namespace sw
+
+using namespace sw;
+
+extern "C" size_t sw_fdtd_batch_table_bytes(int n) {
+  if (n <= 0) return 0;
+  return (size_t)n * std::max(sizeof(TmaF32), sizeof(TmaF64));
+}
+
+extern "C" int sw_fdtd_batch_steps(const sw_fdtd_desc* descs, const int32_t* begins, int n,
+                                   int32_t it0, int32_t nsteps, void* table, size_t table_bytes,
+                                   void* stream) {
+  if (descs == nullptr || n <= 0 || table == nullptr || nsteps < 0) {
+    set_error("sw_fdtd_batch_steps: bad arguments");
+    return SW_EINVAL;
+  }
+  if (table_bytes < sw_fdtd_batch_table_bytes(n) || ((uintptr_t)table & 63u) != 0u) {
+    set_error("sw_fdtd_batch_steps: table must be >= %zu bytes and 64-byte aligned",
+              sw_fdtd_batch_table_bytes(n));
+    return SW_EWORKSPACE;
+  }
+  const int prec = descs[0].precision;
+  for (int i = 0; i < n; ++i) {
+    if (descs[i].precision != prec || descs[i].kernel != 0 || descs[i].n_traces > 0) {
+      set_error("sw_fdtd_batch_steps: solve %d differs in precision, asks for the direct "
+                "kernels or records traces (unsupported in a batch)", i);
+      return SW_EINVAL;
+    }
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  if (prec == SW_PLAIN_F64)
+    return batch_steps<TmaF64>(prec, descs, begins, n, it0, nsteps, table, s);
+  return batch_steps<TmaF32>(prec, descs, begins, n, it0, nsteps, table, s);
+}

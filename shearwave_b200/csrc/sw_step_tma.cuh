@@ -8,27 +8,38 @@
 
 namespace sw {
 
-// Kernel-side view of one mixed-form solve.  The tensor maps cover the two
-// FP32 state buffers as 4-D tensors (pz, ny, nx, 9 components).
+constexpr int round128(int bytes) { return (bytes + 127) / 128 * 128; }
+
+// Kernel-side view of one mixed-form solve.
+//   tm[b]  : state buffer b as a 4-D tensor (pz, ny, nx, 9 components);
+//            box (W, H, 1, 6) = the halo'd u and d of one plane
+//   tmc[b] : the same tensor, box (TZ, TY, 1, 3) = the Kahan compensation
+//   tmm    : material coefficients (pz, ny, nx, ncoef), box (TZ, TY, 1, ncoef)
 struct TmaF32 {
-  static constexpr int TZ = 64, TY = 8;    // output tile (z, y)
-  static constexpr int W = TZ + 8;         // box width: 4 cells of halo each side in z
-  static constexpr int H = TY + 2;         // box height: 1 row of halo each side in y
-  static constexpr int NF = 6;             // halo'd components per plane: u, d
-  static constexpr int NST = 4;            // plane stages in the ring
-  static constexpr int PLANE = W * H * NF; // floats per stage (box of the one TMA load)
-  static constexpr int STAGE = ((PLANE * 4 + 127) / 128) * 128 / 4;  // 128-byte aligned stride
+  static constexpr int TZ = 64, TY = 8;  // output tile (z, y)
+  static constexpr int W = TZ + 8;       // halo box width: 4 cells each side in z
+  static constexpr int H = TY + 2;       // halo box height: 1 row each side in y
+  static constexpr int NA = 4;           // halo ring stages (planes x-1, x, x+1 + 1 ahead)
+  static constexpr int NB = 3;           // point ring stages
+  static constexpr int A_BYTES = W * H * 6 * 4;
+  static constexpr int C_BYTES = TZ * TY * 3 * 4;
+  static constexpr int M_BYTES = TZ * TY * 2 * 4;
+  static constexpr int A_STAGE = round128(A_BYTES);
+  static constexpr int B_STAGE = round128(C_BYTES) + round128(M_BYTES);
+  static constexpr int CONSUMER_WARPS = TY;
+  static constexpr int THREADS = 32 * (CONSUMER_WARPS + 1);
   CUtensorMap tm[2];
+  CUtensorMap tmc[2];
+  CUtensorMap tmm;
   Geom g;
   TileSpace ts;
   float* state[2];
-  const float* m;
-  const float* e;
   const float* pat;
   const int* term_off;
   const int* term_pat;
   const double* term_scale;
   float hx, hy, hz, damp;
+  int ncoef;  // 1: mu only, 2: mu and eta
   int use_damp, kahan, n_steps, snap_stride;
   float* snaps;
   int* flags;
@@ -36,30 +47,33 @@ struct TmaF32 {
   int tile_base;  // first global tile of this solve in a batched launch
 };
 
-// Kernel-side view of one plain-FP64 solve: three rotating buffers, each a
-// 4-D tensor (pz, ny, nx, 3 components).
+// Kernel-side view of one plain-FP64 solve.
+//   tm[b] : rotating buffer b as a 4-D tensor (pz, ny, nx, 3); box (W, H, 1, 3)
+//   tmm   : material coefficients (pz, ny, nx, ncoef), box (TZ, TY, 1, ncoef)
 struct TmaF64 {
   static constexpr int TZ = 32, TY = 8;
   static constexpr int W = TZ + 4;  // 2 cells of halo each side in z (16-byte aligned)
   static constexpr int H = TY + 2;
-  static constexpr int NF = 6;      // u_prev (3) then u_curr (3)
-  static constexpr int NST = 4;
-  static constexpr int PLANE = W * H * NF;  // doubles of the two boxes
-  // each box lands on a 128-byte boundary (TMA destination alignment)
-  static constexpr int HALF = ((W * H * 3 * 8 + 127) / 128) * 128 / 8;
-  static constexpr int STAGE = 2 * HALF;
+  static constexpr int NA = 4, NB = 3;
+  static constexpr int BOX_BYTES = W * H * 3 * 8;        // one buffer's box
+  static constexpr int HALF = round128(BOX_BYTES);        // u_prev box, then u_curr box
+  static constexpr int A_STAGE = 2 * HALF;
+  static constexpr int M_BYTES = TZ * TY * 2 * 8;
+  static constexpr int B_STAGE = round128(M_BYTES);
+  static constexpr int CONSUMER_WARPS = TY;
+  static constexpr int THREADS = 32 * (CONSUMER_WARPS + 1);
   CUtensorMap tm[3];
+  CUtensorMap tmm;
   Geom g;
   TileSpace ts;
   double* state[3];
-  const double* m;
-  const double* e;
   const double* ir;
   const double* pat;
   const int* term_off;
   const int* term_pat;
   const double* term_scale;
   double ihx2, ihy2, ihz2, inv_dt, dt2, damp;
+  int ncoef;
   int use_damp, n_steps, snap_stride;
   double* snaps;
   int* flags;

@@ -43,6 +43,7 @@ __all__ = [
     "project_body_force_to_shear",
     "project_vector_field",
     "shear_fdtd",
+    "shear_fdtd_batch",
     "shear_fdtd_jax",
 ]
 
@@ -327,9 +328,10 @@ class _Run:
         self.state = torch.empty((nbuf, ncomp, self.ncell), dtype=self.dt, device=dev)
         for i in range(nbuf):
             d.state[i] = self.state[i].data_ptr()
-        self.coef_m = torch.zeros(self.ncell, dtype=self.dt, device=dev)
-        d.coef_m = self.coef_m.data_ptr()
-        self.coef_e = None
+        # material coefficients: one allocation, component 0 the mu term,
+        # component 1 the eta term (used only with viscosity)
+        self.coef = torch.zeros((2, self.ncell), dtype=self.dt, device=dev)
+        d.coef_m = self.coef[0].data_ptr()
         self.inv_rho = None
         if prec == _native.SW_PLAIN_F64:
             self.inv_rho = torch.zeros(self.ncell, dtype=self.dt, device=dev)
@@ -349,8 +351,7 @@ class _Run:
         if eta is not None:
             eta_mode = 1
             e, es = _material(eta, self.shape, in_dt, dev)
-            self.coef_e = torch.zeros(self.ncell, dtype=self.dt, device=dev)
-            self.desc.coef_e = self.coef_e.data_ptr()
+            self.desc.coef_e = self.coef[1].data_ptr()
         _native.call("sw_fdtd_materials", self.p(), dtype_code(in_dt), ptr(r), rs, ptr(m), ms,
                      eta_mode, ptr(e), es, stream_handle())
         self.rho_dev, self.rho_s = r, rs
@@ -371,10 +372,12 @@ class _Run:
             self.term_scale = torch.zeros(1, dtype=torch.float64, device=self.dev)
             d.term_scale = self.term_scale.data_ptr()
 
-    def pattern_from(self, ws: _Workspace, dst: torch.Tensor, spacing_dt2: float):
-        """Store the projected force (ws.out) as a pattern of this form."""
+    def pattern_from_tensor(self, fs: torch.Tensor, dst: torch.Tensor, spacing_dt2: float):
+        """Store a projected force (3 padded FP64 components) as a pattern of this form."""
         if self.prec == _native.SW_PLAIN_F64:
-            dst.copy_(ws.out)  # FP64 f_S as is
+            _native.call("sw_convert", 3, fs.data_ptr(), self.nx, self.ny, self.nz,
+                         _native.SW_F64, dst.data_ptr(), self.ncell, self.ny * self.pz, self.pz,
+                         1, 1.0, _native.SW_F64, None, 0, 0, 0, stream_handle())
         else:
             # dT^2 f_S / rho in FP32
             r = self.rho_dev
@@ -384,7 +387,7 @@ class _Run:
             else:
                 scale, rptr, rs = spacing_dt2, ptr(r), (self.ny * self.nz, self.nz, 1)
                 rdt = dtype_code(r.dtype)
-            _native.call("sw_convert", 3, ws.out.data_ptr(), self.nx, self.ny, self.nz,
+            _native.call("sw_convert", 3, fs.data_ptr(), self.nx, self.ny, self.nz,
                          _native.SW_F32, dst.data_ptr(), self.ncell, self.ny * self.pz, self.pz,
                          1, scale, rdt, rptr, *rs, stream_handle())
 
@@ -432,7 +435,204 @@ def _prepare_opts(opts):
     return opts, reproject_every
 
 
-def shear_fdtd(  # noqa: PLR0912, PLR0915
+class _Solve:
+    """Device state and phases of one shear_fdtd problem.
+
+    Construction validates the arguments (the reference's checks and
+    messages), uploads inputs, computes the material coefficients, the
+    initial state and allocates the outputs.  The force projection, the time
+    loop and the outputs are separate phases so that a batch of solves can
+    run each phase for all of them together.
+    """
+
+    def __init__(self, bx, by, bz, rho, mu, dX, dY, dZ, dT, n_steps, opts, *,
+                 snapshot_stride=None, trace_indices=None, return_traces=False):
+        ref = bx if bx is not None else (by if by is not None else bz)
+        if ref is None:
+            raise ValueError("At least one body-force component must be provided.")
+        opts, self.reproject_every = _prepare_opts(opts)
+        if snapshot_stride is None:
+            snapshot_stride = opts.get("snapshot_stride")
+        snapshot_stride, trace_cells = _check_jax_kwargs(n_steps, trace_indices, return_traces,
+                                                         snapshot_stride)
+        n_steps = int(n_steps)
+        self.opts = opts
+        self.n_steps = n_steps
+        self.spacing = (dX, dY, dZ)
+        self.dT = dT
+        self.tol = opts.get("poisson_tol", 1e-5)
+        self.max_iters = opts.get("poisson_max_iters", 200)
+        self.verbose = opts.get("verbose", False)
+        self.progress_every = opts.get("progress_every", max(1, n_steps // 10))
+        self.info = opts.get("info")
+        self.prec = _precision(opts)
+        dt = self.dt = _field_dtype(self.prec)
+        np_dt = np_dtype(dt)
+        shape = self.shape = tuple(int(s) for s in _shape(ref)[:3])
+        nx, ny, nz = shape
+        if trace_cells is not None and trace_cells.size:
+            if np.any(trace_cells < 0) or np.any(trace_cells >= np.asarray(shape)):
+                raise ValueError("trace_indices outside the grid.")
+        eta = opts.get("eta", 0.0)
+        if np.isscalar(eta):
+            eta = float(eta) if float(eta) != 0.0 else None
+        validate_inputs(bx, by, bz, rho, mu, eta, opts, shape, n_steps)
+        kern = opts.get("step_kernel", "tma")
+        if kern not in ("tma", "direct"):
+            raise ValueError("step_kernel must be 'tma' or 'direct'")
+        dev = self.dev = require_cuda()
+        self.forces = _gather_forces(bx, by, bz, opts, shape, n_steps, dt, dev, np_dt)
+
+        self.tev = None  # CUDA events: start, steps begin, steps end, done
+        if self.info is not None:
+            self.tev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+            self.tev[0].record()
+        run = self.run = _Run(shape, (dX, dY, dZ), dT, n_steps, self.prec,
+                              opts.get("kahan", True), dev)
+        run.desc.vel_damp = float(opts.get("vel_damp", 0.0))
+        run.desc.kernel = 0 if kern == "tma" else 1
+        run.desc.xchunk = int(opts.get("xchunk", 0) or 0)
+        run.materials(rho, mu, eta, dt)
+        iu = iv = None
+        if opts.get("initial_u") is not None:
+            iu = to_device(opts["initial_u"], dt, dev)
+        if opts.get("initial_v") is not None:
+            iv = to_device(opts["initial_v"], dt, dev)
+        _native.call("sw_fdtd_init", run.p(), ptr(iu), ptr(iv), stream_handle())
+
+        self.n_sep = len(self.forces.separable)
+        n_pat = self.n_sep + (1 if self.forces.stream4d is not None else 0)
+        self.pats = torch.zeros((max(n_pat, 1), 3, run.ncell), dtype=dt, device=dev)
+        self.cg_log = []
+
+        self.snaps = None
+        if snapshot_stride:
+            self.snaps = torch.zeros((n_steps // snapshot_stride, nx, ny, nz, 3), dtype=dt,
+                                     device=dev)
+            run.desc.snap_stride = snapshot_stride
+            run.desc.snaps = self.snaps.data_ptr()
+        self.traces = None
+        if trace_cells is not None and return_traces:
+            tc = torch.as_tensor(trace_cells.reshape(-1), dtype=torch.int32, device=dev)
+            self.traces = torch.zeros((trace_cells.shape[0], n_steps), dtype=dt, device=dev)
+            run.keep.append(tc)
+            run.desc.n_traces = int(trace_cells.shape[0])
+            run.desc.trace_cells = tc.data_ptr()
+            run.desc.traces = self.traces.data_ptr()
+
+    # ---- phases ---------------------------------------------------------
+    def needs_per_step_host(self, callback) -> bool:
+        """Whether the time loop must return to the host between steps."""
+        return (callback is not None or self.forces.stream4d is not None
+                or bool(self.reproject_every) or bool(self.verbose)
+                or self.run.desc.n_traces > 0 or self.run.desc.kernel != 0)
+
+    def separable_inputs(self):
+        """(pattern index, device components) of every separable force term."""
+        return [(k, comps) for k, (comps, _env) in enumerate(self.forces.separable)]
+
+    def store_pattern(self, k: int, fs_out: torch.Tensor):
+        """Store a projected pattern (3 padded FP64 components) as term k."""
+        self.run.pattern_from_tensor(fs_out, self.pats[k], self.dT * self.dT)
+
+    def build_terms(self):
+        f = self.forces
+        term_off, term_pat, term_scale = [0], [], []
+        for it in range(self.n_steps):
+            for k, (_c, env) in enumerate(f.separable):
+                s = float(env[it])
+                if s != 0.0:
+                    term_pat.append(k)
+                    term_scale.append(s)
+            if f.stream4d is not None and not f.zero_steps[it]:
+                term_pat.append(self.n_sep)
+                term_scale.append(1.0)
+            term_off.append(len(term_pat))
+        self.term_off = term_off
+        self.run.set_patterns(self.pats, term_off, term_pat, term_scale)
+
+    def mark_steps_begin(self):
+        if self.tev is not None:
+            self.tev[1].record()
+
+    def finish(self, return_device: bool):
+        run, dt, dev = self.run, self.dt, self.dev
+        nx, ny, nz = self.shape
+        if self.tev is not None:
+            self.tev[2].record()
+        u = torch.empty((nx, ny, nz, 3), dtype=dt, device=dev)
+        v = torch.empty((nx, ny, nz, 3), dtype=dt, device=dev)
+        _native.call("sw_fdtd_finish", run.p(), self.n_steps, ptr(u), ptr(v), stream_handle())
+        nonfinite = bool(run.flags.item())
+        if self.info is not None:
+            tev = self.tev
+            tev[3].record()
+            tev[3].synchronize()
+            self.info.update(
+                cg=self.cg_log, nonfinite=nonfinite,
+                precision="fp64" if self.prec == _native.SW_PLAIN_F64 else "mixed",
+                t_setup_ms=tev[0].elapsed_time(tev[1]),
+                t_steps_ms=tev[1].elapsed_time(tev[2]),
+                t_finish_ms=tev[2].elapsed_time(tev[3]),
+                n_push_steps=int(sum(1 for i in range(self.n_steps)
+                                     if self.term_off[i + 1] > self.term_off[i])))
+        if nonfinite:
+            warnings.warn("shear_fdtd: non-finite displacement encountered (unstable dT?)",
+                          RuntimeWarning, stacklevel=3)
+        out = [to_host(u, return_device), to_host(v, return_device)]
+        if self.snaps is not None:
+            out.append(to_host(self.snaps, return_device))
+        elif self.traces is not None:
+            out.append(to_host(self.traces, return_device))
+        return tuple(out)
+
+    def run_loop(self, callback, ws: "_Workspace"):
+        """The time loop of solver.py:194-239 for this solve alone."""
+        run, dt, dev = self.run, self.dt, self.dev
+        nx, ny, nz = self.shape
+        n_steps = self.n_steps
+        dX, dY, dZ = self.spacing
+        f = self.forces
+        per_step = callback is not None or f.stream4d is not None
+        events = set()
+        if self.reproject_every:
+            events.update(range(self.reproject_every, n_steps + 1, self.reproject_every))
+        if self.verbose:
+            events.update(range(self.progress_every, n_steps + 1, self.progress_every))
+        u_cb = torch.empty((nx, ny, nz, 3), dtype=dt, device=dev) if callback else None
+        self.mark_steps_begin()
+        it = 0
+        strm = stream_handle()
+        while it < n_steps:
+            if per_step:
+                end = it + 1
+            else:
+                later = [e for e in events if e > it]
+                end = min(later) if later else n_steps
+            if f.stream4d is not None and not f.zero_steps[it]:
+                # per-step projection of b[..., it] (solver.py:198-199)
+                comps = [None if b is None else (b[..., it] if b.dim() == 4 else b).contiguous()
+                         for b in f.stream4d]
+                st = _project_raw(ws, dtype_code(dt), comps, (ny * nz, nz, 1), self.shape, dX,
+                                  dY, dZ, self.tol, self.max_iters)
+                self.cg_log.append(st)
+                self.store_pattern(self.n_sep, ws.out)
+            _native.call("sw_fdtd_steps", run.p(), it, end - it, strm)
+            if callback is not None:
+                _native.call("sw_fdtd_finish", run.p(), end, ptr(u_cb), None, strm)
+                callback(end - 1, u_cb.cpu().numpy())
+            if self.verbose and end % self.progress_every == 0:
+                print(f"FDTD it={end}/{n_steps}")
+            if self.reproject_every and end % self.reproject_every == 0:
+                stats = (_native.CGStats * 2)()
+                _native.call("sw_fdtd_reproject", run.p(), end, float(self.tol),
+                             int(self.max_iters), ws.out.data_ptr(), ptr(ws.ws), ws.bytes, stats,
+                             strm)
+                self.cg_log += [stats[0].as_dict(), stats[1].as_dict()]
+            it = end
+
+
+def shear_fdtd(
     bx,
     by,
     bz,
@@ -468,179 +668,125 @@ def shear_fdtd(  # noqa: PLR0912, PLR0915
 
     Additional opts: ``precision`` ("mixed" default, or "fp64"), ``kahan``
     (True), ``step_kernel`` ("tma" default, or "direct"), ``xchunk`` (planes
-    per tile along x, 0 = automatic), ``force_terms`` (extra separable terms: list of
-    ``((bx, by, bz), env)``), ``snapshot_stride`` (alias of the keyword),
-    ``info`` (dict filled with CG statistics and a non-finite flag).
+    per tile along x, 0 = automatic), ``force_terms`` (extra separable terms:
+    list of ``((bx, by, bz), env)``), ``snapshot_stride`` (alias of the
+    keyword), ``info`` (dict filled with CG statistics, phase times and a
+    non-finite flag).
 
     ``callback(it, u)`` is called after every step with a host copy of the new
     displacement (the reference passes its live buffer; writing into the copy
     does not feed back into the solve).
     """
-    ref = bx if bx is not None else (by if by is not None else bz)
-    if ref is None:
-        raise ValueError("At least one body-force component must be provided.")
-    opts, reproject_every = _prepare_opts(opts)
-    if snapshot_stride is None:
-        snapshot_stride = opts.get("snapshot_stride")
-    snapshot_stride, trace_cells = _check_jax_kwargs(n_steps, trace_indices, return_traces,
-                                                     snapshot_stride)
-    n_steps = int(n_steps)
-    vel_damp = float(opts.get("vel_damp", 0.0))
-    tol = opts.get("poisson_tol", 1e-5)
-    max_iters = opts.get("poisson_max_iters", 200)
-    verbose = opts.get("verbose", False)
-    progress_every = opts.get("progress_every", max(1, n_steps // 10))
-    info = opts.get("info")
-    prec = _precision(opts)
-    dt = _field_dtype(prec)
-    np_dt = np_dtype(dt)
+    sv = _Solve(bx, by, bz, rho, mu, dX, dY, dZ, dT, n_steps, opts,
+                snapshot_stride=snapshot_stride, trace_indices=trace_indices,
+                return_traces=return_traces)
+    return _solve_alone(sv, callback, return_device)
 
-    shape = tuple(int(s) for s in _shape(ref)[:3])
-    nx, ny, nz = shape
-    if trace_cells is not None and trace_cells.size:
-        if np.any(trace_cells < 0) or np.any(trace_cells >= np.asarray(shape)):
-            raise ValueError("trace_indices outside the grid.")
-    eta = opts.get("eta", 0.0)
-    if np.isscalar(eta):
-        eta = float(eta) if float(eta) != 0.0 else None
-    validate_inputs(bx, by, bz, rho, mu, eta, opts, shape, n_steps)
-    dev = require_cuda()
-    forces = _gather_forces(bx, by, bz, opts, shape, n_steps, dt, dev, np_dt)
 
-    tev = None  # CUDA events: start, steps begin, steps end, done
-    if info is not None:
-        tev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
-        tev[0].record()
-    run = _Run(shape, (dX, dY, dZ), dT, n_steps, prec, opts.get("kahan", True), dev)
-    run.desc.vel_damp = vel_damp
-    kern = opts.get("step_kernel", "tma")
-    if kern not in ("tma", "direct"):
-        raise ValueError("step_kernel must be 'tma' or 'direct'")
-    run.desc.kernel = 0 if kern == "tma" else 1
-    run.desc.xchunk = int(opts.get("xchunk", 0) or 0)
-    run.materials(rho, mu, eta, dt)
-
-    init_u = opts.get("initial_u")
-    init_v = opts.get("initial_v")
-    iu = iv = None
-    if init_u is not None:
-        if _shape(init_u) != (*shape, 3):
-            raise ValueError("initial_u must match shape (nx,ny,nz,3)")
-        iu = to_device(init_u, dt, dev)
-    if init_v is not None:
-        if _shape(init_v) != (*shape, 3):
-            raise ValueError("initial_v must match shape (nx,ny,nz,3)")
-        iv = to_device(init_v, dt, dev)
-    _native.call("sw_fdtd_init", run.p(), ptr(iu), ptr(iv), stream_handle())
-
-    # ---- forces: project the separable patterns once (solver.py:188-192) ----
-    ws = _Workspace(nx, ny, nz, dev)
-    cg_log = []
-    n_sep = len(forces.separable)
-    n_pat = n_sep + (1 if forces.stream4d is not None else 0)
-    pats = torch.zeros((max(n_pat, 1), 3, run.ncell), dtype=dt, device=dev)
-    if verbose and n_sep:
+def _solve_alone(sv: _Solve, callback, return_device):
+    """Projection, time loop and outputs of one solve."""
+    nx, ny, nz = sv.shape
+    dX, dY, dZ = sv.spacing
+    ws = _Workspace(nx, ny, nz, sv.dev)
+    if sv.verbose and sv.n_sep:
         print("Pre-computing Helmholtz projection (separable force)...")
-    for k, (comps, _env) in enumerate(forces.separable):
-        st = _project_raw(ws, dtype_code(dt), comps, (ny * nz, nz, 1), shape, dX, dY, dZ, tol,
-                          max_iters)
-        cg_log.append(st)
-        run.pattern_from(ws, pats[k], dT * dT)
-    term_off, term_pat, term_scale = [0], [], []
-    for it in range(n_steps):
-        for k, (_c, env) in enumerate(forces.separable):
-            s = float(env[it])
-            if s != 0.0:
-                term_pat.append(k)
-                term_scale.append(s)
-        if forces.stream4d is not None and not forces.zero_steps[it]:
-            term_pat.append(n_sep)
-            term_scale.append(1.0)
-        term_off.append(len(term_pat))
-    run.set_patterns(pats, term_off, term_pat, term_scale)
+    for k, comps in sv.separable_inputs():
+        st = _project_raw(ws, dtype_code(sv.dt), comps, (ny * nz, nz, 1), sv.shape, dX, dY, dZ,
+                          sv.tol, sv.max_iters)
+        sv.cg_log.append(st)
+        sv.store_pattern(k, ws.out)
+    sv.build_terms()
+    sv.run_loop(callback, ws)
+    return sv.finish(return_device)
 
-    # ---- outputs written by the step kernels ----
-    snaps = None
-    if snapshot_stride:
-        snaps = torch.zeros((n_steps // snapshot_stride, nx, ny, nz, 3), dtype=dt, device=dev)
-        run.desc.snap_stride = snapshot_stride
-        run.desc.snaps = snaps.data_ptr()
-    traces = None
-    if trace_cells is not None and return_traces:
-        tc = torch.as_tensor(trace_cells.reshape(-1), dtype=torch.int32, device=dev)
-        traces = torch.zeros((trace_cells.shape[0], n_steps), dtype=dt, device=dev)
-        run.keep.append(tc)
-        run.desc.n_traces = int(trace_cells.shape[0])
-        run.desc.trace_cells = tc.data_ptr()
-        run.desc.traces = traces.data_ptr()
 
-    # ---- time loop (solver.py:194-239) ----
-    per_step = callback is not None or forces.stream4d is not None
-    events = set()
-    if reproject_every:
-        events.update(range(reproject_every, n_steps + 1, reproject_every))
-    if verbose:
-        events.update(range(progress_every, n_steps + 1, progress_every))
-    u_cb = torch.empty((nx, ny, nz, 3), dtype=dt, device=dev) if callback is not None else None
-    if tev is not None:
-        tev[1].record()
-    tmp_sep = None
-    it = 0
+def shear_fdtd_batch(problems, *, precision=None, return_device=False):
+    """Run many independent ``shear_fdtd`` problems together on one GPU.
+
+    ``problems`` is a sequence of dicts of ``shear_fdtd`` keyword arguments
+    (``bx, by, bz, rho, mu, dX, dY, dZ, dT, n_steps, opts`` and optionally
+    ``snapshot_stride``); grids, materials, pushes and ``n_steps`` may all
+    differ.  The force projections of all problems run as one batched CG
+    (every launch advances every unfinished solve) and the time loops as one
+    launch per step over the tiles of every running solve.  ``precision``
+    overrides ``opts["precision"]`` for all problems.
+
+    Problems that need the host between steps (callback-free here, but 4-D
+    forces, ``reproject_every``, ``verbose``, traces or the direct kernels)
+    are run one after another through :func:`shear_fdtd` on the same GPU.
+    Returns a list of ``shear_fdtd`` results in input order.
+    """
+    solves, results = [], [None] * len(problems)
+    for i, p in enumerate(problems):
+        opts = dict(p.get("opts") or {})
+        if precision is not None:
+            opts["precision"] = precision
+        kw = {k: p[k] for k in ("bx", "by", "bz", "rho", "mu", "dX", "dY", "dZ", "dT", "n_steps")}
+        sv = _Solve(**kw, opts=opts, snapshot_stride=p.get("snapshot_stride"))
+        if sv.needs_per_step_host(None):
+            results[i] = _solve_alone(sv, None, return_device)
+            continue
+        solves.append((i, sv))
+    if not solves:
+        return results
+    precs = {sv.prec for _, sv in solves}
+    groups = [[(i, sv) for i, sv in solves if sv.prec == pr] for pr in sorted(precs)]
+    for group in groups:
+        _run_batch_group([sv for _, sv in group])
+        for i, sv in group:
+            results[i] = sv.finish(return_device)
+    return results
+
+
+def _run_batch_group(solves):
+    """Batched projection + batched time loop for solves of one precision."""
+    lib = _native.load()
+    dev = solves[0].dev
     strm = stream_handle()
-    while it < n_steps:
-        if per_step:
-            end = it + 1
-        else:
-            later = [e for e in events if e > it]
-            end = min(later) if later else n_steps
-        if forces.stream4d is not None and not forces.zero_steps[it]:
-            # per-step projection of b[..., it] (solver.py:198-199)
-            comps = [None if b is None else (b[..., it] if b.dim() == 4 else b).contiguous()
-                     for b in forces.stream4d]
-            st = _project_raw(ws, dtype_code(dt), comps, (ny * nz, nz, 1), shape, dX, dY, dZ,
-                              tol, max_iters)
-            cg_log.append(st)
-            if tmp_sep is None:
-                tmp_sep = pats[n_sep]
-            run.pattern_from(ws, tmp_sep, dT * dT)
-        _native.call("sw_fdtd_steps", run.p(), it, end - it, strm)
-        if callback is not None:
-            _native.call("sw_fdtd_finish", run.p(), end, ptr(u_cb), None, strm)
-            callback(end - 1, u_cb.cpu().numpy())
-        if verbose and end % progress_every == 0:
-            print(f"FDTD it={end}/{n_steps}")
-        if reproject_every and end % reproject_every == 0:
-            stats = (_native.CGStats * 2)()
-            _native.call("sw_fdtd_reproject", run.p(), end, float(tol), int(max_iters),
-                         ws.out.data_ptr(), ptr(ws.ws), ws.bytes, stats, strm)
-            cg_log += [stats[0].as_dict(), stats[1].as_dict()]
-        it = end
-
-    if tev is not None:
-        tev[2].record()
-    u = torch.empty((nx, ny, nz, 3), dtype=dt, device=dev)
-    v = torch.empty((nx, ny, nz, 3), dtype=dt, device=dev)
-    _native.call("sw_fdtd_finish", run.p(), n_steps, ptr(u), ptr(v), strm)
-    nonfinite = bool(run.flags.item())
-    if info is not None:
-        tev[3].record()
-        tev[3].synchronize()
-        info.update(cg=cg_log, nonfinite=nonfinite,
-                    precision="fp64" if prec == _native.SW_PLAIN_F64 else "mixed",
-                    t_setup_ms=tev[0].elapsed_time(tev[1]),
-                    t_steps_ms=tev[1].elapsed_time(tev[2]),
-                    t_finish_ms=tev[2].elapsed_time(tev[3]),
-                    n_push_steps=int(sum(1 for i in range(n_steps)
-                                         if term_off[i + 1] > term_off[i])))
-    if nonfinite:
-        warnings.warn("shear_fdtd: non-finite displacement encountered (unstable dT?)",
-                      RuntimeWarning, stacklevel=2)
-    out = [to_host(u, return_device), to_host(v, return_device)]
-    if snaps is not None:
-        out.append(to_host(snaps, return_device))
-    elif traces is not None:
-        out.append(to_host(traces, return_device))
-    return tuple(out)
+    # ---- batched projection of every separable pattern ----
+    jobs, owners, bufs = [], [], []
+    for sv in solves:
+        nx, ny, nz = sv.shape
+        for k, comps in sv.separable_inputs():
+            ws = _Workspace(nx, ny, nz, dev)
+            j = _native.ProjectJob()
+            j.in_dtype = dtype_code(sv.dt)
+            j.fx, j.fy, j.fz = (ptr(c) if c is not None else None for c in comps)
+            j.sx, j.sy, j.sz = ny * nz, nz, 1
+            j.nx, j.ny, j.nz = nx, ny, nz
+            j.dX, j.dY, j.dZ = sv.spacing
+            j.tol = float(sv.tol)
+            j.max_iters = int(sv.max_iters)
+            j.out = ws.out.data_ptr()
+            j.workspace = ws.ws.data_ptr()
+            j.workspace_bytes = ws.bytes
+            jobs.append(j)
+            owners.append((sv, k))
+            bufs.append(ws)
+    if jobs:
+        dtypes = {j.in_dtype for j in jobs}
+        for dtc in dtypes:
+            idx = [q for q, j in enumerate(jobs) if j.in_dtype == dtc]
+            arr = (_native.ProjectJob * len(idx))(*[jobs[q] for q in idx])
+            stats = (_native.CGStats * len(idx))()
+            tb = int(lib.sw_project_batch_table_bytes(len(idx)))
+            table = torch.empty(tb, dtype=torch.uint8, device=dev)
+            _native.call("sw_project_batch", arr, len(idx), table.data_ptr(), tb, stats, strm)
+            for q, st in zip(idx, stats):
+                sv, k = owners[q]
+                sv.cg_log.append(st.as_dict())
+                sv.store_pattern(k, bufs[q].out)
+    for sv in solves:
+        sv.build_terms()
+        sv.mark_steps_begin()
+    # ---- batched time loop ----
+    n = len(solves)
+    descs = (_native.FdtdDesc * n)(*[sv.run.desc for sv in solves])
+    tb = int(lib.sw_fdtd_batch_table_bytes(n))
+    table = torch.empty(tb + 64, dtype=torch.uint8, device=dev)
+    base = (table.data_ptr() + 63) // 64 * 64
+    steps = max(sv.n_steps for sv in solves)
+    _native.call("sw_fdtd_batch_steps", descs, None, n, 0, steps, base, tb, strm)
 
 
 def shear_fdtd_jax(bx, by, bz, rho, mu, dX, dY, dZ, dT, n_steps, opts=None, callback=None,

@@ -112,6 +112,26 @@ int sw_project(int in_dtype, const void* fx, const void* fy, const void* fz, int
                double dZ, double tol, int max_iters, double* out, void* workspace,
                size_t workspace_bytes, sw_cg_stats* stats, void* stream);
 
+/* Bytes of device workspace sw_project_spectral needs for an (nx, ny, nz) grid. */
+size_t sw_project_spectral_workspace_bytes(int nx, int ny, int nz);
+
+/* The same projection with the Poisson problem solved directly instead of by
+ * CG: A = -div_c(grad_c) is separable into per-axis operators whose
+ * eigenvectors are discrete sine / cosine bases, so phi is three forward
+ * per-axis transforms, a division by the eigenvalue sums and three inverse
+ * transforms, in FP64.  Gives the exact (minimum-norm) solution the
+ * reference's CG approaches as tol -> 0; keeps the max|div| < 1e-12 early
+ * exit.  stats->iters is 0. */
+int sw_project_spectral(int in_dtype, const void* fx, const void* fy, const void* fz,
+                        int64_t in_sx, int64_t in_sy, int64_t in_sz, int nx, int ny, int nz,
+                        double dX, double dY, double dZ, double* out, void* workspace,
+                        size_t workspace_bytes, sw_cg_stats* stats, void* stream);
+
+/* Host helper: the orthonormal basis Q (m x m row-major, m = n - 2) and the
+ * eigenvalues lam (m) of one axis' 1-D operator for n grid points of
+ * spacing h (host buffers). */
+int sw_spectral_basis(int n, double h, double* Q, double* lam);
+
 /* One solve of a batched projection (fields as for sw_project). */
 typedef struct sw_project_job {
   int32_t in_dtype;

@@ -92,6 +92,11 @@ _SIGNATURES = {
     "sw_project_workspace_bytes": ([C.c_int, C.c_int, C.c_int], _sz),
     "sw_project": ([C.c_int, _vp, _vp, _vp, _i64, _i64, _i64, C.c_int, C.c_int, C.c_int, _f64,
                     _f64, _f64, _f64, C.c_int, _vp, _vp, _sz, C.POINTER(CGStats), _vp], C.c_int),
+    "sw_project_spectral_workspace_bytes": ([C.c_int, C.c_int, C.c_int], _sz),
+    "sw_project_spectral": ([C.c_int, _vp, _vp, _vp, _i64, _i64, _i64, C.c_int, C.c_int,
+                             C.c_int, _f64, _f64, _f64, _vp, _vp, _sz, C.POINTER(CGStats), _vp],
+                            C.c_int),
+    "sw_spectral_basis": ([C.c_int, _f64, _vp, _vp], C.c_int),
     "sw_project_batch_table_bytes": ([C.c_int], _sz),
     "sw_project_batch": ([C.POINTER(ProjectJob), C.c_int, _vp, _sz, C.POINTER(CGStats), _vp],
                          C.c_int),

@@ -127,22 +127,51 @@ class _Workspace:
 
     def __init__(self, nx, ny, nz, dev):
         lib = _native.load()
-        self.bytes = int(lib.sw_project_workspace_bytes(nx, ny, nz))
+        self.bytes = max(int(lib.sw_project_workspace_bytes(nx, ny, nz)),
+                         int(lib.sw_project_spectral_workspace_bytes(nx, ny, nz)))
         self.pz = int(lib.sw_pitch(nz))
         self.ncell = nx * ny * self.pz
         self.ws = torch.empty(self.bytes, dtype=torch.uint8, device=dev)
         self.out = torch.empty((3, self.ncell), dtype=torch.float64, device=dev)
 
 
+_METHODS = ("cg", "spectral")
+
+
+def _projection_method(choice: str, prec: int, tol: float) -> str:
+    """Resolve opts["projection"].
+
+    "auto": the plain FP64 form always runs the reference's CG (its 1e-10
+    parity is with the CG's truncated iterate); the mixed form uses the exact
+    spectral solve when poisson_tol <= 1e-8, where it differs from the
+    reference's converged CG by less than the CG's own truncation (far inside
+    the 1e-4 budget), and the CG otherwise.
+    """
+    if choice == "auto":
+        if prec == _native.SW_PLAIN_F64:
+            return "cg"
+        return "spectral" if float(tol) <= 1e-8 else "cg"
+    if choice not in _METHODS:
+        raise ValueError(f"projection must be 'auto' or one of {_METHODS}")
+    return choice
+
+
 def _project_raw(ws: _Workspace, dtype_c: int, comps, strides, shape, dX, dY, dZ, tol,
-                 max_iters) -> dict:
-    """Run sw_project on device components; the result is left in ws.out."""
+                 max_iters, method: str = "cg") -> dict:
+    """Project device components (CG or the direct spectral solve) into ws.out."""
     nx, ny, nz = shape
     st = _native.CGStats()
-    _native.call("sw_project", dtype_c, *[ptr(c) if c is not None else None for c in comps],
-                 *strides, nx, ny, nz, dX, dY, dZ, float(tol), int(max_iters), ptr(ws.out),
-                 ptr(ws.ws), ws.bytes, C.byref(st), stream_handle())
-    return st.as_dict()
+    fs = [ptr(c) if c is not None else None for c in comps]
+    if method == "spectral":
+        _native.call("sw_project_spectral", dtype_c, *fs, *strides, nx, ny, nz, dX, dY, dZ,
+                     ptr(ws.out), ptr(ws.ws), ws.bytes, C.byref(st), stream_handle())
+    else:
+        _native.call("sw_project", dtype_c, *fs, *strides, nx, ny, nz, dX, dY, dZ, float(tol),
+                     int(max_iters), ptr(ws.out), ptr(ws.ws), ws.bytes, C.byref(st),
+                     stream_handle())
+    d = st.as_dict()
+    d["method"] = method
+    return d
 
 
 def _unpad(ws: _Workspace, shape, dt: torch.dtype, dev) -> list[torch.Tensor]:
@@ -156,14 +185,18 @@ def _unpad(ws: _Workspace, shape, dt: torch.dtype, dev) -> list[torch.Tensor]:
     return outs
 
 
-def project_vector_field(fx, fy, fz, dX, dY, dZ, tol, max_iters, *, info=None):
+def project_vector_field(fx, fy, fz, dX, dY, dZ, tol, max_iters, *, info=None, method="cg"):
     """Helmholtz-Hodge projection onto discretely divergence-free fields.
 
     solver.py:644-683.  The CG (solver.py:1010-1050) runs in FP64 on the GPU
-    with the reference's stopping rule.  Returns three arrays in the input
-    dtype (float32 unless the inputs are float64).  ``info`` (dict) receives
-    the CG iteration count and exit reason.
+    with the reference's stopping rule.  ``method="spectral"`` solves the
+    Poisson problem directly instead (exact solution, ``tol`` and
+    ``max_iters`` unused).  Returns three arrays in the input dtype (float32
+    unless the inputs are float64).  ``info`` (dict) receives the CG
+    iteration count and exit reason.
     """
+    if method not in _METHODS:
+        raise ValueError(f"method must be one of {_METHODS}")
     dev = require_cuda()
     dt = torch.promote_types(torch.promote_types(_op_dtype(fx), _op_dtype(fy)), _op_dtype(fz))
     comps = [to_device(v, dt, dev) for v in (fx, fy, fz)]
@@ -173,7 +206,7 @@ def project_vector_field(fx, fy, fz, dX, dY, dZ, tol, max_iters, *, info=None):
     nx, ny, nz = shape
     ws = _Workspace(nx, ny, nz, dev)
     st = _project_raw(ws, dtype_code(dt), comps, (ny * nz, nz, 1), shape, dX, dY, dZ, tol,
-                      max_iters)
+                      max_iters, method)
     if info is not None:
         info.update(st)
     outs = _unpad(ws, shape, dt, dev)
@@ -480,6 +513,7 @@ class _Solve:
         kern = opts.get("step_kernel", "tma")
         if kern not in ("tma", "direct"):
             raise ValueError("step_kernel must be 'tma' or 'direct'")
+        self.method = _projection_method(opts.get("projection", "auto"), self.prec, self.tol)
         dev = self.dev = require_cuda()
         self.forces = _gather_forces(bx, by, bz, opts, shape, n_steps, dt, dev, np_dt)
 
@@ -614,7 +648,7 @@ class _Solve:
                 comps = [None if b is None else (b[..., it] if b.dim() == 4 else b).contiguous()
                          for b in f.stream4d]
                 st = _project_raw(ws, dtype_code(dt), comps, (ny * nz, nz, 1), self.shape, dX,
-                                  dY, dZ, self.tol, self.max_iters)
+                                  dY, dZ, self.tol, self.max_iters, self.method)
                 self.cg_log.append(st)
                 self.store_pattern(self.n_sep, ws.out)
             _native.call("sw_fdtd_steps", run.p(), it, end - it, strm)
@@ -666,8 +700,10 @@ def shear_fdtd(
     traces ``(n_traces, n_steps)``) and ``return_device`` (torch CUDA tensors
     instead of numpy arrays).
 
-    Additional opts: ``precision`` ("mixed" default, or "fp64"), ``kahan``
-    (True), ``step_kernel`` ("tma" default, or "direct"), ``xchunk`` (planes
+    Additional opts: ``precision`` ("mixed" default, or "fp64"), ``projection``
+    ("auto" default: the reference's CG for fp64, and for mixed the exact
+    direct spectral Poisson solve when ``poisson_tol <= 1e-8``; or "cg" /
+    "spectral" explicitly), ``kahan`` (True), ``step_kernel`` ("tma" default, or "direct"), ``xchunk`` (planes
     per tile along x, 0 = automatic), ``force_terms`` (extra separable terms:
     list of ``((bx, by, bz), env)``), ``snapshot_stride`` (alias of the
     keyword), ``info`` (dict filled with CG statistics, phase times and a
@@ -692,7 +728,7 @@ def _solve_alone(sv: _Solve, callback, return_device):
         print("Pre-computing Helmholtz projection (separable force)...")
     for k, comps in sv.separable_inputs():
         st = _project_raw(ws, dtype_code(sv.dt), comps, (ny * nz, nz, 1), sv.shape, dX, dY, dZ,
-                          sv.tol, sv.max_iters)
+                          sv.tol, sv.max_iters, sv.method)
         sv.cg_log.append(st)
         sv.store_pattern(k, ws.out)
     sv.build_terms()
@@ -747,6 +783,14 @@ def _run_batch_group(solves):
     jobs, owners, bufs = [], [], []
     for sv in solves:
         nx, ny, nz = sv.shape
+        if sv.method == "spectral":  # direct solves: one after another, each ~1 ms
+            ws = _Workspace(nx, ny, nz, dev)
+            for k, comps in sv.separable_inputs():
+                st = _project_raw(ws, dtype_code(sv.dt), comps, (ny * nz, nz, 1), sv.shape,
+                                  *sv.spacing, sv.tol, sv.max_iters, "spectral")
+                sv.cg_log.append(st)
+                sv.store_pattern(k, ws.out)
+            continue
         for k, comps in sv.separable_inputs():
             ws = _Workspace(nx, ny, nz, dev)
             j = _native.ProjectJob()

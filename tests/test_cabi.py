@@ -52,3 +52,38 @@ def test_library_is_in_tree_and_built_for_sm100a():
     assert path.parent.parent.name == "shearwave_b200"
     # the descriptor layout used by ctypes matches the C header's field order
     assert ctypes.sizeof(native.FdtdDesc) > 0
+
+
+def test_spectral_basis_diagonalises_the_projection_operator():
+    """Host-side basis of the direct Poisson solve: Q^T A_1 Q = diag(lam), Q orthonormal.
+
+    A_1 is the reference's 1-D operator -div_c(grad_c .) with both
+    differences zero on the shell (src/shearwave/solver.py:708-729,
+    1024-1026), built here column by column.
+    """
+    import numpy as np
+
+    lib = native.load()
+
+    def a1(n, h):
+        m = n - 2
+        A = np.zeros((m, m))
+        for col in range(m):
+            x = np.zeros(n)
+            x[col + 1] = 1.0
+            g = np.zeros(n)
+            g[1:-1] = (x[2:] - x[:-2]) / (2 * h)
+            d = np.zeros(n)
+            d[1:-1] = (g[2:] - g[:-2]) / (2 * h)
+            A[:, col] = -d[1:-1]
+        return A
+
+    for n in (4, 5, 6, 7, 10, 11, 64, 65, 130):
+        m = n - 2
+        Q = np.zeros(m * m)
+        lam = np.zeros(m)
+        assert lib.sw_spectral_basis(n, 0.5e-3, Q.ctypes.data, lam.ctypes.data) == 0
+        Q = Q.reshape(m, m)
+        A = a1(n, 0.5e-3)
+        assert np.abs(Q.T @ Q - np.eye(m)).max() < 1e-13
+        assert np.abs(Q.T @ A @ Q - np.diag(lam)).max() / np.abs(A).max() < 1e-13

@@ -156,6 +156,26 @@ size_t sw_project_batch_table_bytes(int n);
 int sw_project_batch(const sw_project_job* jobs, int n, void* table, size_t table_bytes,
                      sw_cg_stats* stats, void* stream);
 
+/* sw_project for callers that cannot allocate device memory.  No counterpart
+ * in the reference: it exists for hosts that give the library nothing but
+ * their own input and output buffers (applications whose device memory is
+ * reserved up front by their own pool or budget and may not grow, bindings
+ * with no way to allocate a device workspace).  Same arguments, solve and
+ * results as sw_project, without the workspace: the CG scratch is a fixed
+ * array of sw_project_noalloc_scratch_bytes() (32 MiB) compiled into the
+ * library, resident on every GPU that loads it until the process exits.
+ * Grids whose scratch would not fit (more than about 0.7 million padded
+ * cells) are rejected with SW_ERANGE.  The array's device address is looked
+ * up on the first call made on each device, so make that first call before
+ * any stream capture.  Every call shares the array: calls whose work
+ * overlaps on the GPU (e.g. on two streams) race and corrupt each other.
+ * Nothing is allocated: no cudaMalloc, no cudaFree, no heap. */
+size_t sw_project_noalloc_scratch_bytes(void);
+int sw_project_noalloc(int in_dtype, const void* fx, const void* fy, const void* fz,
+                       int64_t in_sx, int64_t in_sy, int64_t in_sz, int nx, int ny, int nz,
+                       double dX, double dY, double dZ, double tol, int max_iters, double* out,
+                       sw_cg_stats* stats, void* stream);
+
 /* dst = src * scale / rho (rho NULL: dst = src * scale) for `ncomp` padded FP64
  * components into `dst` (dtype out_dtype, element (x,y,z) of component c at
  * c*dst_cs + x*dst_sx + y*dst_sy + z*dst_sz).  rho is dense or strided like

@@ -16,6 +16,7 @@ LIB_PATH = Path(__file__).resolve().parent / "_lib" / "libshearwave_b200.so"
 SW_F32, SW_F64 = 0, 1
 SW_PLAIN_F64, SW_MIXED_F32 = 0, 1
 SW_OK, SW_EINVAL, SW_ECUDA, SW_ENONFINITE, SW_ERANGE, SW_EWORKSPACE = range(6)
+SW_CG_CONVERGED = 1
 CG_REASONS = {0: "running", 1: "converged", 2: "breakdown", 3: "nonfinite", 4: "max_iters",
               5: "early_exit"}
 
@@ -97,6 +98,10 @@ _SIGNATURES = {
                              C.c_int, _f64, _f64, _f64, _vp, _vp, _sz, C.POINTER(CGStats), _vp],
                             C.c_int),
     "sw_spectral_basis": ([C.c_int, _f64, _vp, _vp], C.c_int),
+    "sw_project_noalloc_scratch_bytes": ([], _sz),
+    "sw_project_noalloc": ([C.c_int, _vp, _vp, _vp, _i64, _i64, _i64, C.c_int, C.c_int,
+                            C.c_int, _f64, _f64, _f64, _f64, C.c_int, _vp, C.POINTER(CGStats),
+                            _vp], C.c_int),
     "sw_project_batch_table_bytes": ([C.c_int], _sz),
     "sw_project_batch": ([C.POINTER(ProjectJob), C.c_int, _vp, _sz, C.POINTER(CGStats), _vp],
                          C.c_int),

@@ -349,10 +349,12 @@ int cg_run(const CgInst* d_tab, int ninst, int ntiles, CgState* d_states, int ns
   // instance's exit reason (one small D2H copy of the contiguous state
   // array) and stop when all are done.
   const int grid = std::max(1, std::min(ntiles, 148 * 8));
-  std::vector<CgState> h(nst);
+  CgState local[4];  // a single solve polls without touching the heap
+  std::vector<CgState> heap(nst > 4 ? nst : 0);
+  CgState* h = nst > 4 ? heap.data() : local;
   int batch = 4;
   for (;;) {
-    cudaError_t e = cudaMemcpyAsync(h.data(), d_states, nst * sizeof(CgState),
+    cudaError_t e = cudaMemcpyAsync(h, d_states, nst * sizeof(CgState),
                                     cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return cuda_status(e, "cg state readback");

@@ -193,8 +193,10 @@ typedef struct sw_fdtd_desc {
   double dX, dY, dZ, dT, vel_damp;
   /* SW_PLAIN_F64: state[0..2] are three rotating FP64 buffers of 3 padded
    *   components (u_prev, u_curr, u_next).
-   * SW_MIXED_F32: state[0], state[1] are two FP32 buffers of 9 padded
-   *   components (u, d = u - u_prev, Kahan compensation c), ping-ponged. */
+   * SW_MIXED_F32: state[0..2] are three FP32 buffers of 9 padded
+   *   components (u, d = u - u_prev, Kahan compensation c); the state after
+   *   t steps is in buffer t mod 3 (a kernel fusing two steps reads one
+   *   buffer and writes another). */
   void* state[3];
   /* Material coefficients, padded, written by sw_fdtd_materials:
    *   F64: coef_m = mu/rho, coef_e = eta/rho (NULL: no viscosity), inv_rho = 1/rho.

@@ -13,7 +13,9 @@
 // Two forms:
 //  * plain FP64 (SW_PLAIN_F64): state u_prev / u_curr / u_next in three
 //    rotating FP64 buffers, the reference's arithmetic in FP64.
-//  * mixed FP32 (SW_MIXED_F32): state (u, d = u_c - u_p, c) in FP32 with
+//  * mixed FP32 (SW_MIXED_F32): state (u, d = u_c - u_p, c) in FP32, three
+//    rotating buffers (the state after t steps in buffer t mod 3, so a kernel
+//    that fuses two steps never writes the buffer it reads), with
 //    d_n = (1 - vd) (d + m' L7(u) + e' L7(d) + sum_j s_j P_j),
 //    m' = dT^2 mu/rho, e' = dT eta/rho, P_j = dT^2 f_S/rho, and the
 //    displacement accumulated as u_n = u + d_n with Kahan compensation c.
@@ -83,7 +85,8 @@ int make_step_args(const sw_fdtd_desc* d, StepArgs* a) {
   a->flags = d->flags;
   a->kernel = d->kernel;
   a->xchunk = d->xchunk;
-  const int nbuf = d->precision == SW_PLAIN_F64 ? 3 : 2;
+  a->steps_per_pass = d->steps_per_pass;
+  const int nbuf = 3;
   for (int i = 0; i < nbuf; ++i)
     if (a->state[i] == nullptr) {
       set_error("descriptor: state[%d] is null", i);
@@ -157,15 +160,17 @@ __global__ void init_kernel(StepArgs a, const T* __restrict__ iu, const T* __res
         b2[c * g.ncell + i] = 0.0;
       } else {
         float* s0 = (float*)a.state[0];
-        float* s1 = (float*)a.state[1];
         // d = u_curr - u_prev: dT v with initial_v, u_curr without it
         const double d0 = iv ? a.dT * v0 : u0;
         s0[c * g.ncell + i] = (float)u0;
         s0[(3 + c) * g.ncell + i] = in ? (float)d0 : 0.0f;
         s0[(6 + c) * g.ncell + i] = 0.0f;
-        s1[c * g.ncell + i] = 0.0f;
-        s1[(3 + c) * g.ncell + i] = 0.0f;
-        s1[(6 + c) * g.ncell + i] = 0.0f;
+        for (int b = 1; b < 3; ++b) {
+          float* sb = (float*)a.state[b];
+          sb[c * g.ncell + i] = 0.0f;
+          sb[(3 + c) * g.ncell + i] = 0.0f;
+          sb[(6 + c) * g.ncell + i] = 0.0f;
+        }
       }
     }
   }
@@ -245,8 +250,8 @@ __global__ void __launch_bounds__(TILE_THREADS) step_f64(const __grid_constant__
 __global__ void __launch_bounds__(TILE_THREADS) step_f32(const __grid_constant__ StepArgs a,
                                                          int it) {
   const Geom& g = a.g;
-  const float* __restrict__ S = (const float*)a.state[it & 1];
-  float* __restrict__ D = (float*)a.state[(it + 1) & 1];
+  const float* __restrict__ S = (const float*)a.state[it % 3];
+  float* __restrict__ D = (float*)a.state[(it + 1) % 3];
   const float* __restrict__ mr = (const float*)a.coef_m;
   const float* __restrict__ er = (const float*)a.coef_e;
   const float* __restrict__ pat = (const float*)a.patterns;
@@ -317,7 +322,7 @@ __global__ void trace_kernel(const __grid_constant__ StepArgs a, int it) {
       const double* un = (const double*)a.state[(it + 2) % 3];
       ((double*)a.traces)[(long long)k * a.n_steps + it] = un[i];
     } else {
-      const float* D = (const float*)a.state[(it + 1) & 1];
+      const float* D = (const float*)a.state[(it + 1) % 3];
       ((float*)a.traces)[(long long)k * a.n_steps + it] = D[i];
     }
   }
@@ -342,7 +347,7 @@ __global__ void finish_kernel(StepArgs a, int done, void* uo, void* vo) {
         if (uo) ((double*)uo)[3 * q + c] = cu;
         if (vo) ((double*)vo)[3 * q + c] = (cu - up[c * g.ncell + i]) / a.dT;
       } else {
-        const float* S = (const float*)a.state[done & 1];
+        const float* S = (const float*)a.state[done % 3];
         if (uo) ((float*)uo)[3 * q + c] = S[c * g.ncell + i];
         if (vo) ((float*)vo)[3 * q + c] = S[(3 + c) * g.ncell + i] / (float)a.dT;
       }
@@ -516,7 +521,7 @@ extern "C" int sw_fdtd_reproject(const sw_fdtd_desc* d, int32_t steps_done, doub
     }
   } else {
     // project u and the increment d (= P(u_curr) - P(u_prev) by linearity)
-    float* S = (float*)a.state[steps_done & 1];
+    float* S = (float*)a.state[steps_done % 3];
     for (int k = 0; k < 2; ++k) {
       float* b = S + (long long)(3 * k) * g.ncell;
       rc = project_field(SW_F32, b, b + g.ncell, b + 2 * g.ncell, st, g, d->dX, d->dY, d->dZ, tol,

@@ -27,8 +27,9 @@ struct StepArgs {
   const int* trace_cells;
   void* traces;
   int* flags;
-  int kernel;  // 0 TMA-staged, 1 direct loads
-  int xchunk;  // requested planes per tile (0 automatic)
+  int kernel;          // 0 TMA-staged, 1 direct loads
+  int xchunk;          // requested planes per tile (0 automatic)
+  int steps_per_pass;  // mixed form: 1 one step per launch, 2 (or 0 = auto) two
 };
 
 int make_step_args(const sw_fdtd_desc* d, StepArgs* a);

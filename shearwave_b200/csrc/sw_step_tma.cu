@@ -75,51 +75,6 @@ int encode_tmap_4d(CUtensorMap* map, CUtensorMapDataType dt, void* base, const u
 // ---------------------------------------------------------------------------
 // pipeline helpers
 // ---------------------------------------------------------------------------
-// mbarrier arrive (no transaction), used by consumer warps to free a stage.
-__device__ inline void mbar_arrive(uint64_t* bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
-}
-
-// Shared-memory header of the warp-specialised kernels (first 128 bytes).
-struct WsHeader {
-  uint64_t fullA[4], emptyA[4], fullB[4], emptyB[4];  // 128 bytes
-};
-
-// A bounded wait that also gives up as soon as another thread has aborted.
-__device__ inline bool ws_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag) {
-  if (mbar_try_wait(bar, parity)) return true;
-  const long long t0 = clock64();
-  while (!mbar_try_wait(bar, parity)) {
-    if (*abort_flag) return false;
-    if (clock64() - t0 > 4000000000LL) {
-      *abort_flag = 1;
-      return false;
-    }
-  }
-  return true;
-}
-
-// Resolve the tile's instance and local step; false if the tile is idle.
-template <typename Inst, bool BATCH>
-__device__ inline bool resolve_tile(const Inst& one, const Inst* __restrict__ tab, int ninst,
-                                    int t, int it, const Inst*& in, int& local, int& lit) {
-  if (BATCH) {
-    int lo = 0, hi = ninst - 1;
-    while (lo < hi) {
-      int mid = (lo + hi + 1) >> 1;
-      if (tab[mid].tile_base <= t) lo = mid;
-      else hi = mid - 1;
-    }
-    in = &tab[lo];
-    local = t - in->tile_base;
-  } else {
-    in = &one;
-    local = t;
-  }
-  lit = it - in->it_begin;
-  return lit >= 0 && lit < in->n_steps;
-}
-
 // ---------------------------------------------------------------------------
 // mixed FP32 step: warp-specialised TMA pipeline
 // ---------------------------------------------------------------------------
@@ -166,8 +121,8 @@ __global__ void __launch_bounds__(TmaF32::THREADS, 2)
         int local, lit;
         if (!resolve_tile<TmaF32, BATCH>(one, tab, ninst, t, it, in, local, lit)) continue;
         const TileCoord tc = tile_coord_t(in->g, in->ts, local, TZ, TY);
-        const CUtensorMap* tma = &in->tm[lit & 1];
-        const CUtensorMap* tmc = &in->tmc[lit & 1];
+        const CUtensorMap* tma = &in->tm[lit % 3];
+        const CUtensorMap* tmc = &in->tmc[lit % 3];
         const uint32_t bbytes = (in->kahan ? TmaF32::C_BYTES : 0) + TZ * TY * 4 * in->ncoef;
         for (int p = tc.x0 - 1; p <= tc.x1 && !*abort_flag; ++p) {
           const int sa = pa % NA;
@@ -198,8 +153,8 @@ __global__ void __launch_bounds__(TmaF32::THREADS, 2)
       if (!resolve_tile<TmaF32, BATCH>(one, tab, ninst, t, it, in, local, lit)) continue;
       const Geom& g = in->g;
       const TileCoord tc = tile_coord_t(g, in->ts, local, TZ, TY);
-      const float* __restrict__ S = in->state[lit & 1];
-      float* __restrict__ D = in->state[(lit + 1) & 1];
+      const float* __restrict__ S = in->state[lit % 3];
+      float* __restrict__ D = in->state[(lit + 1) % 3];
       const int y = tc.y0 + ly;
       const bool yin = (y >= 1 && y <= g.ny - 2);
       const int z0 = tc.z0 + lane, z1 = z0 + 32;
@@ -568,7 +523,7 @@ int make_tma_f32(const StepArgs& a, int xchunk, TmaF32* t) {
                                (uint64_t)a.g.ncell * 4};
   const uint32_t box_halo[4] = {TmaF32::W, TmaF32::H, 1, 6};
   const uint32_t box_pt[4] = {TmaF32::TZ, TmaF32::TY, 1, 3};
-  for (int b = 0; b < 2; ++b) {
+  for (int b = 0; b < 3; ++b) {
     t->state[b] = (float*)a.state[b];
     rc = encode_tmap_4d(&t->tm[b], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, a.state[b], dims, strides,
                         box_halo);
@@ -659,13 +614,34 @@ int launch_steps_tma(const StepArgs& a, int xchunk, int it0, int nsteps, cudaStr
     for (int it = it0; it < it0 + nsteps; ++it)
       step_f64_tma<false><<<grid, TmaF64::THREADS, smem, s>>>(t, nullptr, 1, t.ts.count, it);
   } else {
+    // two steps per launch where two remain, one step otherwise
+    const bool fuse = a.steps_per_pass != 1 && nsteps >= 2;
     TmaF32 t;
     rc = make_tma_f32(a, xchunk, &t);
     if (rc != SW_OK) return rc;
     if (t.ts.count == 0) return SW_OK;
+    TmaF32TB tb;
+    if (fuse) {
+      rc = make_tma_f32_tb(a, 0, &tb);
+      if (rc != SW_OK) return rc;
+      rc = launch_fused2_prepare();
+      if (rc != SW_OK) return rc;
+    }
     const int grid = std::min(t.ts.count, 148 * 2);
-    for (int it = it0; it < it0 + nsteps; ++it)
-      step_f32_tma<false><<<grid, TmaF32::THREADS, smem, s>>>(t, nullptr, 1, t.ts.count, it);
+    unsigned long long n_launch = 0;
+    for (int it = it0; it < it0 + nsteps;) {
+      if (fuse && it + 1 < it0 + nsteps) {
+        launch_fused2_raw(tb, it, s);
+        it += 2;
+      } else {
+        step_f32_tma<false><<<grid, TmaF32::THREADS, smem, s>>>(t, nullptr, 1, t.ts.count, it);
+        it += 1;
+      }
+      ++n_launch;
+    }
+    count_launches(n_launch);
+    SW_CHECK_LAUNCH("step (tma)");
+    return SW_OK;
   }
   count_launches((unsigned long long)nsteps);
   SW_CHECK_LAUNCH("step (tma)");
@@ -751,6 +727,93 @@ int build_batch<TmaF64>(const sw_fdtd_desc* descs, const int32_t* begins, int n,
   return SW_OK;
 }
 
+// Mixed form: two steps per launch whenever every running solve runs both
+// steps of the pair; one-step launches around starts and ends.  The table
+// holds the one-step instance array, then the fused-kernel array.
+int batch_steps_mixed(const sw_fdtd_desc* descs, const int32_t* begins, int n, int it0,
+                      int nsteps, void* table, cudaStream_t s) {
+  char* tab_single = (char*)table;
+  char* tab_fused = (char*)table + (size_t)n * sizeof(TmaF32);
+  bool fuse_ok = true;
+  for (int i = 0; i < n; ++i) fuse_ok &= (descs[i].steps_per_pass != 1);
+  auto active = [&](int i, int it) {
+    const int lit = it - (begins ? begins[i] : 0);
+    return lit >= 0 && lit < descs[i].n_steps;
+  };
+  std::vector<int> cur(n, -1);
+  int cur_kind = -1;  // 0 single, 1 fused
+  std::vector<TmaF32> tsingle;
+  std::vector<TmaF32TB> tfused;
+  int ntiles = 0;
+  if (fuse_ok) {
+    int rc = launch_fused2_prepare();
+    if (rc != SW_OK) return rc;
+  }
+  const int end = it0 + nsteps;
+  for (int it = it0; it < end;) {
+    bool any = false, pair = fuse_ok && it + 1 < end;
+    for (int i = 0; i < n; ++i) {
+      const bool a0 = active(i, it);
+      any |= a0;
+      if (pair && a0 != active(i, it + 1)) pair = false;
+    }
+    if (!any) {
+      ++it;
+      continue;
+    }
+    const int kind = pair ? 1 : 0;
+    bool rebuild = kind != cur_kind;
+    for (int i = 0; i < n && !rebuild; ++i) rebuild = (cur[i] != (active(i, it) ? 1 : 0));
+    if (rebuild) {
+      tsingle.clear();
+      tfused.clear();
+      ntiles = 0;
+      for (int i = 0; i < n; ++i) {
+        cur[i] = active(i, it) ? 1 : 0;
+        if (!cur[i]) continue;
+        StepArgs a;
+        int rc = make_step_args(&descs[i], &a);
+        if (rc != SW_OK) return rc;
+        if (kind == 1) {
+          TmaF32TB t;
+          rc = make_tma_f32_tb(a, descs[i].xchunk > 0 ? descs[i].xchunk : 24, &t);
+          if (rc != SW_OK) return rc;
+          t.it_begin = begins ? begins[i] : 0;
+          t.tile_base = ntiles;
+          ntiles += t.ts.count;
+          tfused.push_back(t);
+        } else {
+          TmaF32 t;
+          rc = make_tma_f32(a, descs[i].xchunk > 0 ? descs[i].xchunk : 16, &t);
+          if (rc != SW_OK) return rc;
+          t.it_begin = begins ? begins[i] : 0;
+          t.tile_base = ntiles;
+          ntiles += t.ts.count;
+          tsingle.push_back(t);
+        }
+      }
+      cudaError_t e = kind == 1 ? cudaMemcpyAsync(tab_fused, tfused.data(),
+                                                  tfused.size() * sizeof(TmaF32TB),
+                                                  cudaMemcpyHostToDevice, s)
+                                : cudaMemcpyAsync(tab_single, tsingle.data(),
+                                                  tsingle.size() * sizeof(TmaF32),
+                                                  cudaMemcpyHostToDevice, s);
+      if (e != cudaSuccess) return cuda_status(e, "batch table upload");
+      cur_kind = kind;
+    }
+    int rc;
+    if (kind == 1) {
+      rc = launch_fused2_batch(tab_fused, (int)tfused.size(), ntiles, it, s);
+      it += 2;
+    } else {
+      rc = launch_steps_tma_batch(SW_MIXED_F32, tab_single, (int)tsingle.size(), ntiles, it, s);
+      it += 1;
+    }
+    if (rc != SW_OK) return rc;
+  }
+  return SW_OK;
+}
+
 template <typename Inst>
 int batch_steps(int precision, const sw_fdtd_desc* descs, const int32_t* begins, int n, int it0,
                 int nsteps, void* table, cudaStream_t s) {
@@ -794,7 +857,7 @@ using namespace sw;
 
 extern "C" size_t sw_fdtd_batch_table_bytes(int n) {
   if (n <= 0) return 0;
-  return (size_t)n * std::max(sizeof(TmaF32), sizeof(TmaF64));
+  return (size_t)n * std::max(sizeof(TmaF32) + sizeof(TmaF32TB), sizeof(TmaF64));
 }
 
 extern "C" int sw_fdtd_batch_steps(const sw_fdtd_desc* descs, const int32_t* begins, int n,
@@ -820,5 +883,5 @@ extern "C" int sw_fdtd_batch_steps(const sw_fdtd_desc* descs, const int32_t* beg
   cudaStream_t s = (cudaStream_t)stream;
   if (prec == SW_PLAIN_F64)
     return batch_steps<TmaF64>(prec, descs, begins, n, it0, nsteps, table, s);
-  return batch_steps<TmaF32>(prec, descs, begins, n, it0, nsteps, table, s);
+  return batch_steps_mixed(descs, begins, n, it0, nsteps, table, s);
 }

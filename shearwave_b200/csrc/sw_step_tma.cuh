@@ -10,7 +10,7 @@ namespace sw {
 
 constexpr int round128(int bytes) { return (bytes + 127) / 128 * 128; }
 
-// Kernel-side view of one mixed-form solve.
+// Kernel-side view of one mixed-form solve (state after t steps in buffer t mod 3).
 //   tm[b]  : state buffer b as a 4-D tensor (pz, ny, nx, 9 components);
 //            box (W, H, 1, 6) = the halo'd u and d of one plane
 //   tmc[b] : the same tensor, box (TZ, TY, 1, 3) = the Kahan compensation
@@ -28,12 +28,12 @@ struct TmaF32 {
   static constexpr int B_STAGE = round128(C_BYTES) + round128(M_BYTES);
   static constexpr int CONSUMER_WARPS = TY;
   static constexpr int THREADS = 32 * (CONSUMER_WARPS + 1);
-  CUtensorMap tm[2];
-  CUtensorMap tmc[2];
+  CUtensorMap tm[3];
+  CUtensorMap tmc[3];
   CUtensorMap tmm;
   Geom g;
   TileSpace ts;
-  float* state[2];
+  float* state[3];
   const float* pat;
   const int* term_off;
   const int* term_pat;
@@ -81,7 +81,56 @@ struct TmaF64 {
   int tile_base;
 };
 
+// Kernel-side view of one mixed-form solve for the two-steps-per-pass kernel.
+// Step t+1 is computed on an LZ x LY region (the output tile plus one cell of
+// halo), step t+2 on the OZ x OY output tile.  Output tiles start at z = 1 +
+// 62 k and y = 1 + 6 k; the TMA boxes start at the 16-byte aligned z at or
+// below the region they cover, and the kernel indexes from that offset.
+//   tm[b]  : state buffer b (pz, ny, nx, 9), box (W, H, 1, 6): u and d with
+//            two cells of halo around the output tile
+//   tmc[b] : state buffer b, box (WB, HB, 1, 3) at component 6: Kahan c on
+//            the step-(t+1) region
+//   tmm    : coefficients (pz, ny, nx, ncoef), box (WB, HB, 1, ncoef)
+struct TmaF32TB {
+  static constexpr int OZ = 62, OY = 6;   // output tile (z, y)
+  static constexpr int LZ = 64, LY = 8;   // step-(t+1) region
+  static constexpr int W = 72, H = OY + 4;
+  static constexpr int WB = 72, HB = LY;
+  static constexpr int NA = 4, NB = 2, NL = 4;  // ring stages: level 0, point data, level 1
+  static constexpr int A_BYTES = W * H * 6 * 4;
+  static constexpr int C_BYTES = WB * HB * 3 * 4;
+  static constexpr int M_BYTES = WB * HB * 2 * 4;
+  static constexpr int A_STAGE = round128(A_BYTES);
+  static constexpr int B_STAGE = round128(C_BYTES) + round128(M_BYTES);
+  static constexpr int L_STAGE = round128(LZ * LY * 6 * 4);
+  static constexpr int CONSUMER_WARPS = LY;
+  static constexpr int THREADS = 32 * (CONSUMER_WARPS + 1);
+  CUtensorMap tm[3];
+  CUtensorMap tmc[3];
+  CUtensorMap tmm;
+  Geom g;
+  TileSpace ts;  // z tiles of OZ, y tiles of OY, x chunks
+  float* state[3];
+  const float* pat;
+  const int* term_off;
+  const int* term_pat;
+  const double* term_scale;
+  float hx, hy, hz, damp;
+  int ncoef;
+  int use_damp, kahan, n_steps, snap_stride;
+  float* snaps;
+  int* flags;
+  int it_begin;
+  int tile_base;
+};
+
 size_t tma_smem_bytes(int precision);
+size_t tb_smem_bytes();
+int make_tma_f32_tb(const StepArgs& a, int xchunk, TmaF32TB* t);
+int launch_fused2(const StepArgs& a, int xchunk, int it, cudaStream_t s);
+int launch_fused2_prepare();                                   // kernel attributes, once
+void launch_fused2_raw(const TmaF32TB& t, int it, cudaStream_t s);  // enqueue one launch
+int launch_fused2_batch(const void* d_tab, int ninst, int ntiles, int it, cudaStream_t s);
 int tma_xchunk(const Geom& g, int tz, int ty, long long want_tiles);
 int make_tma_f32(const StepArgs& a, int xchunk, TmaF32* t);
 int make_tma_f64(const StepArgs& a, int xchunk, TmaF64* t);

@@ -74,6 +74,70 @@ __device__ inline void prefetch_tmap(const CUtensorMap* map) {
   asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(map)) : "memory");
 }
 
+// ---------------------------------------------------------------------------
+// warp-specialised pipeline pieces shared by the step kernels
+// ---------------------------------------------------------------------------
+// mbarrier arrive (no transaction), used by consumer warps to free a stage.
+__device__ inline void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
+// Shared-memory header of the warp-specialised kernels (first 128 bytes).
+struct WsHeader {
+  uint64_t fullA[4], emptyA[4], fullB[4], emptyB[4];  // 128 bytes
+};
+
+// A bounded wait that also gives up as soon as another thread has aborted.
+__device__ inline bool ws_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const long long t0 = clock64();
+  while (!mbar_try_wait(bar, parity)) {
+    if (*abort_flag) return false;
+    if (clock64() - t0 > 4000000000LL) {
+      *abort_flag = 1;
+      return false;
+    }
+  }
+  return true;
+}
+
+// Resolve the tile's instance and local step; false if the tile is idle.
+template <typename Inst, bool BATCH>
+__device__ inline bool resolve_tile(const Inst& one, const Inst* __restrict__ tab, int ninst,
+                                    int t, int it, const Inst*& in, int& local, int& lit) {
+  if (BATCH) {
+    int lo = 0, hi = ninst - 1;
+    while (lo < hi) {
+      int mid = (lo + hi + 1) >> 1;
+      if (tab[mid].tile_base <= t) lo = mid;
+      else hi = mid - 1;
+    }
+    in = &tab[lo];
+    local = t - in->tile_base;
+  } else {
+    in = &one;
+    local = t;
+  }
+  lit = it - in->it_begin;
+  return lit >= 0 && lit < in->n_steps;
+}
+
+// Barrier among the consumer warps only (named barrier 1, `nthreads`
+// threads), reducing a failure flag: returns true in every participant when
+// any participant passed true.  The producer warp never joins it.
+__device__ inline bool consumer_sync_or(bool fail, int nthreads) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.u32 p, %1, 0;\n\t"
+      "bar.red.or.pred q, 1, %2, p;\n\t"
+      "selp.u32 %0, 1, 0, q;\n\t}"
+      : "=r"(r)
+      : "r"((uint32_t)fail), "r"(nthreads)
+      : "memory");
+  return r != 0u;
+}
+
 // Host: encode a 4-D tiled tensor map (dims innermost first, strides in
 // bytes for dims 1..3).  Returns a CUDA driver status.
 int encode_tmap_4d(CUtensorMap* map, CUtensorMapDataType dt, void* base, const uint64_t dims[4],

@@ -357,7 +357,7 @@ class _Run:
         d.dT = dT
         d.kahan = 1 if kahan else 0
         self.desc = d
-        nbuf, ncomp = (3, 3) if prec == _native.SW_PLAIN_F64 else (2, 9)
+        nbuf, ncomp = (3, 3) if prec == _native.SW_PLAIN_F64 else (3, 9)
         self.state = torch.empty((nbuf, ncomp, self.ncell), dtype=self.dt, device=dev)
         for i in range(nbuf):
             d.state[i] = self.state[i].data_ptr()
@@ -526,6 +526,10 @@ class _Solve:
         run.desc.vel_damp = float(opts.get("vel_damp", 0.0))
         run.desc.kernel = 0 if kern == "tma" else 1
         run.desc.xchunk = int(opts.get("xchunk", 0) or 0)
+        spp = int(opts.get("steps_per_pass", 0) or 0)
+        if spp not in (0, 1, 2):
+            raise ValueError("steps_per_pass must be 1 or 2 (0 = automatic)")
+        run.desc.steps_per_pass = spp
         run.materials(rho, mu, eta, dt)
         iu = iv = None
         if opts.get("initial_u") is not None:
@@ -704,7 +708,9 @@ def shear_fdtd(
     ("auto" default: the reference's CG for fp64, and for mixed the exact
     direct spectral Poisson solve when ``poisson_tol <= 1e-8``; or "cg" /
     "spectral" explicitly), ``kahan`` (True), ``step_kernel`` ("tma" default, or "direct"), ``xchunk`` (planes
-    per tile along x, 0 = automatic), ``force_terms`` (extra separable terms:
+    per tile along x, 0 = automatic), ``steps_per_pass`` (mixed form: 2
+    fuses two time steps per pass over HBM, the default; 1 one step per
+    launch), ``force_terms`` (extra separable terms:
     list of ``((bx, by, bz), env)``), ``snapshot_stride`` (alias of the
     keyword), ``info`` (dict filled with CG statistics, phase times and a
     non-finite flag).

@@ -82,3 +82,41 @@ def test_against_oracle(cuda, shape):
     for r, a, b in zip(ref, g64, g32):
         assert rel_l2(a, r) <= 1e-10
         assert rel_l2(b, r) <= 1e-4
+
+
+FUSED_GRIDS = [(5, 7, 9), (17, 13, 11), (3, 20, 70), (40, 9, 133), (12, 33, 65), (70, 16, 64)]
+
+
+@pytest.mark.parametrize("shape", FUSED_GRIDS)
+@pytest.mark.parametrize("kahan", [True, False])
+def test_two_steps_per_pass_matches_one(cuda, shape, kahan):
+    """The fused two-step kernel reproduces two one-step launches.
+
+    Odd n_steps (the last step runs alone), snapshots every 3 steps (both
+    parities of the fused pair), pushes, damping and viscosity.
+    """
+    p, opts = _problem(shape, seed=11 + sum(shape), n_steps=25)
+    opts = dict(opts, kahan=kahan)
+    import shearwave_b200 as sw
+
+    def run(spp):
+        return sw.shear_fdtd(p["bx"], p["by"], p["bz"], p["rho"], p["mu"], p["dX"], p["dY"],
+                             p["dZ"], p["dT"], p["n_steps"],
+                             dict(opts, precision="mixed", steps_per_pass=spp),
+                             snapshot_stride=5)
+
+    a, b = run(2), run(1)
+    for x, y in zip(a, b):
+        assert rel_l2(x, y) <= 1e-6
+
+
+def test_two_steps_per_pass_without_viscosity(cuda):
+    p, opts = _problem((30, 20, 90), seed=5, n_steps=16)
+    opts = dict(opts, eta=0.0)
+    import shearwave_b200 as sw
+
+    outs = [sw.shear_fdtd(p["bx"], p["by"], p["bz"], p["rho"], p["mu"], p["dX"], p["dY"], p["dZ"],
+                          p["dT"], p["n_steps"], dict(opts, steps_per_pass=spp))
+            for spp in (2, 1)]
+    for x, y in zip(*outs):
+        assert rel_l2(x, y) <= 1e-6

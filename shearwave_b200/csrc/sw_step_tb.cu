@@ -5,9 +5,9 @@
 //
 //   level 0  the state at step t, streamed by TMA: u and d of a plane with two
 //            cells of halo around the 62 x 6 output tile (one 72 x 10 x 1 x 6
-//            box per plane, 4-stage ring), and the point-wise data of the
-//            64 x 8 level-1 region (Kahan c, material coefficients; 2-stage
-//            ring);
+//            box per plane, 6-stage ring: three planes in use, three in
+//            flight), and the point-wise data of the 64 x 8 level-1 region
+//            (Kahan c, material coefficients; 4-stage ring);
 //   level 1  step t+1 on the 64 x 8 region (the output tile plus one cell of
 //            halo), written to a 4-slot shared-memory ring of planes;
 //   level 2  step t+2 on the output tile, read from the level-1 ring and
@@ -82,8 +82,8 @@ __global__ void __launch_bounds__(TmaF32TB::THREADS, 1)
   extern __shared__ unsigned char smem_raw[];
   unsigned char* base = smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u);
   WsHeader* hd = reinterpret_cast<WsHeader*>(base);
-  volatile int* abort_flag = reinterpret_cast<volatile int*>(base + 128);
-  float* ringA = reinterpret_cast<float*>(base + 256);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(base + kAbortFlagOffset);
+  float* ringA = reinterpret_cast<float*>(base + kRingOffset);
   float* ringB = ringA + NA * AF;
   float* ringL = ringB + NB * BF;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;

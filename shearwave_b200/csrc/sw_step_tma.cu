@@ -89,8 +89,8 @@ __global__ void __launch_bounds__(TmaF32::THREADS, 2)
   extern __shared__ unsigned char smem_raw[];
   unsigned char* base = smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u);
   WsHeader* hd = reinterpret_cast<WsHeader*>(base);
-  volatile int* abort_flag = reinterpret_cast<volatile int*>(base + 128);
-  float* ringA = reinterpret_cast<float*>(base + 256);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(base + kAbortFlagOffset);
+  float* ringA = reinterpret_cast<float*>(base + kRingOffset);
   float* ringB = ringA + NA * AF;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if ((smem_addr(ringA) & 127u) != 0u) {  // never issue a TMA to a misaligned destination
@@ -278,8 +278,8 @@ __global__ void __launch_bounds__(TmaF64::THREADS, 2)
   extern __shared__ unsigned char smem_raw[];
   unsigned char* base = smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u);
   WsHeader* hd = reinterpret_cast<WsHeader*>(base);
-  volatile int* abort_flag = reinterpret_cast<volatile int*>(base + 128);
-  double* ringA = reinterpret_cast<double*>(base + 256);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(base + kAbortFlagOffset);
+  double* ringA = reinterpret_cast<double*>(base + kRingOffset);
   double* ringB = ringA + NA * AD;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if ((smem_addr(ringA) & 127u) != 0u) {

@@ -96,7 +96,8 @@ struct TmaF32TB {
   static constexpr int LZ = 64, LY = 8;   // step-(t+1) region
   static constexpr int W = 72, H = OY + 4;
   static constexpr int WB = 72, HB = LY;
-  static constexpr int NA = 4, NB = 2, NL = 4;  // ring stages: level 0, point data, level 1
+  // ring stages: level 0 (3 planes in use, 3 in flight), point data, level 1
+  static constexpr int NA = 6, NB = 4, NL = 4;
   static constexpr int A_BYTES = W * H * 6 * 4;
   static constexpr int C_BYTES = WB * HB * 3 * 4;
   static constexpr int M_BYTES = WB * HB * 2 * 4;

@@ -82,10 +82,14 @@ __device__ inline void mbar_arrive(uint64_t* bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
 }
 
-// Shared-memory header of the warp-specialised kernels (first 128 bytes).
+// Shared-memory header of the warp-specialised kernels: the mbarriers at
+// offset 0, the abort flag at offset 192, the rings from offset 256.
 struct WsHeader {
-  uint64_t fullA[4], emptyA[4], fullB[4], emptyB[4];  // 128 bytes
+  uint64_t fullA[6], emptyA[6], fullB[4], emptyB[4];  // 160 bytes
 };
+static_assert(sizeof(WsHeader) <= 192, "header overlaps the abort flag");
+constexpr int kAbortFlagOffset = 192;
+constexpr int kRingOffset = 256;
 
 // A bounded wait that also gives up as soon as another thread has aborted.
 __device__ inline bool ws_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag) {

@@ -388,13 +388,14 @@ def main(argv=None) -> int:
     # launches one kernel per pair of time steps (one per single step at an
     # odd end); a batched run covers all running solves in each launch.
     # achieved = algorithmic bytes of the launches / their device time.
+    spl = 2 if a.steps_per_pass == 2 else 1
     if len(probs) > 1:
         step_ms = max(i["t_steps_ms"] for i in infos)
         steps_total = max(p["n_steps"] for p in probs)
     else:
         step_ms = infos[0]["t_steps_ms"]
         steps_total = probs[0]["n_steps"]
-    launches_step = (steps_total + 1) // 2
+    launches_step = (steps_total + spl - 1) // spl
     alg_bytes = 0.0
     for p, i in zip(probs, infos):
         nx, ny, nz = _shape(p)
@@ -406,8 +407,9 @@ def main(argv=None) -> int:
     traffic = ncu_traffic("step_f32", a.workload)
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
-            "kernel": "step_f32_fused2 (two KV steps per pass, mixed form)",
-            "steps_per_launch": 2,
+            "kernel": ("step_f32_fused2 (two KV steps per pass, mixed form)" if spl == 2
+                       else "step_f32_tma (fused KV step, mixed form)"),
+            "steps_per_launch": spl,
             "mean_launch_us": per_launch_ms * 1e3,
             "alg_bytes_per_launch": alg_bytes / launches_step,
             "step_only_gcell_steps_s": cs_rank / (step_ms / 1e3) / 1e9}

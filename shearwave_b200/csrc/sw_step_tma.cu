@@ -614,8 +614,9 @@ int launch_steps_tma(const StepArgs& a, int xchunk, int it0, int nsteps, cudaStr
     for (int it = it0; it < it0 + nsteps; ++it)
       step_f64_tma<false><<<grid, TmaF64::THREADS, smem, s>>>(t, nullptr, 1, t.ts.count, it);
   } else {
-    // two steps per launch where two remain, one step otherwise
-    const bool fuse = a.steps_per_pass != 1 && nsteps >= 2;
+    // steps_per_pass 2: two steps per launch where two remain, one step
+    // otherwise; 0 (automatic) and 1: one step per launch
+    const bool fuse = a.steps_per_pass == 2 && nsteps >= 2;
     TmaF32 t;
     rc = make_tma_f32(a, xchunk, &t);
     if (rc != SW_OK) return rc;
@@ -735,7 +736,7 @@ int batch_steps_mixed(const sw_fdtd_desc* descs, const int32_t* begins, int n, i
   char* tab_single = (char*)table;
   char* tab_fused = (char*)table + (size_t)n * sizeof(TmaF32);
   bool fuse_ok = true;
-  for (int i = 0; i < n; ++i) fuse_ok &= (descs[i].steps_per_pass != 1);
+  for (int i = 0; i < n; ++i) fuse_ok &= (descs[i].steps_per_pass == 2);
   auto active = [&](int i, int it) {
     const int lit = it - (begins ? begins[i] : 0);
     return lit >= 0 && lit < descs[i].n_steps;

@@ -709,7 +709,7 @@ def shear_fdtd(
     direct spectral Poisson solve when ``poisson_tol <= 1e-8``; or "cg" /
     "spectral" explicitly), ``kahan`` (True), ``step_kernel`` ("tma" default, or "direct"), ``xchunk`` (planes
     per tile along x, 0 = automatic), ``steps_per_pass`` (mixed form: 2
-    fuses two time steps per pass over HBM, the default; 1 one step per
+    fuses two time steps per pass over HBM; 1 or 0 (default) one step per
     launch), ``force_terms`` (extra separable terms:
     list of ``((bx, by, bz), env)``), ``snapshot_stride`` (alias of the
     keyword), ``info`` (dict filled with CG statistics, phase times and a

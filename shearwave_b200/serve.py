@@ -1,0 +1,345 @@
+"""Continuous-batching request loop for shear_fdtd solves on one GPU.
+
+Requests (dicts of ``shear_fdtd`` keyword arguments) arrive at any time.  A
+background thread owns the GPU: at every chunk boundary it admits waiting
+requests, in arrival order, while their device-memory footprint fits the
+budget and a slot is free; it then advances every running solve together
+(one batched launch per time step covers the tiles of all of them, each at
+its own step offset); solves that finish are copied out, their futures
+resolved and their memory returned to the budget.  Admission and completion
+happen between launches, so a request never waits for a whole batch to
+drain, and a solve's result is the same alone and in any mix: every cell of
+a batched launch runs the same kernel code as a solve run alone.
+
+The queue, admission and bookkeeping are plain Python over an engine with
+six methods (footprint, admit, advance, steps, finish, release); the GPU
+engine drives the CUDA library, and the test suite drives the same loop with
+a fake engine on the CPU.
+"""
+
+from __future__ import annotations
+
+import collections
+import math
+import threading
+import time
+from concurrent.futures import CancelledError, Future
+
+import numpy as np
+
+__all__ = ["GpuEngine", "ShearServer", "latency_percentiles"]
+
+
+def latency_percentiles(lat_s) -> dict:
+    """p50 / p95 / p99 / mean / max of a list of latencies (seconds)."""
+    if not lat_s:
+        return {"p50": None, "p95": None, "p99": None, "mean": None, "max": None, "n": 0}
+    a = np.asarray(lat_s, dtype=np.float64)
+    return {"p50": float(np.percentile(a, 50)), "p95": float(np.percentile(a, 95)),
+            "p99": float(np.percentile(a, 99)), "mean": float(a.mean()), "max": float(a.max()),
+            "n": int(a.size)}
+
+
+class _Request:
+    __slots__ = ("problem", "future", "t_arrive", "t_admit", "t_done", "footprint", "handle",
+                 "begin", "rid")
+
+    def __init__(self, problem, rid):
+        self.problem = problem
+        self.future = Future()
+        self.t_arrive = time.perf_counter()
+        self.t_admit = None
+        self.t_done = None
+        self.footprint = 0
+        self.handle = None
+        self.begin = 0
+        self.rid = rid
+
+
+class GpuEngine:
+    """The CUDA engine: one ``_Solve`` per admitted request, batched steps."""
+
+    def __init__(self, precision="mixed", return_device=False):
+        import torch
+
+        from . import _native
+        from ._device import require_cuda
+
+        self.torch = torch
+        self.native = _native
+        self.dev = require_cuda()
+        self.precision = precision
+        self.return_device = return_device
+        self.stream = torch.cuda.Stream(device=self.dev)
+
+    # -- sizes -------------------------------------------------------------
+    @staticmethod
+    def _shape(p):
+        ref = p["bx"] if p["bx"] is not None else (p["by"] if p["by"] is not None else p["bz"])
+        if ref is None:
+            raise ValueError("At least one body-force component must be provided.")
+        return tuple(int(s) for s in ref.shape[:3])
+
+    def footprint(self, p) -> int:
+        """Device bytes a request holds while it runs (state, materials,
+        force patterns, outputs and the projection's scratch)."""
+        nx, ny, nz = self._shape(p)
+        pz = (nz + 7) // 8 * 8
+        ncell = nx * ny * pz
+        es = 8 if (p.get("opts") or {}).get("precision", self.precision) == "fp64" else 4
+        nterms = 1 + len((p.get("opts") or {}).get("force_terms") or ())
+        state = 3 * (3 if es == 8 else 9) * ncell * es
+        coef = 2 * ncell * es
+        pats = nterms * 3 * ncell * es
+        outs = 2 * 3 * nx * ny * nz * es
+        scratch = 8 * ncell * 8  # projection vectors (FP64), freed after admission
+        return int(state + coef + pats + outs + scratch)
+
+    # -- lifecycle ---------------------------------------------------------
+    def on_thread_start(self):
+        """Make this engine's device current on the serving thread."""
+        self.torch.cuda.set_device(self.dev)
+        self.native.call("sw_set_device", self.dev.index)
+
+    def admit(self, p):
+        from .solver import _Solve, _Workspace, _project_raw, dtype_code
+
+        with self.torch.cuda.stream(self.stream):
+            opts = dict(p.get("opts") or {})
+            opts.setdefault("precision", self.precision)
+            kw = {k: p[k] for k in ("bx", "by", "bz", "rho", "mu", "dX", "dY", "dZ", "dT",
+                                    "n_steps")}
+            sv = _Solve(**kw, opts=opts, snapshot_stride=p.get("snapshot_stride"))
+            if sv.needs_per_step_host(None):
+                raise ValueError("the server runs batchable requests only (no 4-D forces, "
+                                 "reproject_every, verbose, traces or direct kernels)")
+            nx, ny, nz = sv.shape
+            ws = _Workspace(nx, ny, nz, sv.dev)
+            for k, comps in sv.separable_inputs():
+                st = _project_raw(ws, dtype_code(sv.dt), comps, (ny * nz, nz, 1), sv.shape,
+                                  *sv.spacing, sv.tol, sv.max_iters, sv.method)
+                sv.cg_log.append(st)
+                sv.store_pattern(k, ws.out)
+            sv.build_terms()
+            sv.mark_steps_begin()
+            return sv
+
+    @staticmethod
+    def steps(handle) -> int:
+        return handle.n_steps
+
+    def advance(self, handles, begins, clock, nsteps):
+        torch, native = self.torch, self.native
+        lib = native.load()
+        import ctypes as C
+
+        with torch.cuda.stream(self.stream):
+            groups = {}
+            for h, b in zip(handles, begins):
+                groups.setdefault(h.prec, []).append((h, b))
+            for items in groups.values():
+                n = len(items)
+                descs = (native.FdtdDesc * n)(*[h.run.desc for h, _ in items])
+                beg = (C.c_int32 * n)(*[b for _, b in items])
+                tb = int(lib.sw_fdtd_batch_table_bytes(n))
+                table = torch.empty(tb + 64, dtype=torch.uint8, device=self.dev)
+                base = (table.data_ptr() + 63) // 64 * 64
+                native.call("sw_fdtd_batch_steps", descs, beg, n, int(clock), int(nsteps), base,
+                            tb, self.stream.cuda_stream)
+
+    def finish(self, handle):
+        with self.torch.cuda.stream(self.stream):
+            return handle.finish(self.return_device)
+
+    @staticmethod
+    def release(handle):
+        del handle
+
+
+class ShearServer:
+    """Continuous-batching server: ``submit(problem) -> Future``.
+
+    ``hbm_budget``: device bytes the running requests may hold together
+    (150 GB by default); ``max_active``: running requests at most;
+    ``chunk_steps``: time steps between two admission / completion points.
+    Use as a context manager or call :meth:`start` / :meth:`stop`.
+    """
+
+    def __init__(self, engine=None, *, hbm_budget=150e9, max_active=64, chunk_steps=50,
+                 precision="mixed", return_device=False):
+        self.engine = engine if engine is not None else GpuEngine(precision, return_device)
+        self.hbm_budget = float(hbm_budget)
+        self.max_active = int(max_active)
+        self.chunk_steps = int(chunk_steps)
+        self._pending = collections.deque()
+        self._active = []
+        self._cv = threading.Condition()
+        self._stop = False
+        self._thread = None
+        self._clock = 0
+        self._used = 0
+        self._next_id = 0
+        self.completed = []  # (rid, latency_s, queue_s, cell_steps)
+        self.rejected = 0
+        self.failed = 0
+        self.busy_s = 0.0
+        self._t_start = None
+        self._error = None
+
+    # -- public API --------------------------------------------------------
+    def submit(self, problem) -> Future:
+        """Queue one request; the future resolves to the shear_fdtd result."""
+        fp = self.engine.footprint(problem)  # validates the force arguments
+        if fp > self.hbm_budget:
+            self.rejected += 1
+            raise MemoryError(
+                f"request needs {fp / 1e9:.2f} GB of device memory, above the "
+                f"{self.hbm_budget / 1e9:.2f} GB budget")
+        with self._cv:
+            if self._stop:
+                raise RuntimeError("server is stopped")
+            req = _Request(problem, self._next_id)
+            req.footprint = fp
+            self._next_id += 1
+            self._pending.append(req)
+            self._cv.notify()
+        return req.future
+
+    def start(self):
+        if self._thread is None:
+            self._t_start = time.perf_counter()
+            self._thread = threading.Thread(target=self._loop, name="shearwave-server",
+                                            daemon=True)
+            self._thread.start()
+        return self
+
+    def stop(self, wait=True):
+        with self._cv:
+            self._stop = True
+            self._cv.notify()
+        if wait and self._thread is not None:
+            self._thread.join()
+        if self._error is not None:
+            raise self._error
+
+    def __enter__(self):
+        return self.start()
+
+    def __exit__(self, *exc):
+        self.stop()
+
+    def stats(self) -> dict:
+        lat = [c[1] for c in self.completed]
+        queue = [c[2] for c in self.completed]
+        cells = sum(c[3] for c in self.completed)
+        wall = (time.perf_counter() - self._t_start) if self._t_start else 0.0
+        return {"completed": len(self.completed), "rejected": self.rejected,
+                "failed": self.failed, "latency_s": latency_percentiles(lat),
+                "queue_s": latency_percentiles(queue),
+                "gcell_steps_per_s": cells / wall / 1e9 if wall > 0 else None,
+                "gcell_steps_per_busy_s": cells / self.busy_s / 1e9 if self.busy_s > 0 else None,
+                "wall_s": wall}
+
+    # -- the loop ------------------------------------------------------------
+    def _loop(self):
+        try:
+            if hasattr(self.engine, "on_thread_start"):
+                self.engine.on_thread_start()
+            while True:
+                with self._cv:
+                    while not self._stop and not self._pending and not self._active:
+                        self._cv.wait(timeout=0.05)
+                    if self._stop and not self._pending and not self._active:
+                        return
+                self._admit()
+                if not self._active:
+                    continue
+                t0 = time.perf_counter()
+                self._advance()
+                self._complete()
+                self.busy_s += time.perf_counter() - t0
+        except BaseException as e:  # surface engine failures to every waiter
+            self._error = e
+            with self._cv:
+                for r in list(self._pending) + self._active:
+                    if not r.future.done():
+                        r.future.set_exception(e)
+                self._pending.clear()
+                self._active = []
+
+    def _admit(self):
+        while True:
+            with self._cv:
+                if not self._pending or len(self._active) >= self.max_active:
+                    return
+                req = self._pending[0]
+                if req.future.cancelled():
+                    self._pending.popleft()
+                    continue
+                if self._used + req.footprint > self.hbm_budget:
+                    return  # wait for memory: keep arrival order
+                self._pending.popleft()
+                if not req.future.set_running_or_notify_cancel():
+                    continue
+            try:
+                req.handle = self.engine.admit(req.problem)
+            except (ValueError, MemoryError) as e:  # bad request or no memory: fail it alone
+                self.failed += 1
+                req.future.set_exception(e)
+                continue
+            req.begin = self._clock
+            req.t_admit = time.perf_counter()
+            self._used += req.footprint
+            self._active.append(req)
+
+    def _advance(self):
+        remaining = [self.engine.steps(r.handle) - (self._clock - r.begin) for r in self._active]
+        n = max(1, min(self.chunk_steps, min(remaining)))
+        self.engine.advance([r.handle for r in self._active], [r.begin for r in self._active],
+                            self._clock, n)
+        self._clock += n
+
+    def _complete(self):
+        keep = []
+        for r in self._active:
+            if self._clock - r.begin < self.engine.steps(r.handle):
+                keep.append(r)
+                continue
+            result = self.engine.finish(r.handle)
+            r.t_done = time.perf_counter()
+            cells = _cell_steps(r.problem)
+            self.completed.append((r.rid, r.t_done - r.t_arrive, r.t_admit - r.t_arrive, cells))
+            self.engine.release(r.handle)
+            r.handle = None
+            self._used -= r.footprint
+            r.future.set_result(result)
+        self._active = keep
+
+
+def _cell_steps(p) -> int:
+    ref = p["bx"] if p["bx"] is not None else (p["by"] if p["by"] is not None else p["bz"])
+    return int(math.prod(ref.shape[:3])) * int(p["n_steps"])
+
+
+def poisson_arrivals(rate_hz: float, n: int, seed: int = 0) -> np.ndarray:
+    """Arrival times (s) of a Poisson process with the given mean rate."""
+    rng = np.random.default_rng(seed)
+    return np.cumsum(rng.exponential(1.0 / rate_hz, size=n))
+
+
+def run_stream(server: ShearServer, problems, arrivals_s, timeout_s=None):
+    """Submit ``problems`` at ``arrivals_s`` (seconds from now) and wait for all."""
+    t0 = time.perf_counter()
+    futs = []
+    for p, ta in zip(problems, arrivals_s):
+        dt = ta - (time.perf_counter() - t0)
+        if dt > 0:
+            time.sleep(dt)
+        futs.append(server.submit(p))
+    out = []
+    for f in futs:
+        try:
+            out.append(f.result(timeout=timeout_s))
+        except CancelledError:
+            out.append(None)
+    return out

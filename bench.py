@@ -54,6 +54,18 @@ def rank_info():
     return r, w, lr
 
 
+def reduce_scalar(x: float, op: str, device, world: int) -> float:
+    """Max or sum of a per-rank number over all ranks (identity for one rank)."""
+    if world == 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
+    return float(t.item())
+
+
 def measured_hbm():
     p = ROOT / "MEASURED_PEAKS.json"
     try:
@@ -305,6 +317,29 @@ def run_reference(a, rank, world):
 
 
 # ---------------------------------------------------------------------------
+# serving: config-4 request stream through the continuous-batching server
+# ---------------------------------------------------------------------------
+def serving_run(n_requests: int, rate_hz: float, seed: int = 0) -> dict:
+    """Poisson arrivals of config-4 requests (log-uniform 64^3..256^3 cubes,
+    1 or 4 pushes, nT 500..4000, inclusion media, HBM budget 150 GB)."""
+    from shearwave_b200 import workloads as W
+    from shearwave_b200.serve import ShearServer, poisson_arrivals, run_stream
+
+    rng = np.random.default_rng(1234 + seed)
+    probs = [W.problem_c4(rng) for _ in range(n_requests)]
+    arrivals = poisson_arrivals(rate_hz, n_requests, seed=seed)
+    with ShearServer(hbm_budget=150e9, chunk_steps=50) as srv:
+        run_stream(srv, probs, arrivals)
+    st = srv.stats()
+    return {"requests": n_requests, "rate_hz": rate_hz,
+            "latency_s": st["latency_s"], "queue_s": st["queue_s"],
+            "gcell_steps_per_s": st["gcell_steps_per_s"],
+            "cell_steps": int(sum(W.cell_steps(p) for p in probs)),
+            "workload": "config-4 requests (log-uniform 64^3..256^3, 1 or 4 pushes, "
+                        "nT 500..4000), Poisson arrivals, budget 150 GB, mixed form"}
+
+
+# ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
 def main(argv=None) -> int:
@@ -319,6 +354,10 @@ def main(argv=None) -> int:
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--grid", type=int, default=None, help="c1 only: cubic grid override")
     ap.add_argument("--nsteps", type=int, default=None, help="c1 only: nT override")
+    ap.add_argument("--serve-requests", type=int, default=16,
+                    help="requests of the config-4 serving stream run after the timing (0: skip)")
+    ap.add_argument("--serve-rate", type=float, default=4.0,
+                    help="mean Poisson arrival rate of the serving stream (requests/s)")
     ap.add_argument("--steps-per-pass", type=int, default=0, choices=[0, 1, 2],
                     help="mixed form: time steps fused per pass over HBM (0 = library default)")
     a = ap.parse_args(argv)
@@ -343,18 +382,10 @@ def main(argv=None) -> int:
             dist.barrier()
 
     def max_over_ranks(x: float) -> float:
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return reduce_scalar(x, "max", dev, world)
 
     def sum_over_ranks(x: float) -> float:
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.SUM)
-        return float(t.item())
+        return reduce_scalar(x, "sum", dev, world)
 
     probs = make_workload(a.workload, rank, a.grid, a.nsteps)
     if a.steps_per_pass:
@@ -462,6 +493,9 @@ def main(argv=None) -> int:
                        "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                        "note": "numpy inputs/outputs through shear_fdtd / shear_fdtd_batch, "
                                "wall clock, one step"}
+
+    if rank == 0 and world == 1 and a.serve_requests > 0:
+        line["serving"] = serving_run(a.serve_requests, a.serve_rate, seed=rank)
 
     if rank == 0 and world == 1 and not a.no_cpu:
         line["cpu_baseline"] = cpu_baseline(probs)

@@ -48,19 +48,31 @@ def gaussian_push(shape, centre, sig_lat=1.5e-3, sig_ax=5e-3, amp=1e3, h=H):
 
 
 def inclusion_medium(rng, shape, n_inc=12, h=H):
-    """rho +-5 % noise; 12 spheres (radius 2-8 mm, mu log-uniform 1-20 kPa, eta 0.5-5)."""
-    x, y, z = _coords(shape, h)
+    """rho +-5 % noise; 12 spheres (radius 2-8 mm, mu log-uniform 1-20 kPa, eta 0.5-5).
+
+    Spheres are painted in order (later ones overwrite earlier ones); each is
+    evaluated on its bounding box only.
+    """
     L = np.array(shape) * h
-    rho = 1000.0 * (1.0 + rng.uniform(-0.05, 0.05, shape))
-    mu = np.full(shape, 3e3)
-    eta = np.full(shape, 1.0)
+    rho = _f32(1000.0 * (1.0 + rng.uniform(-0.05, 0.05, shape)))
+    mu = np.full(shape, 3e3, dtype=np.float32)
+    eta = np.full(shape, 1.0, dtype=np.float32)
     for _ in range(n_inc):
         c = rng.uniform(0.0, 1.0, 3) * L
         r = rng.uniform(2e-3, 8e-3)
-        inside = (x - c[0]) ** 2 + (y - c[1]) ** 2 + (z - c[2]) ** 2 < r * r
-        mu[inside] = math.exp(rng.uniform(math.log(1e3), math.log(2e4)))
-        eta[inside] = rng.uniform(0.5, 5.0)
-    return _f32(rho), _f32(mu), _f32(eta)
+        mu_i = math.exp(rng.uniform(math.log(1e3), math.log(2e4)))
+        eta_i = rng.uniform(0.5, 5.0)
+        lo = [max(0, int(math.floor((c[a] - r) / h)) - 1) for a in range(3)]
+        hi = [min(shape[a], int(math.ceil((c[a] + r) / h)) + 2) for a in range(3)]
+        if any(hi[a] <= lo[a] for a in range(3)):
+            continue
+        ax = [np.arange(lo[a], hi[a]) * h - c[a] for a in range(3)]
+        d2 = (ax[0][:, None, None] ** 2 + ax[1][None, :, None] ** 2 + ax[2][None, None, :] ** 2)
+        inside = d2 < r * r
+        box = tuple(slice(lo[a], hi[a]) for a in range(3))
+        mu[box][inside] = np.float32(mu_i)
+        eta[box][inside] = np.float32(eta_i)
+    return rho, mu, eta
 
 
 def stable_dt(rho, mu, eta, dt_max, cfl=None, h=H):

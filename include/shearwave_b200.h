@@ -224,6 +224,10 @@ typedef struct sw_fdtd_desc {
   int32_t xchunk;         /* planes per tile along x (0 = automatic) */
   int32_t steps_per_pass; /* F32: 2 = two steps per pass over HBM; 0 (automatic) / 1 = one */
   int32_t kernel;         /* 0: TMA-staged step kernels (default), 1: direct-load kernels */
+  /* Device int the step loop may use as its step counter: with it, long runs
+   * of sw_fdtd_steps replay one instantiated CUDA graph of 32 steps instead
+   * of launching every step (NULL: direct launches only). */
+  int32_t* clock;
 } sw_fdtd_desc;
 
 /* Material coefficients from rho, mu, eta.  Each of rho/mu/eta is a dense

@@ -74,6 +74,7 @@ class FdtdDesc(C.Structure):
         ("xchunk", C.c_int32),
         ("steps_per_pass", C.c_int32),
         ("kernel", C.c_int32),
+        ("clock", C.c_void_p),
     ]
 
 

@@ -86,6 +86,7 @@ int make_step_args(const sw_fdtd_desc* d, StepArgs* a) {
   a->kernel = d->kernel;
   a->xchunk = d->xchunk;
   a->steps_per_pass = d->steps_per_pass;
+  a->clock = d->clock;
   const int nbuf = 3;
   for (int i = 0; i < nbuf; ++i)
     if (a->state[i] == nullptr) {

@@ -29,7 +29,8 @@ struct StepArgs {
   int* flags;
   int kernel;          // 0 TMA-staged, 1 direct loads
   int xchunk;          // requested planes per tile (0 automatic)
-  int steps_per_pass;  // mixed form: 1 one step per launch, 2 (or 0 = auto) two
+  int steps_per_pass;  // mixed form: 2 two steps per launch, 0 / 1 one
+  int* clock;          // device step counter for graph replays (or null)
 };
 
 int make_step_args(const sw_fdtd_desc* d, StepArgs* a);

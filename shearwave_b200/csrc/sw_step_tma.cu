@@ -81,7 +81,8 @@ int encode_tmap_4d(CUtensorMap* map, CUtensorMapDataType dt, void* base, const u
 template <bool BATCH>
 __global__ void __launch_bounds__(TmaF32::THREADS, 2)
     step_f32_tma(const __grid_constant__ TmaF32 one, const TmaF32* __restrict__ tab, int ninst,
-                 int ntiles, int it) {
+                 int ntiles, int it, const int* __restrict__ it_dev) {
+  if (it_dev != nullptr) it += *it_dev;  // step counter kept on the device (graph replays)
   constexpr int NA = TmaF32::NA, NB = TmaF32::NB, W = TmaF32::W, H = TmaF32::H;
   constexpr int TZ = TmaF32::TZ, TY = TmaF32::TY;
   constexpr int AF = TmaF32::A_STAGE / 4, BF = TmaF32::B_STAGE / 4;  // floats per stage
@@ -271,7 +272,8 @@ __global__ void __launch_bounds__(TmaF32::THREADS, 2)
 template <bool BATCH>
 __global__ void __launch_bounds__(TmaF64::THREADS, 2)
     step_f64_tma(const __grid_constant__ TmaF64 one, const TmaF64* __restrict__ tab, int ninst,
-                 int ntiles, int it) {
+                 int ntiles, int it, const int* __restrict__ it_dev) {
+  if (it_dev != nullptr) it += *it_dev;  // step counter kept on the device (graph replays)
   constexpr int NA = TmaF64::NA, NB = TmaF64::NB, W = TmaF64::W, H = TmaF64::H;
   constexpr int TZ = TmaF64::TZ, TY = TmaF64::TY;
   constexpr int AD = TmaF64::A_STAGE / 8, BD = TmaF64::B_STAGE / 8, HALF = TmaF64::HALF / 8;
@@ -601,6 +603,70 @@ int make_tma_f64(const StepArgs& a, int xchunk, TmaF64* t) {
   return SW_OK;
 }
 
+__global__ void clock_set(int* c, int v) { *c = v; }
+__global__ void clock_add(int* c, int by) { *c += by; }
+
+// Replay the step loop as one instantiated CUDA graph per segment: the graph
+// holds `seg` launches of `func` (each advancing `per_launch` steps, offsets
+// 0, per_launch, ...) reading the step counter `clock`, then a node that
+// advances the counter.  Returns the number of steps enqueued this way (0
+// when the run is too short to be worth a graph).  Kernel nodes are built
+// explicitly, so the caller's stream may be the legacy default stream.
+template <typename Inst>
+int graph_loop(void* func, const Inst& t, int grid, int threads, size_t smem, int per_launch,
+               int seg, int* clock, int it0, int nsteps, cudaStream_t s, int* done) {
+  *done = 0;
+  const int seg_steps = per_launch * seg;
+  const int reps = nsteps / seg_steps;
+  if (reps < 2 || clock == nullptr) return SW_OK;
+  cudaGraph_t g = nullptr;
+  cudaGraphExec_t ex = nullptr;
+  cudaError_t e = cudaGraphCreate(&g, 0);
+  cudaGraphNode_t prev = nullptr;
+  const Inst* tab = nullptr;
+  int ninst = 1, ntiles = t.ts.count;
+  const int* itd = clock;
+  std::vector<int> offs(seg);
+  for (int k = 0; k < seg && e == cudaSuccess; ++k) {
+    offs[k] = k * per_launch;
+    void* args[] = {(void*)&t, (void*)&tab, (void*)&ninst, (void*)&ntiles, (void*)&offs[k],
+                    (void*)&itd};
+    cudaKernelNodeParams p{};
+    p.func = func;
+    p.gridDim = dim3(grid);
+    p.blockDim = dim3(threads);
+    p.sharedMemBytes = (unsigned)smem;
+    p.kernelParams = args;
+    cudaGraphNode_t node;
+    e = cudaGraphAddKernelNode(&node, g, prev ? &prev : nullptr, prev ? 1 : 0, &p);
+    prev = node;
+  }
+  int by = seg_steps;
+  int* cl = clock;
+  if (e == cudaSuccess) {
+    void* args[] = {(void*)&cl, (void*)&by};
+    cudaKernelNodeParams p{};
+    p.func = (void*)clock_add;
+    p.gridDim = dim3(1);
+    p.blockDim = dim3(1);
+    p.kernelParams = args;
+    cudaGraphNode_t node;
+    e = cudaGraphAddKernelNode(&node, g, &prev, 1, &p);
+  }
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&ex, g, 0);
+  if (e == cudaSuccess) {
+    clock_set<<<1, 1, 0, s>>>(clock, it0);
+    e = cudaGetLastError();
+  }
+  for (int r = 0; r < reps && e == cudaSuccess; ++r) e = cudaGraphLaunch(ex, s);
+  if (ex) cudaGraphExecDestroy(ex);  // freed once the enqueued replays complete
+  if (g) cudaGraphDestroy(g);
+  if (e != cudaSuccess) return cuda_status(e, "step-loop graph");
+  count_launches((unsigned long long)reps * (seg + 1) + 1);
+  *done = reps * seg_steps;
+  return SW_OK;
+}
+
 int launch_steps_tma(const StepArgs& a, int xchunk, int it0, int nsteps, cudaStream_t s) {
   int rc = set_smem_attr(a.precision);
   if (rc != SW_OK) return rc;
@@ -611,8 +677,16 @@ int launch_steps_tma(const StepArgs& a, int xchunk, int it0, int nsteps, cudaStr
     if (rc != SW_OK) return rc;
     if (t.ts.count == 0) return SW_OK;
     const int grid = std::min(t.ts.count, 148 * 2);
-    for (int it = it0; it < it0 + nsteps; ++it)
-      step_f64_tma<false><<<grid, TmaF64::THREADS, smem, s>>>(t, nullptr, 1, t.ts.count, it);
+    int done = 0;
+    rc = graph_loop(reinterpret_cast<void*>(step_f64_tma<false>), t, grid, TmaF64::THREADS, smem,
+                    1, 32, a.clock, it0, nsteps, s, &done);
+    if (rc != SW_OK) return rc;
+    for (int it = it0 + done; it < it0 + nsteps; ++it)
+      step_f64_tma<false><<<grid, TmaF64::THREADS, smem, s>>>(t, nullptr, 1, t.ts.count, it,
+                                                              nullptr);
+    count_launches((unsigned long long)(nsteps - done));
+    SW_CHECK_LAUNCH("step (tma)");
+    return SW_OK;
   } else {
     // steps_per_pass 2: two steps per launch where two remain, one step
     // otherwise; 0 (automatic) and 1: one step per launch
@@ -630,12 +704,22 @@ int launch_steps_tma(const StepArgs& a, int xchunk, int it0, int nsteps, cudaStr
     }
     const int grid = std::min(t.ts.count, 148 * 2);
     unsigned long long n_launch = 0;
-    for (int it = it0; it < it0 + nsteps;) {
+    int done = 0;
+    if (fuse && tb.ts.count > 0)
+      rc = graph_loop(const_cast<void*>(step_f32_fused2_ptr()), tb,
+                      std::min(tb.ts.count, 148), TmaF32TB::THREADS, tb_smem_bytes(), 2, 16,
+                      a.clock, it0, nsteps, s, &done);
+    else
+      rc = graph_loop(reinterpret_cast<void*>(step_f32_tma<false>), t, grid, TmaF32::THREADS,
+                      smem, 1, 32, a.clock, it0, nsteps, s, &done);
+    if (rc != SW_OK) return rc;
+    for (int it = it0 + done; it < it0 + nsteps;) {
       if (fuse && it + 1 < it0 + nsteps) {
         launch_fused2_raw(tb, it, s);
         it += 2;
       } else {
-        step_f32_tma<false><<<grid, TmaF32::THREADS, smem, s>>>(t, nullptr, 1, t.ts.count, it);
+        step_f32_tma<false><<<grid, TmaF32::THREADS, smem, s>>>(t, nullptr, 1, t.ts.count, it,
+                                                                nullptr);
         it += 1;
       }
       ++n_launch;
@@ -659,11 +743,11 @@ int launch_steps_tma_batch(int precision, const void* d_tab, int ninst, int ntil
   if (precision == SW_PLAIN_F64) {
     TmaF64 dummy{};
     step_f64_tma<true><<<grid, TmaF64::THREADS, smem, s>>>(dummy, (const TmaF64*)d_tab, ninst,
-                                                          ntiles, it);
+                                                          ntiles, it, nullptr);
   } else {
     TmaF32 dummy{};
     step_f32_tma<true><<<grid, TmaF32::THREADS, smem, s>>>(dummy, (const TmaF32*)d_tab, ninst,
-                                                          ntiles, it);
+                                                          ntiles, it, nullptr);
   }
   count_launches(1);
   SW_CHECK_LAUNCH("step (tma, batch)");

@@ -131,6 +131,7 @@ int make_tma_f32_tb(const StepArgs& a, int xchunk, TmaF32TB* t);
 int launch_fused2(const StepArgs& a, int xchunk, int it, cudaStream_t s);
 int launch_fused2_prepare();                                   // kernel attributes, once
 void launch_fused2_raw(const TmaF32TB& t, int it, cudaStream_t s);  // enqueue one launch
+const void* step_f32_fused2_ptr();  // the single-solve fused kernel (for graph nodes)
 int launch_fused2_batch(const void* d_tab, int ninst, int ntiles, int it, cudaStream_t s);
 int tma_xchunk(const Geom& g, int tz, int ty, long long want_tiles);
 int make_tma_f32(const StepArgs& a, int xchunk, TmaF32* t);

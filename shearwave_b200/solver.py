@@ -371,6 +371,9 @@ class _Run:
             d.inv_rho = self.inv_rho.data_ptr()
         self.flags = torch.zeros(1, dtype=torch.int32, device=dev)
         d.flags = self.flags.data_ptr()
+        # device step counter: lets the library replay the loop as CUDA graphs
+        self.clock = torch.zeros(1, dtype=torch.int32, device=dev)
+        d.clock = self.clock.data_ptr()
         self.keep = []  # tensors referenced by the descriptor
 
     def p(self):
@@ -530,6 +533,8 @@ class _Solve:
         if spp not in (0, 1, 2):
             raise ValueError("steps_per_pass must be 1 or 2 (0 = automatic)")
         run.desc.steps_per_pass = spp
+        if not opts.get("cuda_graph", True):
+            run.desc.clock = None
         run.materials(rho, mu, eta, dt)
         iu = iv = None
         if opts.get("initial_u") is not None:
@@ -710,7 +715,8 @@ def shear_fdtd(
     "spectral" explicitly), ``kahan`` (True), ``step_kernel`` ("tma" default, or "direct"), ``xchunk`` (planes
     per tile along x, 0 = automatic), ``steps_per_pass`` (mixed form: 2
     fuses two time steps per pass over HBM; 1 or 0 (default) one step per
-    launch), ``force_terms`` (extra separable terms:
+    launch), ``cuda_graph`` (True: long step runs replay one instantiated CUDA
+    graph of 32 steps), ``force_terms`` (extra separable terms:
     list of ``((bx, by, bz), env)``), ``snapshot_stride`` (alias of the
     keyword), ``info`` (dict filled with CG statistics, phase times and a
     non-finite flag).

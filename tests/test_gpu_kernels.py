@@ -120,3 +120,20 @@ def test_two_steps_per_pass_without_viscosity(cuda):
             for spp in (2, 1)]
     for x, y in zip(*outs):
         assert rel_l2(x, y) <= 1e-6
+
+
+@pytest.mark.parametrize("precision,spp", [("mixed", 1), ("mixed", 2), ("fp64", 0)])
+def test_cuda_graph_replay_matches_direct_launches(cuda, precision, spp):
+    """Long step runs replay an instantiated graph; results are bit-identical."""
+    import shearwave_b200 as sw
+
+    p, opts = _problem((20, 18, 40), seed=9, n_steps=137)
+
+    def run(graph):
+        return sw.shear_fdtd(p["bx"], p["by"], p["bz"], p["rho"], p["mu"], p["dX"], p["dY"],
+                             p["dZ"], p["dT"], p["n_steps"],
+                             dict(opts, precision=precision, steps_per_pass=spp,
+                                  cuda_graph=graph), snapshot_stride=None)
+
+    for x, y in zip(run(True), run(False)):
+        assert np.array_equal(x, y)

@@ -27,6 +27,7 @@
  *  src/shearwave/solver.py:644-683    project_vector_field   -> sw_project
  *  src/shearwave/solver.py:1010-1050  poisson_cg             -> sw_project (CG stage)
  *  src/shearwave/solver.py:686-729    laplacian/divergence/gradient_center -> sw_laplacian, ...
+ *  src/shearwave/solver.py:569-625    elastic_solve_static   -> sw_static_solve
  *  src/shearwave/strain.py:16-135     compute_strain_tensor / _invariants -> sw_strain*
  */
 #ifndef SHEARWAVE_B200_H
@@ -184,6 +185,16 @@ int sw_convert(int ncomp, const double* src, int nx, int ny, int nz, int out_dty
                int64_t dst_cs, int64_t dst_sx, int64_t dst_sy, int64_t dst_sz, double scale,
                int rho_dtype, const void* rho, int64_t rho_sx, int64_t rho_sy, int64_t rho_sz,
                void* stream);
+
+/* ---- static elastic solve (solver.py:569-625) ---------------------------- */
+/* CG on (-mu L7) u = b with zero shell, in FP64, with the reference's loop
+ * (break on p.Ap <= 0, stop at sqrt(r.r / rs0) < tol).  b and mu (NULL: the
+ * scalar mu_s) are `dtype` arrays with element strides (sx, sy, sz); u is
+ * written to `out` as one padded FP64 field.  Workspace: as sw_project. */
+int sw_static_solve(int dtype, const void* b, const void* mu, double mu_s, int64_t sx,
+                    int64_t sy, int64_t sz, int nx, int ny, int nz, double dX, double dY,
+                    double dZ, double tol, int max_iters, double* out, void* workspace,
+                    size_t workspace_bytes, sw_cg_stats* stats, void* stream);
 
 /* ---- time loop (solver.py:27-243) --------------------------------------- */
 typedef struct sw_fdtd_desc {

@@ -9,6 +9,7 @@ loudly if it is missing or no CUDA device is present.
 
 from .solver import (
     divergence_center,
+    elastic_solve_static,
     gradient_center,
     laplacian_center,
     project_body_force_to_shear,
@@ -27,6 +28,7 @@ __all__ = [
     "compute_strain_invariants",
     "compute_strain_tensor",
     "divergence_center",
+    "elastic_solve_static",
     "gradient_center",
     "laplacian_center",
     "project_body_force_to_shear",

@@ -109,6 +109,9 @@ _SIGNATURES = {
     "sw_fdtd_batch_table_bytes": ([C.c_int], _sz),
     "sw_fdtd_batch_steps": ([C.POINTER(FdtdDesc), C.POINTER(C.c_int32), C.c_int, _i32, _i32, _vp,
                              _sz, _vp], C.c_int),
+    "sw_static_solve": ([C.c_int, _vp, _vp, _f64, _i64, _i64, _i64, C.c_int, C.c_int, C.c_int,
+                         _f64, _f64, _f64, _f64, C.c_int, _vp, _vp, _sz, C.POINTER(CGStats), _vp],
+                        C.c_int),
     "sw_convert": ([C.c_int, _vp, C.c_int, C.c_int, C.c_int, C.c_int, _vp, _i64, _i64, _i64,
                     _i64, _f64, C.c_int, _vp, _i64, _i64, _i64, _vp], C.c_int),
     "sw_fdtd_materials": ([C.POINTER(FdtdDesc), C.c_int, _vp, _f64, _vp, _f64, C.c_int, _vp,

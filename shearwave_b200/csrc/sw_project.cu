@@ -99,7 +99,19 @@ __global__ void __launch_bounds__(TILE_THREADS) cg_prep(const CgInst* __restrict
     const TileCoord tc = tile_coord(g, in.ts, local);
     const int z = tc.z0 + threadIdx.x, y = tc.y0 + threadIdx.y;
     double acc = 0.0, mx = 0.0;
-    for (int x = tc.x0; x < tc.x1; ++x) {
+    if (in.op == 1) {  // static elastic solve: r = p = mask b, mu to FP64
+      const T* mu = fin[3 * ii + 1];
+      for (int x = tc.x0; x < tc.x1; ++x) {
+        if (!interior(g, x, y, z)) continue;
+        const long long i = (long long)x * g.sxy + (long long)y * g.pz + z;
+        const double b = ld_masked(fx, in, s, x, y, z);
+        in.r[i] = b;
+        in.p0[i] = b;
+        in.muf[i] = mu ? ld_masked(mu, in, s, x, y, z) : in.mu_s;
+        acc += b * b;
+      }
+    }
+    for (int x = tc.x0; x < tc.x1 && in.op == 0; ++x) {
       if (!interior(g, x, y, z)) continue;
       double tx = (ld_masked(fx, in, s, x + 1, y, z) - ld_masked(fx, in, s, x - 1, y, z)) * in.c2x;
       double ty = (ld_masked(fy, in, s, x, y + 1, z) - ld_masked(fy, in, s, x, y - 1, z)) * in.c2y;
@@ -127,7 +139,7 @@ __global__ void __launch_bounds__(TILE_THREADS) cg_prep(const CgInst* __restrict
         st->iters = 0;
         st->k = 0;
         st->rel = nan("");
-        if (tot.y < 1e-12) st->reason = SW_CG_EARLY_EXIT;
+        if (in.op == 0 && tot.y < 1e-12) st->reason = SW_CG_EARLY_EXIT;
         else if (st->max_iters <= 0) st->reason = SW_CG_MAXITERS;
         else st->reason = SW_CG_RUNNING;
         __threadfence();
@@ -175,6 +187,16 @@ __global__ void __launch_bounds__(TILE_THREADS) cg_apply(const CgInst* __restric
       if (!interior(g, x, y, z)) continue;
       const long long i = (long long)x * g.sxy + (long long)y * g.pz + z;
       const double pc = pv(i);
+      if (in.op == 1) {  // -mu L7(p), laplacian_center's operation order
+        const double lap = ((pv(i + g.sxy) - 2.0 * pc) + pv(i - g.sxy)) * in.ihx2 +
+                           ((pv(i + g.pz) - 2.0 * pc) + pv(i - g.pz)) * in.ihy2 +
+                           ((pv(i + 1) - 2.0 * pc) + pv(i - 1)) * in.ihz2;
+        const double ap = -in.muf[i] * lap;
+        in.ap[i] = ap;
+        if (!pv.first) pnew[i] = pc;
+        acc += pc * ap;
+        continue;
+      }
       double gp, gm, tx, ty, tz;
       gp = (x + 1 <= g.nx - 2) ? (pv(i + 2 * g.sxy) - pc) * in.c2x : 0.0;
       gm = (x - 1 >= 1) ? (pc - pv(i - 2 * g.sxy)) * in.c2x : 0.0;
@@ -198,7 +220,8 @@ __global__ void __launch_bounds__(TILE_THREADS) cg_apply(const CgInst* __restric
         CgState* w = in.st;
         w->ticket = 0u;
         const double denom = tot.x;
-        if (!isfinite(denom) || denom <= 0.0) w->reason = SW_CG_BREAKDOWN;
+        const bool stop = (in.op == 1) ? (denom <= 0.0) : (!isfinite(denom) || denom <= 0.0);
+        if (stop) w->reason = SW_CG_BREAKDOWN;
         else w->alpha = w->rs / denom;
         __threadfence();
       }
@@ -244,7 +267,7 @@ __global__ void __launch_bounds__(TILE_THREADS) cg_update(const CgInst* __restri
         w->ticket = 0u;
         const double rs_new = tot.x;
         w->iters += 1;
-        if (!isfinite(rs_new)) {
+        if (in.op == 0 && !isfinite(rs_new)) {
           w->reason = SW_CG_NONFINITE;
         } else {
           const double rel = sqrt(rs_new / w->rs0);
@@ -302,7 +325,7 @@ size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
 size_t cg_workspace_bytes(const Geom& g, const TileSpace& ts) {
   size_t vec = align_up((size_t)g.ncell * sizeof(double), 256);
-  size_t b = 5 * vec;                                            // x r p0 p1 ap
+  size_t b = 6 * vec;                                            // x r p0 p1 ap muf
   b += align_up((size_t)ts.count * sizeof(double2), 256);        // partials
   b += align_up(sizeof(CgState), 256);                           // state
   b += align_up(sizeof(CgInst), 256);                            // instance table
@@ -332,6 +355,8 @@ int cg_layout(const Geom& g, char* ws, size_t ws_bytes, CgInst* in, CgState** st
   in->p1 = (double*)p;
   p += vec;
   in->ap = (double*)p;
+  p += vec;
+  in->muf = (double*)p;
   p += vec;
   in->partials = (double2*)p;
   p += align_up((size_t)in->ts.count * sizeof(double2), 256);
@@ -405,9 +430,9 @@ int project_one(const void* fx, const void* fy, const void* fz, InStride fs, con
   hst.max_iters = max_iters;
   hst.reason = SW_CG_RUNNING;
   cudaError_t e;
-  // x r p0 p1 ap are consecutive 256-byte aligned vectors: zero all of them
+  // x r p0 p1 ap muf are consecutive 256-byte aligned vectors: zero all of them
   const size_t vec = align_up((size_t)g.ncell * sizeof(double), 256);
-  e = cudaMemsetAsync(in.x, 0, 5 * vec, s);
+  e = cudaMemsetAsync(in.x, 0, 6 * vec, s);
   if (e == cudaSuccess) e = cudaMemcpyAsync(st, &hst, sizeof(hst), cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess) e = cudaMemcpyAsync(d_tab, &in, sizeof(in), cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess)
@@ -442,6 +467,61 @@ int project_one(const void* fx, const void* fy, const void* fz, InStride fs, con
     stats->reason = hst.reason;
     stats->rel = hst.rel;
     stats->max_div = hst.maxdiv;
+  }
+  return SW_OK;
+}
+
+// Static elastic solve: CG on (-mu L7) u = b (solver.py:569-625) in FP64;
+// u (padded FP64) is written to `out`.
+template <typename T>
+int static_one(const void* b, const void* mu, double mu_s, InStride fs, const Geom& g,
+               double dX, double dY, double dZ, double tol, int max_iters, double* out,
+               void* ws, size_t ws_bytes, sw_cg_stats* stats, cudaStream_t s) {
+  CgInst in{};
+  CgState* st = nullptr;
+  char* tail = nullptr;
+  int rc = cg_layout(g, (char*)ws, ws_bytes, &in, &st, &tail);
+  if (rc != SW_OK) return rc;
+  in.op = 1;
+  in.ihx2 = 1.0 / (dX * dX);
+  in.ihy2 = 1.0 / (dY * dY);
+  in.ihz2 = 1.0 / (dZ * dZ);
+  in.mu_s = mu_s;
+  CgInst* d_tab = (CgInst*)tail;
+  tail += align_up(sizeof(CgInst), 256);
+  const T** d_fin = (const T**)tail;
+  InStride* d_fs = (InStride*)(tail + 3 * sizeof(void*));
+  const void* fin[3] = {b, mu, nullptr};
+  CgState hst{};
+  hst.tol = tol;
+  hst.max_iters = max_iters;
+  hst.reason = SW_CG_RUNNING;
+  const size_t vec = align_up((size_t)g.ncell * sizeof(double), 256);
+  cudaError_t e = cudaMemsetAsync(in.x, 0, 6 * vec, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(st, &hst, sizeof(hst), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d_tab, &in, sizeof(in), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(d_fin, fin, 3 * sizeof(void*), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d_fs, &fs, sizeof(fs), cudaMemcpyHostToDevice, s);
+  if (e != cudaSuccess) return cuda_status(e, "static solve setup");
+  const int ntiles = in.ts.count;
+  if (ntiles > 0) {
+    const int grid = std::max(1, std::min(ntiles, 148 * 8));
+    cg_prep<T><<<grid, dim3(TILE_Z, TILE_Y), 0, s>>>(d_tab, 1, ntiles, d_fin, d_fs);
+    count_launches(1);
+    SW_CHECK_LAUNCH("static cg_prep");
+    rc = cg_run(d_tab, 1, ntiles, st, 1, s);
+    if (rc != SW_OK) return rc;
+  }
+  e = cudaMemcpyAsync(out, in.x, (size_t)g.ncell * sizeof(double), cudaMemcpyDeviceToDevice, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&hst, st, sizeof(hst), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return cuda_status(e, "static solve readback");
+  if (stats) {
+    stats->iters = hst.iters;
+    stats->reason = ntiles > 0 ? hst.reason : SW_CG_MAXITERS;
+    stats->rel = hst.rel;
+    stats->max_div = 0.0;
   }
   return SW_OK;
 }
@@ -548,7 +628,7 @@ int project_batch_t(const sw_project_job* jobs, int n, char* table, sw_cg_stats*
     strides[i] = InStride{j.sx, j.sy, j.sz};
     outs[i] = j.out;
     const size_t vec = align_up((size_t)g.ncell * sizeof(double), 256);
-    if (e == cudaSuccess) e = cudaMemsetAsync(insts[i].x, 0, 5 * vec, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(insts[i].x, 0, 6 * vec, s);
     if (e == cudaSuccess) e = cudaMemsetAsync(j.out, 0, (size_t)g.ncell * 3 * sizeof(double), s);
   }
   if (e == cudaSuccess)
@@ -623,5 +703,28 @@ extern "C" int sw_project_batch(const sw_project_job* jobs, int n, void* table,
   if (dt == SW_F32) return project_batch_t<float>(jobs, n, (char*)table, stats, s);
   if (dt == SW_F64) return project_batch_t<double>(jobs, n, (char*)table, stats, s);
   set_error("sw_project_batch: unknown dtype %d", dt);
+  return SW_EINVAL;
+}
+
+extern "C" int sw_static_solve(int dtype, const void* b, const void* mu, double mu_s,
+                               int64_t sx, int64_t sy, int64_t sz, int nx, int ny, int nz,
+                               double dX, double dY, double dZ, double tol, int max_iters,
+                               double* out, void* workspace, size_t workspace_bytes,
+                               sw_cg_stats* stats, void* stream) {
+  if (nx <= 0 || ny <= 0 || nz <= 0 || out == nullptr || b == nullptr ||
+      !(dX > 0 && dY > 0 && dZ > 0)) {
+    set_error("sw_static_solve: bad grid, spacing or null pointer");
+    return SW_EINVAL;
+  }
+  Geom g = make_geom(nx, ny, nz, pad_pitch(nz));
+  InStride fs{sx, sy, sz};
+  cudaStream_t s = (cudaStream_t)stream;
+  if (dtype == SW_F32)
+    return static_one<float>(b, mu, mu_s, fs, g, dX, dY, dZ, tol, max_iters, out, workspace,
+                             workspace_bytes, stats, s);
+  if (dtype == SW_F64)
+    return static_one<double>(b, mu, mu_s, fs, g, dX, dY, dZ, tol, max_iters, out, workspace,
+                              workspace_bytes, stats, s);
+  set_error("sw_static_solve: unknown dtype %d", dtype);
   return SW_EINVAL;
 }

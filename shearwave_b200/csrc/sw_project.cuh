@@ -27,14 +27,23 @@ struct CgState {
 };
 
 // One solve in a launch's instance table.
+//   op 0: the projection's Poisson operator A = -div_c(grad_c .)
+//         (src/shearwave/solver.py:1024-1026), rhs = -div_c(mask f);
+//   op 1: the static elastic operator A = -mu L7(.) (solver.py:596-597),
+//         rhs = mask b; no non-finite breaks and no early exit, like the
+//         reference's elastic_solve_static loop (solver.py:605-623).
 struct CgInst {
   Geom g;
   TileSpace ts;
   double c2x, c2y, c2z;  // 1 / (2 h)
+  double ihx2, ihy2, ihz2;  // 1 / h^2 (op 1)
   double *x, *r, *p0, *p1, *ap;
+  double* muf;           // mu on interior cells, FP64 (op 1)
+  double mu_s;           // scalar mu when no field is given (op 1)
   double2* partials;     // per tile: (sum, max)
   CgState* st;
   int tile_base;         // first global tile index of this instance
+  int op;
 };
 
 size_t align_up(size_t v, size_t a);

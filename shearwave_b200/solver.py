@@ -38,6 +38,7 @@ from ._device import (
 
 __all__ = [
     "divergence_center",
+    "elastic_solve_static",
     "gradient_center",
     "laplacian_center",
     "project_body_force_to_shear",
@@ -213,6 +214,38 @@ def project_vector_field(fx, fy, fz, dX, dY, dZ, tol, max_iters, *, info=None, m
     if is_tensor(fx):
         return tuple(outs)
     return tuple(o.cpu().numpy() for o in outs)
+
+
+def elastic_solve_static(bz, dX, dY, dZ, mu, tol=1e-6, max_iters=1500, *, verbose=False,
+                         info=None):
+    """Solve ``mu * laplace(u) = -bz`` (zero shell) by CG on ``(-mu L7) u = bz``.
+
+    solver.py:569-625, with the reference's loop (break on ``p.Ap <= 0``,
+    stop at ``sqrt(r.r / rs0) < tol``) in FP64 on the GPU.  Returns u in the
+    dtype of ``bz`` (float32 unless bz is float64).
+    """
+    dev = require_cuda()
+    dt = _op_dtype(bz)
+    b = to_device(bz, dt, dev)
+    shape = _shape(b)
+    if len(shape) != 3:
+        raise ValueError("bz must be a 3-D array")
+    nx, ny, nz = shape
+    m, ms = _material(mu, shape, dt, dev)
+    ws = _Workspace(nx, ny, nz, dev)
+    st = _native.CGStats()
+    _native.call("sw_static_solve", dtype_code(dt), ptr(b), ptr(m), ms, ny * nz, nz, 1, nx, ny,
+                 nz, dX, dY, dZ, float(tol), int(max_iters), ws.out.data_ptr(), ptr(ws.ws),
+                 ws.bytes, C.byref(st), stream_handle())
+    u = torch.empty(shape, dtype=dt, device=dev)
+    _native.call("sw_convert", 1, ws.out.data_ptr(), nx, ny, nz, dtype_code(dt), ptr(u), 0,
+                 ny * nz, nz, 1, 1.0, _native.SW_F32, None, 0, 0, 0, stream_handle())
+    d = st.as_dict()
+    if verbose:
+        print(f"CG (GPU): it={d['iters']}/{max_iters}, rel={d['rel']:.3e}, {d['reason']}")
+    if info is not None:
+        info.update(d)
+    return u if is_tensor(bz) else u.cpu().numpy()
 
 
 def project_body_force_to_shear(bz, dX, dY, dZ, tol=5e-5, max_iters=400):

@@ -143,3 +143,24 @@ def test_strain_bitexact(cuda, tag, dt):
     assert np.array_equal(eps2, eps)
     for k in inv:
         assert np.array_equal(inv2[k], inv[k]), k
+
+
+def test_static_solve_matches_reference(cuda):
+    """elastic_solve_static (solver.py:569-625) against the reference's fixture."""
+    import shearwave_b200 as sw
+
+    case = cases.CASES["static_a"]
+    gold = load_golden("static_a")
+    bz = cases.static_inputs(case)
+    d = case["h"]
+    info = {}
+    u64 = sw.elastic_solve_static(bz.astype(np.float64), d, d, d, case["mu"], tol=case["tol"],
+                                  max_iters=case["max_iters"], info=info)
+    assert u64.dtype == np.float64
+    assert info["reason"] == "converged"
+    assert info["iters"] + 1 == int(gold["f64_apply_calls"])  # + the initial residual
+    assert rel_l2(u64, gold["f64_u"]) <= FP64_TOL
+    u32 = sw.elastic_solve_static(bz, d, d, d, case["mu"], tol=case["tol"],
+                                  max_iters=case["max_iters"])
+    assert u32.dtype == np.float32
+    assert rel_l2(u32, gold["f64_u"]) <= 1e-6

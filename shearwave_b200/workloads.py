@@ -133,6 +133,42 @@ def problem_c1(seed=0, n_steps=2000, shape=(192, 192, 192)):
     return p
 
 
+def problem_c2(seed=0, n_steps=4000, shape=(256, 256, 384), n_push=8):
+    """Config 2: a 5 mm stiff slab (z in [2.5, 7.5) mm; mu 500 kPa, eta 2, rho
+    1900) over soft tissue (mu 2 kPa, eta 1, rho 1040), every map scaled by
+    (1 + 0.1 s) with s Gaussian-filtered white noise (sigma 4 voxels, max
+    |s| = 1); 8 pushes (sigma 1 mm lateral, 4 mm axial, 1e3 N/m^3) centred in
+    the soft region, each on for 20 steps (100 us) from a start in
+    [0, nT/4); dT 5 us.
+    """
+    from scipy.ndimage import gaussian_filter
+
+    rng = np.random.default_rng(seed)
+    nz = shape[2]
+    zc = (np.arange(nz) + 0.5) * H
+    slab = (zc >= 2.5e-3) & (zc < 7.5e-3)
+    mu = np.where(slab, 500e3, 2e3)[None, None, :] * np.ones(shape)
+    eta = np.where(slab, 2.0, 1.0)[None, None, :] * np.ones(shape)
+    rho = np.where(slab, 1900.0, 1040.0)[None, None, :] * np.ones(shape)
+    sm = gaussian_filter(rng.standard_normal(shape).astype(np.float32), sigma=4.0)
+    sm /= np.max(np.abs(sm))
+    var = 1.0 + 0.1 * sm
+    mu, eta, rho = _f32(mu * var), _f32(eta * var), _f32(rho * var)
+    L = np.array(shape) * H
+    pushes = []
+    for _ in range(n_push):
+        c = np.array([rng.uniform(0.25, 0.75) * L[0], rng.uniform(0.25, 0.75) * L[1],
+                      rng.uniform(9e-3, L[2] - 4e-3)])
+        start = int(rng.integers(0, max(1, n_steps // 4)))
+        pushes.append((gaussian_push(shape, c, sig_lat=1e-3, sig_ax=4e-3),
+                       _envelope(n_steps, 20, start)))
+    opts = {"eta": eta, "env_t": pushes[0][1], "poisson_tol": 1e-10,
+            "poisson_max_iters": 3 * max(shape),
+            "force_terms": [((None, None, b), env) for b, env in pushes[1:]]}
+    return {"name": "c2", "bx": None, "by": None, "bz": pushes[0][0], "rho": rho, "mu": mu,
+            "dX": H, "dY": H, "dZ": H, "dT": 5e-6, "n_steps": int(n_steps), "opts": opts}
+
+
 def batch_c3(seed=0, n=48, shrink=1.0):
     """48 seeded instances: grids U(64,160) x U(64,160) x U(64,224), nT U[500,3000].
 

@@ -168,7 +168,7 @@ def describe(name: str, probs) -> dict:
             "instances": len(probs), "cell_steps_per_rank": cs,
             "grid": list(_shape(probs[0])) if len(probs) == 1 else "varied",
             "n_steps": probs[0]["n_steps"] if len(probs) == 1 else "varied",
-            "dX_m": probs[0]["dX"], "precision": "mixed (FP32 fields, Kahan u, FP64 CG)",
+            "dX_m": probs[0]["dX"], "precision": "mixed (FP32 u and increment, FP64 projection)",
             "l2_flush": "none needed: per-solve state is larger than the 126 MB L2",
             "data": "seeded synthetic inputs with the config shapes"}
     return desc

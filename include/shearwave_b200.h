@@ -65,7 +65,7 @@ enum sw_cg_reason {
 
 enum sw_precision {
   SW_PLAIN_F64 = 0, /* FP64 fields, reference arithmetic (the plain drop-in) */
-  SW_MIXED_F32 = 1  /* FP32 fields in increment form, Kahan-compensated u */
+  SW_MIXED_F32 = 1  /* FP32 fields in increment form (u compensated when desc.kahan) */
 };
 
 /* ---- library --------------------------------------------------------- */

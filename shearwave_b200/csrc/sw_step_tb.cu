@@ -161,8 +161,10 @@ __global__ void __launch_bounds__(TmaF32TB::THREADS, 1)
       const T* in;
       int local, lit;
       if (!resolve_tile<T, BATCH>(one, tab, ninst, t, it, in, local, lit)) continue;
-      const Geom& g = in->g;
+      const Geom& g = in->g;  // hot switches in registers (see step_f32_tma)
       const TbCoord tc = tb_coord(g, in->ts, local);
+      const bool use_damp = in->use_damp != 0;
+      const float damp = in->damp;
       const int zA0 = floor4(tc.z_start - 2), zB0 = floor4(tc.z_start - 1);
       const int offA = tc.z_start - 1 - zA0;  // level-1 column 0 in the level-0 box
       const int offB = tc.z_start - 1 - zB0;  // level-1 column 0 in the point box
@@ -245,7 +247,7 @@ __global__ void __launch_bounds__(TmaF32TB::THREADS, 1)
                 for (int j = ja0; j < ja1; ++j)
                   inc += in->pat[((long long)in->term_pat[j] * 3 + comp) * nc + i] *
                          (float)in->term_scale[j];
-                if (in->use_damp) inc *= in->damp;
+                if (use_damp) inc *= damp;
                 if (kahan) {
                   const float c0 = Bc[comp * HB * WB + ob];
                   const float yk = inc - c0;
@@ -306,19 +308,17 @@ __global__ void __launch_bounds__(TmaF32TB::THREADS, 1)
               for (int j = jb0; j < jb1; ++j)
                 inc += in->pat[((long long)in->term_pat[j] * 3 + comp) * nc + i] *
                        (float)in->term_scale[j];
-              if (in->use_damp) inc *= in->damp;
-              float unew, cnew;
+              if (use_damp) inc *= damp;
+              float unew;
               if (kahan) {
                 const float yk = inc - cp[k][comp];
                 unew = u0 + yk;
-                cnew = (unew - u0) - yk;
+                D[(6 + comp) * nc + i] = (unew - u0) - yk;
               } else {
-                unew = u0 + inc;
-                cnew = 0.0f;
+                unew = u0 + inc;  // compensation planes unused
               }
               D[comp * nc + i] = unew;
               D[(3 + comp) * nc + i] = inc;
-              D[(6 + comp) * nc + i] = cnew;
               bad |= !isfinite(unew);
               if (snap2)
                 in->snaps[((((long long)slot2 * g.nx + x) * g.ny + y) * g.nz + zc[k]) * 3 +

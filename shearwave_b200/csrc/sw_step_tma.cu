@@ -9,7 +9,10 @@
 //  * One elected thread streams planes into a 4-stage shared-memory ring with
 //    4-D TMA tile loads (all halo'd components of a plane in one box, or two
 //    boxes for the two FP64 buffers), completion on one mbarrier per stage.
-//    Two planes are always in flight ahead of the plane being computed.
+//    The x neighbours at x-1 come from registers (each thread keeps the centre
+//    values of the plane it computed last), so a stage is freed as soon as
+//    its plane is computed: the ring holds planes x and x+1, and planes x+2
+//    and x+3 are in flight while plane x is computed.
 //  * The box starts 4 (FP32) / 2 (FP64) cells before the tile in z so the
 //    innermost coordinate stays 16-byte aligned; y starts one row before.
 //    Out-of-range rows/columns are zero-filled by TMA.
@@ -152,10 +155,14 @@ __global__ void __launch_bounds__(TmaF32::THREADS, 2)
       const TmaF32* in;
       int local, lit;
       if (!resolve_tile<TmaF32, BATCH>(one, tab, ninst, t, it, in, local, lit)) continue;
+      // the per-cell switches in registers: the table lives in global memory and
+      // the stores below could otherwise force reloads of its fields (fields
+      // used only on push / snapshot steps are read where they are used)
       const Geom& g = in->g;
       const TileCoord tc = tile_coord_t(g, in->ts, local, TZ, TY);
-      const float* __restrict__ S = in->state[lit % 3];
       float* __restrict__ D = in->state[(lit + 1) % 3];
+      const bool kahan = in->kahan != 0, use_damp = in->use_damp != 0;
+      const float damp = in->damp;
       const int y = tc.y0 + ly;
       const bool yin = (y >= 1 && y <= g.ny - 2);
       const int z0 = tc.z0 + lane, z1 = z0 + 32;
@@ -169,32 +176,56 @@ __global__ void __launch_bounds__(TmaF32::THREADS, 2)
       const long long nc = g.ncell;
       const bool visc = in->ncoef > 1;
       const float hx = in->hx, hy = in->hy, hz = in->hz;
-      int s_prev, s_cur, s_next;  // ring A stages of planes x-1, x, x+1
+      // Plane x-1 enters only through its centre values (x neighbours of the
+      // Laplacians), which each thread keeps in registers from the plane it
+      // computed last; so a plane's stage is released as soon as the plane is
+      // computed, and the ring holds planes x and x+1 with two more in flight.
+      float pu[2][3], pd[2][3];  // u and d of plane x-1 at this thread's cells
       bool ok = true;
-      s_prev = ca % NA;
-      ok &= ws_wait(&hd->fullA[s_prev], (ca / NA) & 1u, abort_flag);
+      int s_cur = ca % NA;  // the chunk's first halo plane x0-1: centres only
+      ok &= ws_wait(&hd->fullA[s_cur], (ca / NA) & 1u, abort_flag);
       ++ca;
+      if (ok) {
+        const float* P0 = ringA + s_cur * AF;
+#pragma unroll
+        for (int k = 0; k < 2; ++k)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            const int o = (c * H + ly + 1) * W + lane + 32 * k + 4;
+            pu[k][c] = P0[o];
+            pd[k][c] = P0[o + 3 * H * W];
+          }
+      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&hd->emptyA[s_cur]);
       s_cur = ca % NA;
       ok &= ws_wait(&hd->fullA[s_cur], (ca / NA) & 1u, abort_flag);
       ++ca;
       long long irow = (long long)tc.x0 * g.sxy + (long long)y * g.pz;
       for (int x = tc.x0; x < tc.x1 && ok; ++x, irow += g.sxy) {
-        s_next = ca % NA;
+        const int s_next = ca % NA;
         ok &= ws_wait(&hd->fullA[s_next], (ca / NA) & 1u, abort_flag);
         ++ca;
         const int sb = cb % NB;
         ok &= ws_wait(&hd->fullB[sb], (cb / NB) & 1u, abort_flag);
         ++cb;
         if (!ok) break;
-        const float* Pp = ringA + s_prev * AF;
         const float* Pc = ringA + s_cur * AF;
         const float* Pn = ringA + s_next * AF;
         const float* Bc = ringB + sb * BF;
         const float* Bm = Bc + CF;
 #pragma unroll
         for (int k = 0; k < 2; ++k) {
-          if (!(k == 0 ? act0 : act1)) continue;
           const int lz = lane + 32 * k;
+          if (!(k == 0 ? act0 : act1)) {  // keep the centres for the next plane
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+              const int o = (c * H + ly + 1) * W + lz + 4;
+              pu[k][c] = Pc[o];
+              pd[k][c] = Pc[o + 3 * H * W];
+            }
+            continue;
+          }
           const int z = tc.z0 + lz;
           const long long i = irow + z;
           const float m = Bm[ly * TZ + lz];
@@ -205,54 +236,49 @@ __global__ void __launch_bounds__(TmaF32::THREADS, 2)
             const int o = (c * H + ly + 1) * W + lz + 4;
             const int od = o + 3 * H * W;
             const float u0 = Pc[o], d0 = Pc[od];
-            const float lu = ((Pn[o] + Pp[o]) - 2.0f * u0) * hx +
+            const float lu = ((Pn[o] + pu[k][c]) - 2.0f * u0) * hx +
                              ((Pc[o + W] + Pc[o - W]) - 2.0f * u0) * hy +
                              ((Pc[o + 1] + Pc[o - 1]) - 2.0f * u0) * hz;
             float inc = d0 + m * lu;
             if (visc) {
-              const float ld = ((Pn[od] + Pp[od]) - 2.0f * d0) * hx +
+              const float ld = ((Pn[od] + pd[k][c]) - 2.0f * d0) * hx +
                                ((Pc[od + W] + Pc[od - W]) - 2.0f * d0) * hy +
                                ((Pc[od + 1] + Pc[od - 1]) - 2.0f * d0) * hz;
               inc += e * ld;
             }
+            pu[k][c] = u0;
+            pd[k][c] = d0;
             for (int j = j0; j < j1; ++j)
               inc += in->pat[((long long)in->term_pat[j] * 3 + c) * nc + i] *
                      (float)in->term_scale[j];
-            if (in->use_damp) inc *= in->damp;
-            float unew, cnew;
-            if (in->kahan) {
+            if (use_damp) inc *= damp;
+            float unew;
+            if (kahan) {
               const float cc = Bc[(c * TY + ly) * TZ + lz];
               const float yk = inc - cc;
               unew = u0 + yk;
-              cnew = (unew - u0) - yk;
+              D[(6 + c) * nc + i] = (unew - u0) - yk;
             } else {
-              unew = u0 + inc;
-              cnew = 0.0f;
+              unew = u0 + inc;  // the compensation planes are neither read nor written
             }
             D[c * nc + i] = unew;
             D[(3 + c) * nc + i] = inc;
-            D[(6 + c) * nc + i] = cnew;
             bad |= !isfinite(unew);
             if (snap)
               in->snaps[((((long long)slot * g.nx + x) * g.ny + y) * g.nz + z) * 3 + c] = unew;
           }
           if (bad && in->flags) atomicOr(in->flags, 1);
         }
-        (void)S;
         __syncwarp();
         if (lane == 0) {
-          mbar_arrive(&hd->emptyA[s_prev]);  // plane x-1 is done
+          mbar_arrive(&hd->emptyA[s_cur]);  // plane x is done
           mbar_arrive(&hd->emptyB[sb]);
         }
-        s_prev = s_cur;
         s_cur = s_next;
       }
       if (!ok) break;
       __syncwarp();
-      if (lane == 0) {  // planes x1-1 and x1 are done too
-        mbar_arrive(&hd->emptyA[s_prev]);
-        mbar_arrive(&hd->emptyA[s_cur]);
-      }
+      if (lane == 0) mbar_arrive(&hd->emptyA[s_cur]);  // the closing halo plane x1
     }
   }
   __syncthreads();
@@ -340,9 +366,11 @@ __global__ void __launch_bounds__(TmaF64::THREADS, 2)
       const TmaF64* in;
       int local, lit;
       if (!resolve_tile<TmaF64, BATCH>(one, tab, ninst, t, it, in, local, lit)) continue;
-      const Geom& g = in->g;
+      const Geom& g = in->g;  // hot switches in registers (see step_f32_tma)
       const TileCoord tc = tile_coord_t(g, in->ts, local, TZ, TY);
       double* __restrict__ un = in->state[(lit + 2) % 3];
+      const bool use_damp = in->use_damp != 0;
+      const double dt2 = in->dt2, damp = in->damp;
       const int y = tc.y0 + ly, z = tc.z0 + lane;
       const bool act = (y >= 1 && y <= g.ny - 2 && z >= 1 && z <= g.nz - 2);
       const int j0 = in->term_off ? in->term_off[lit] : 0;
@@ -353,27 +381,40 @@ __global__ void __launch_bounds__(TmaF64::THREADS, 2)
       const long long nc = g.ncell;
       const bool visc = in->ncoef > 1;
       const double ihx2 = in->ihx2, ihy2 = in->ihy2, ihz2 = in->ihz2, inv_dt = in->inv_dt;
-      int s_prev, s_cur, s_next;
+      // plane x-1 enters through its centre values only, kept in registers
+      // (u_curr and u_prev per component), so a plane's stage is released as
+      // soon as the plane is computed (see step_f32_tma)
+      double qc[3], qp[3];
       bool ok = true;
-      s_prev = ca % NA;
-      ok &= ws_wait(&hd->fullA[s_prev], (ca / NA) & 1u, abort_flag);
+      int s_cur = ca % NA;
+      ok &= ws_wait(&hd->fullA[s_cur], (ca / NA) & 1u, abort_flag);
       ++ca;
+      if (ok) {
+        const double* P0 = ringA + s_cur * AD;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const int op = (c * H + ly + 1) * W + lane + 2;
+          qp[c] = P0[op];
+          qc[c] = P0[op + HALF];
+        }
+      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&hd->emptyA[s_cur]);
       s_cur = ca % NA;
       ok &= ws_wait(&hd->fullA[s_cur], (ca / NA) & 1u, abort_flag);
       ++ca;
       long long i = (long long)tc.x0 * g.sxy + (long long)y * g.pz + z;
       for (int x = tc.x0; x < tc.x1 && ok; ++x, i += g.sxy) {
-        s_next = ca % NA;
+        const int s_next = ca % NA;
         ok &= ws_wait(&hd->fullA[s_next], (ca / NA) & 1u, abort_flag);
         ++ca;
         const int sb = cb % NB;
         ok &= ws_wait(&hd->fullB[sb], (cb / NB) & 1u, abort_flag);
         ++cb;
         if (!ok) break;
+        const double* Pc = ringA + s_cur * AD;
+        const double* Pn = ringA + s_next * AD;
         if (act) {
-          const double* Pp = ringA + s_prev * AD;
-          const double* Pc = ringA + s_cur * AD;
-          const double* Pn = ringA + s_next * AD;
           const double* Bm = ringB + sb * BD;
           const double m = Bm[ly * TZ + lane];
           const double e = visc ? Bm[(TY + ly) * TZ + lane] : 0.0;
@@ -384,7 +425,7 @@ __global__ void __launch_bounds__(TmaF64::THREADS, 2)
             const int op = (c * H + ly + 1) * W + lane + 2;  // u_prev component c
             const int oc = op + HALF;                        // u_curr component c
             const double ucc = Pc[oc];
-            const double lap_u = ((Pn[oc] - 2.0 * ucc) + Pp[oc]) * ihx2 +
+            const double lap_u = ((Pn[oc] - 2.0 * ucc) + qc[c]) * ihx2 +
                                  ((Pc[oc + W] - 2.0 * ucc) + Pc[oc - W]) * ihy2 +
                                  ((Pc[oc + 1] - 2.0 * ucc) + Pc[oc - 1]) * ihz2;
             double f = 0.0;
@@ -398,7 +439,7 @@ __global__ void __launch_bounds__(TmaF64::THREADS, 2)
             if (visc) {
               const double vc = (ucc - upc) * inv_dt;
               const double lap_v =
-                  (((Pn[oc] - Pn[op]) * inv_dt - 2.0 * vc) + (Pp[oc] - Pp[op]) * inv_dt) * ihx2 +
+                  (((Pn[oc] - Pn[op]) * inv_dt - 2.0 * vc) + (qc[c] - qp[c]) * inv_dt) * ihx2 +
                   (((Pc[oc + W] - Pc[op + W]) * inv_dt - 2.0 * vc) +
                    (Pc[oc - W] - Pc[op - W]) * inv_dt) *
                       ihy2 +
@@ -407,29 +448,34 @@ __global__ void __launch_bounds__(TmaF64::THREADS, 2)
                       ihz2;
               acc += e * lap_v;
             }
-            double unew = (2.0 * ucc - upc) + in->dt2 * acc;
-            if (in->use_damp) unew = ucc + in->damp * (unew - ucc);
+            qc[c] = ucc;
+            qp[c] = upc;
+            double unew = (2.0 * ucc - upc) + dt2 * acc;
+            if (use_damp) unew = ucc + damp * (unew - ucc);
             un[c * nc + i] = unew;
             bad |= !isfinite(unew);
             if (snap)
               in->snaps[((((long long)slot * g.nx + x) * g.ny + y) * g.nz + z) * 3 + c] = unew;
           }
           if (bad && in->flags) atomicOr(in->flags, 1);
+        } else {  // keep the centres for the next plane
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            const int op = (c * H + ly + 1) * W + lane + 2;
+            qp[c] = Pc[op];
+            qc[c] = Pc[op + HALF];
+          }
         }
         __syncwarp();
         if (lane == 0) {
-          mbar_arrive(&hd->emptyA[s_prev]);
+          mbar_arrive(&hd->emptyA[s_cur]);  // plane x is done
           mbar_arrive(&hd->emptyB[sb]);
         }
-        s_prev = s_cur;
         s_cur = s_next;
       }
       if (!ok) break;
       __syncwarp();
-      if (lane == 0) {
-        mbar_arrive(&hd->emptyA[s_prev]);
-        mbar_arrive(&hd->emptyA[s_cur]);
-      }
+      if (lane == 0) mbar_arrive(&hd->emptyA[s_cur]);  // the closing halo plane x1
     }
   }
   __syncthreads();

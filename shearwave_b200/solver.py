@@ -8,9 +8,14 @@ arrays to the device (torch owns the memory) and sequences the C-ABI calls.
 
 Precision (``opts["precision"]``):
 
-* ``"mixed"`` (default): FP32 fields in increment form with a Kahan-
-  compensated displacement, FP64 CG projection; returns float32 like the
-  reference.
+* ``"mixed"`` (default): FP32 fields in increment form (displacement and
+  per-step increment stored, so the velocity never comes from a difference
+  of two nearly equal displacements), FP64 projection; returns float32 like
+  the reference.  ``opts["kahan"]=True`` adds a compensated displacement
+  sum (12 more bytes read and written per cell-step) for very long runs:
+  without it the measured error against the FP64 form is 2e-7 (u) and
+  2.4e-6 (v) relative L2 after 4000 steps of the 256x256x384 layered case,
+  growing about linearly with the step count.
 * ``"fp64"``: the plain FP64 form, the reference's arithmetic in float64
   (matches an FP64 run of the reference to relative L2 <= 1e-10); returns
   float64.
@@ -558,7 +563,7 @@ class _Solve:
             self.tev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
             self.tev[0].record()
         run = self.run = _Run(shape, (dX, dY, dZ), dT, n_steps, self.prec,
-                              opts.get("kahan", True), dev)
+                              opts.get("kahan", False), dev)
         run.desc.vel_damp = float(opts.get("vel_damp", 0.0))
         run.desc.kernel = 0 if kern == "tma" else 1
         run.desc.xchunk = int(opts.get("xchunk", 0) or 0)
@@ -745,7 +750,7 @@ def shear_fdtd(
     Additional opts: ``precision`` ("mixed" default, or "fp64"), ``projection``
     ("auto" default: the reference's CG for fp64, and for mixed the exact
     direct spectral Poisson solve when ``poisson_tol <= 1e-8``; or "cg" /
-    "spectral" explicitly), ``kahan`` (True), ``step_kernel`` ("tma" default, or "direct"), ``xchunk`` (planes
+    "spectral" explicitly), ``kahan`` (False: compensated displacement sum), ``step_kernel`` ("tma" default, or "direct"), ``xchunk`` (planes
     per tile along x, 0 = automatic), ``steps_per_pass`` (mixed form: 2
     fuses two time steps per pass over HBM; 1 or 0 (default) one step per
     launch), ``cuda_graph`` (True: long step runs replay one instantiated CUDA

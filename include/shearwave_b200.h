@@ -80,6 +80,21 @@ size_t sw_fdtd_desc_size(void);
 /* Number of kernels this library has launched in the process so far. */
 uint64_t sw_launch_count(void);
 
+/* Launch-shape knobs of the step kernels (no counterpart in the reference:
+ * the autotuner in shearwave_b200/tune.py sweeps them per workload).  They
+ * change how the grid is cut into tiles, never the results.  Process-wide;
+ * set them between solves, not while one is running.                      */
+enum sw_tune_knob {
+  SW_TUNE_STEP_CTAS_PER_SM = 0,    /* resident step CTAs per SM: 1 or 2 (default 2) */
+  SW_TUNE_BATCH_TILES_PER_CTA = 1, /* batched launches: tiles per CTA, 1..64 (8)   */
+  SW_TUNE_XCHUNK = 2,              /* planes per x chunk, 0 = automatic (0)          */
+  SW_TUNE_COUNT = 3
+};
+/* SW_EINVAL for an unknown knob or a value out of range. */
+int sw_tune_set(int knob, int value);
+/* Current value, or -1 for an unknown knob. */
+int sw_tune_get(int knob);
+
 /* ---- collocated FD operators on dense arrays (solver.py:686-729) ------- */
 /* laplacian_center: interior 7-point Laplacian, zero shell. */
 int sw_laplacian(int dtype, const void* f, void* out, int nx, int ny, int nz, double dX,

@@ -85,6 +85,8 @@ _SIGNATURES = {
     "sw_pitch": ([C.c_int], C.c_int),
     "sw_fdtd_desc_size": ([], _sz),
     "sw_launch_count": ([], C.c_uint64),
+    "sw_tune_set": ([C.c_int, C.c_int], C.c_int),
+    "sw_tune_get": ([C.c_int], C.c_int),
     "sw_laplacian": ([C.c_int, _vp, _vp, C.c_int, C.c_int, C.c_int, _f64, _f64, _f64, _vp],
                      C.c_int),
     "sw_divergence": ([C.c_int, _vp, _vp, _vp, _vp, C.c_int, C.c_int, C.c_int, _f64, _f64, _f64,

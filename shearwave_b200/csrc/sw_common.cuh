@@ -183,6 +183,11 @@ __device__ inline bool interior(const Geom& g, int x, int y, int z) {
 // Host-side error plumbing
 // ---------------------------------------------------------------------------
 void set_error(const char* fmt, ...);
+// Launch-shape knob (enum sw_tune_knob), process-wide.
+int tune_get(int knob);
+constexpr int kNumSMs = 148;  // B200
+// Resident CTA slots of the step kernels (SMs x CTAs per SM).
+inline int step_slots() { return kNumSMs * tune_get(SW_TUNE_STEP_CTAS_PER_SM); }
 int cuda_status(cudaError_t e, const char* what);
 // Count kernel launches issued by this library (exported as sw_launch_count).
 void count_launches(unsigned long long n);

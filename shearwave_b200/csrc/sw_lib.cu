@@ -21,6 +21,10 @@ static std::atomic<unsigned long long> g_launches{0};
 
 void count_launches(unsigned long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
+static std::atomic<int> g_tune[SW_TUNE_COUNT] = {{2}, {8}, {0}};
+
+int tune_get(int knob) { return (knob >= 0 && knob < SW_TUNE_COUNT) ? g_tune[knob].load() : -1; }
+
 int cuda_status(cudaError_t e, const char* what) {
   set_error("%s: %s (%s)", what, cudaGetErrorString(e), cudaGetErrorName(e));
   return SW_ECUDA;
@@ -43,3 +47,15 @@ extern "C" int sw_pitch(int nz) { return nz > 0 ? sw::pad_pitch(nz) : 0; }
 extern "C" size_t sw_fdtd_desc_size(void) { return sizeof(sw_fdtd_desc); }
 
 extern "C" uint64_t sw_launch_count(void) { return sw::g_launches.load(); }
+
+extern "C" int sw_tune_set(int knob, int value) {
+  static const int lo[SW_TUNE_COUNT] = {1, 1, 0}, hi[SW_TUNE_COUNT] = {2, 64, 1 << 20};
+  if (knob < 0 || knob >= SW_TUNE_COUNT || value < lo[knob] || value > hi[knob]) {
+    sw::set_error("sw_tune_set: knob %d does not take the value %d", knob, value);
+    return SW_EINVAL;
+  }
+  sw::g_tune[knob].store(value);
+  return SW_OK;
+}
+
+extern "C" int sw_tune_get(int knob) { return sw::tune_get(knob); }

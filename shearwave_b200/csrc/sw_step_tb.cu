@@ -73,7 +73,8 @@ __device__ inline int floor4(int v) { return v & ~3; }  // floor to a multiple o
 template <bool BATCH>
 __global__ void __launch_bounds__(TmaF32TB::THREADS, 1)
     step_f32_fused2(const __grid_constant__ TmaF32TB one, const TmaF32TB* __restrict__ tab,
-                    int ninst, int ntiles, int it, const int* __restrict__ it_dev) {
+                    int ninst, int ntiles, int it, const int* __restrict__ it_dev,
+                    int* /*queues: unused; keeps the step kernels' parameters alike*/) {
   if (it_dev != nullptr) it += *it_dev;  // step counter kept on the device (graph replays)
   using T = TmaF32TB;
   constexpr int NA = T::NA, NB = T::NB, NL = T::NL, W = T::W, H = T::H, WB = T::WB, HB = T::HB;
@@ -458,7 +459,7 @@ const void* step_f32_fused2_ptr() { return reinterpret_cast<const void*>(step_f3
 void launch_fused2_raw(const TmaF32TB& t, int it, cudaStream_t s) {
   if (t.ts.count == 0) return;
   step_f32_fused2<false><<<std::min(t.ts.count, 148), TmaF32TB::THREADS, tb_smem_bytes(), s>>>(
-      t, nullptr, 1, t.ts.count, it, nullptr);
+      t, nullptr, 1, t.ts.count, it, nullptr, nullptr);
 }
 
 int launch_fused2(const StepArgs& a, int xchunk, int it, cudaStream_t s) {
@@ -469,8 +470,8 @@ int launch_fused2(const StepArgs& a, int xchunk, int it, cudaStream_t s) {
   if (rc != SW_OK) return rc;
   if (t.ts.count == 0) return SW_OK;
   const int grid = std::min(t.ts.count, 148);
-  step_f32_fused2<false><<<grid, TmaF32TB::THREADS, tb_smem_bytes(), s>>>(t, nullptr, 1,
-                                                                          t.ts.count, it, nullptr);
+  step_f32_fused2<false><<<grid, TmaF32TB::THREADS, tb_smem_bytes(), s>>>(
+      t, nullptr, 1, t.ts.count, it, nullptr, nullptr);
   count_launches(1);
   SW_CHECK_LAUNCH("fused two-step kernel");
   return SW_OK;
@@ -482,7 +483,7 @@ int launch_fused2_batch(const void* d_tab, int ninst, int ntiles, int it, cudaSt
   if (ntiles == 0) return SW_OK;
   TmaF32TB dummy{};
   step_f32_fused2<true><<<std::min(ntiles, 148), TmaF32TB::THREADS, tb_smem_bytes(), s>>>(
-      dummy, (const TmaF32TB*)d_tab, ninst, ntiles, it, nullptr);
+      dummy, (const TmaF32TB*)d_tab, ninst, ntiles, it, nullptr, nullptr);
   count_launches(1);
   SW_CHECK_LAUNCH("fused two-step kernel (batch)");
   return SW_OK;

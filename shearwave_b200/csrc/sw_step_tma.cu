@@ -84,8 +84,12 @@ int encode_tmap_4d(CUtensorMap* map, CUtensorMapDataType dt, void* base, const u
 template <bool BATCH>
 __global__ void __launch_bounds__(TmaF32::THREADS, 2)
     step_f32_tma(const __grid_constant__ TmaF32 one, const TmaF32* __restrict__ tab, int ninst,
-                 int ntiles, int it, const int* __restrict__ it_dev) {
+                 int ntiles, int it, const int* __restrict__ it_dev, int* queues) {
   if (it_dev != nullptr) it += *it_dev;  // step counter kept on the device (graph replays)
+  // batched launches take tiles from queue it & 1 and reset the other one
+  // for the next launch of the stream
+  int* queue = (BATCH && queues != nullptr) ? queues + (it & 1) : nullptr;
+  if (queue != nullptr && blockIdx.x == 0 && threadIdx.x == 0) queues[(it + 1) & 1] = 0;
   constexpr int NA = TmaF32::NA, NB = TmaF32::NB, W = TmaF32::W, H = TmaF32::H;
   constexpr int TZ = TmaF32::TZ, TY = TmaF32::TY;
   constexpr int AF = TmaF32::A_STAGE / 4, BF = TmaF32::B_STAGE / 4;  // floats per stage
@@ -120,10 +124,22 @@ __global__ void __launch_bounds__(TmaF32::THREADS, 2)
     // ------------------------------- producer -----------------------------
     if (lane == 0) {
       uint32_t pa = 0, pb = 0;  // loads issued into ring A / ring B
-      for (int t = blockIdx.x; t < ntiles && !*abort_flag; t += gridDim.x) {
-        const TmaF32* in;
-        int local, lit;
-        if (!resolve_tile<TmaF32, BATCH>(one, tab, ninst, t, it, in, local, lit)) continue;
+      int stride_next = blockIdx.x;
+      while (!*abort_flag) {
+        const int t = next_tile(queue, stride_next);
+        if (t >= ntiles) {  // end of this CTA's work: arm one stage without a copy
+          const int sa = pa % NA;
+          if (!ws_wait(&hd->emptyA[sa], ((pa / NA) & 1u) ^ 1u, abort_flag)) break;
+          tile_slots(base)[sa] = -1;
+          mbar_arrive(&hd->fullA[sa]);
+          ++pa;
+          break;
+        }
+        const int k = BATCH ? find_solve(tab, ninst, t) : 0;
+        const TmaF32* in = BATCH ? &tab[k] : &one;
+        const int local = BATCH ? t - in->tile_base : t;
+        const int lit = it - in->it_begin;
+        if (lit < 0 || lit >= in->n_steps) continue;
         const TileCoord tc = tile_coord_t(in->g, in->ts, local, TZ, TY);
         const CUtensorMap* tma = &in->tm[lit % 3];
         const CUtensorMap* tmc = &in->tmc[lit % 3];
@@ -131,6 +147,10 @@ __global__ void __launch_bounds__(TmaF32::THREADS, 2)
         for (int p = tc.x0 - 1; p <= tc.x1 && !*abort_flag; ++p) {
           const int sa = pa % NA;
           if (!ws_wait(&hd->emptyA[sa], ((pa / NA) & 1u) ^ 1u, abort_flag)) break;
+          if (p == tc.x0 - 1) {
+            tile_slots(base)[sa] = t;
+            solve_slots(base)[sa] = k;
+          }
           fence_proxy_async_smem();
           mbar_arrive_expect_tx(&hd->fullA[sa], TmaF32::A_BYTES);
           tma_load_4d(ringA + sa * AF, tma, &hd->fullA[sa], tc.z0 - 4, tc.y0 - 1, p, 0);
@@ -151,10 +171,14 @@ __global__ void __launch_bounds__(TmaF32::THREADS, 2)
     // ------------------------------- consumers ----------------------------
     const int ly = warp;
     uint32_t ca = 0, cb = 0;  // planes consumed from ring A / ring B
-    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-      const TmaF32* in;
-      int local, lit;
-      if (!resolve_tile<TmaF32, BATCH>(one, tab, ninst, t, it, in, local, lit)) continue;
+    while (true) {
+      int s_cur = ca % NA;  // the tile's first plane (its halo plane x0-1)
+      if (!ws_wait(&hd->fullA[s_cur], (ca / NA) & 1u, abort_flag)) break;
+      const int t = tile_slots(base)[s_cur];
+      if (t < 0) break;
+      const TmaF32* in = BATCH ? &tab[solve_slots(base)[s_cur]] : &one;
+      const int local = BATCH ? t - in->tile_base : t;
+      const int lit = it - in->it_begin;
       // the per-cell switches in registers: the table lives in global memory and
       // the stores below could otherwise force reloads of its fields (fields
       // used only on push / snapshot steps are read where they are used)
@@ -182,10 +206,8 @@ __global__ void __launch_bounds__(TmaF32::THREADS, 2)
       // computed, and the ring holds planes x and x+1 with two more in flight.
       float pu[2][3], pd[2][3];  // u and d of plane x-1 at this thread's cells
       bool ok = true;
-      int s_cur = ca % NA;  // the chunk's first halo plane x0-1: centres only
-      ok &= ws_wait(&hd->fullA[s_cur], (ca / NA) & 1u, abort_flag);
-      ++ca;
-      if (ok) {
+      ++ca;  // plane x0-1 (waited for above): centres only
+      {
         const float* P0 = ringA + s_cur * AF;
 #pragma unroll
         for (int k = 0; k < 2; ++k)
@@ -298,8 +320,10 @@ __global__ void __launch_bounds__(TmaF32::THREADS, 2)
 template <bool BATCH>
 __global__ void __launch_bounds__(TmaF64::THREADS, 2)
     step_f64_tma(const __grid_constant__ TmaF64 one, const TmaF64* __restrict__ tab, int ninst,
-                 int ntiles, int it, const int* __restrict__ it_dev) {
+                 int ntiles, int it, const int* __restrict__ it_dev, int* queues) {
   if (it_dev != nullptr) it += *it_dev;  // step counter kept on the device (graph replays)
+  int* queue = (BATCH && queues != nullptr) ? queues + (it & 1) : nullptr;  // see step_f32_tma
+  if (queue != nullptr && blockIdx.x == 0 && threadIdx.x == 0) queues[(it + 1) & 1] = 0;
   constexpr int NA = TmaF64::NA, NB = TmaF64::NB, W = TmaF64::W, H = TmaF64::H;
   constexpr int TZ = TmaF64::TZ, TY = TmaF64::TY;
   constexpr int AD = TmaF64::A_STAGE / 8, BD = TmaF64::B_STAGE / 8, HALF = TmaF64::HALF / 8;
@@ -332,10 +356,22 @@ __global__ void __launch_bounds__(TmaF64::THREADS, 2)
   if (warp == TmaF64::CONSUMER_WARPS) {
     if (lane == 0) {
       uint32_t pa = 0, pb = 0;
-      for (int t = blockIdx.x; t < ntiles && !*abort_flag; t += gridDim.x) {
-        const TmaF64* in;
-        int local, lit;
-        if (!resolve_tile<TmaF64, BATCH>(one, tab, ninst, t, it, in, local, lit)) continue;
+      int stride_next = blockIdx.x;
+      while (!*abort_flag) {
+        const int t = next_tile(queue, stride_next);
+        if (t >= ntiles) {  // end of this CTA's work: arm one stage without a copy
+          const int sa = pa % NA;
+          if (!ws_wait(&hd->emptyA[sa], ((pa / NA) & 1u) ^ 1u, abort_flag)) break;
+          tile_slots(base)[sa] = -1;
+          mbar_arrive(&hd->fullA[sa]);
+          ++pa;
+          break;
+        }
+        const int k = BATCH ? find_solve(tab, ninst, t) : 0;
+        const TmaF64* in = BATCH ? &tab[k] : &one;
+        const int local = BATCH ? t - in->tile_base : t;
+        const int lit = it - in->it_begin;
+        if (lit < 0 || lit >= in->n_steps) continue;
         const TileCoord tc = tile_coord_t(in->g, in->ts, local, TZ, TY);
         const CUtensorMap* tmp = &in->tm[lit % 3];
         const CUtensorMap* tmc = &in->tm[(lit + 1) % 3];
@@ -343,6 +379,10 @@ __global__ void __launch_bounds__(TmaF64::THREADS, 2)
         for (int p = tc.x0 - 1; p <= tc.x1 && !*abort_flag; ++p) {
           const int sa = pa % NA;
           if (!ws_wait(&hd->emptyA[sa], ((pa / NA) & 1u) ^ 1u, abort_flag)) break;
+          if (p == tc.x0 - 1) {
+            tile_slots(base)[sa] = t;
+            solve_slots(base)[sa] = k;
+          }
           fence_proxy_async_smem();
           mbar_arrive_expect_tx(&hd->fullA[sa], 2 * TmaF64::BOX_BYTES);
           tma_load_4d(ringA + sa * AD, tmp, &hd->fullA[sa], tc.z0 - 2, tc.y0 - 1, p, 0);
@@ -362,10 +402,14 @@ __global__ void __launch_bounds__(TmaF64::THREADS, 2)
   } else {
     const int ly = warp;
     uint32_t ca = 0, cb = 0;
-    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-      const TmaF64* in;
-      int local, lit;
-      if (!resolve_tile<TmaF64, BATCH>(one, tab, ninst, t, it, in, local, lit)) continue;
+    while (true) {
+      int s_cur = ca % NA;  // the tile's first plane (its halo plane x0-1)
+      if (!ws_wait(&hd->fullA[s_cur], (ca / NA) & 1u, abort_flag)) break;
+      const int t = tile_slots(base)[s_cur];
+      if (t < 0) break;
+      const TmaF64* in = BATCH ? &tab[solve_slots(base)[s_cur]] : &one;
+      const int local = BATCH ? t - in->tile_base : t;
+      const int lit = it - in->it_begin;
       const Geom& g = in->g;  // hot switches in registers (see step_f32_tma)
       const TileCoord tc = tile_coord_t(g, in->ts, local, TZ, TY);
       double* __restrict__ un = in->state[(lit + 2) % 3];
@@ -386,10 +430,8 @@ __global__ void __launch_bounds__(TmaF64::THREADS, 2)
       // soon as the plane is computed (see step_f32_tma)
       double qc[3], qp[3];
       bool ok = true;
-      int s_cur = ca % NA;
-      ok &= ws_wait(&hd->fullA[s_cur], (ca / NA) & 1u, abort_flag);
-      ++ca;
-      if (ok) {
+      ++ca;  // plane x0-1 (waited for above): centres only
+      {
         const double* P0 = ringA + s_cur * AD;
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
@@ -562,7 +604,8 @@ static int coef_components(const StepArgs& a, size_t es, int* ncoef) {
 int make_tma_f32(const StepArgs& a, int xchunk, TmaF32* t) {
   *t = TmaF32{};
   t->g = a.g;
-  const int xc = xchunk > 0 ? xchunk : tma_xchunk(a.g, TmaF32::TZ, TmaF32::TY, 2 * 148);
+  const int xt = xchunk > 0 ? xchunk : tune_get(SW_TUNE_XCHUNK);
+  const int xc = xt > 0 ? xt : tma_xchunk(a.g, TmaF32::TZ, TmaF32::TY, step_slots());
   t->ts = make_tiles_t(a.g, xc, TmaF32::TZ, TmaF32::TY);
   int rc = coef_components(a, 4, &t->ncoef);
   if (rc != SW_OK) return rc;
@@ -608,7 +651,8 @@ int make_tma_f32(const StepArgs& a, int xchunk, TmaF32* t) {
 int make_tma_f64(const StepArgs& a, int xchunk, TmaF64* t) {
   *t = TmaF64{};
   t->g = a.g;
-  const int xc = xchunk > 0 ? xchunk : tma_xchunk(a.g, TmaF64::TZ, TmaF64::TY, 2 * 148);
+  const int xt = xchunk > 0 ? xchunk : tune_get(SW_TUNE_XCHUNK);
+  const int xc = xt > 0 ? xt : tma_xchunk(a.g, TmaF64::TZ, TmaF64::TY, step_slots());
   t->ts = make_tiles_t(a.g, xc, TmaF64::TZ, TmaF64::TY);
   int rc = coef_components(a, 8, &t->ncoef);
   if (rc != SW_OK) return rc;
@@ -672,11 +716,12 @@ int graph_loop(void* func, const Inst& t, int grid, int threads, size_t smem, in
   const Inst* tab = nullptr;
   int ninst = 1, ntiles = t.ts.count;
   const int* itd = clock;
+  int* queues = nullptr;
   std::vector<int> offs(seg);
   for (int k = 0; k < seg && e == cudaSuccess; ++k) {
     offs[k] = k * per_launch;
-    void* args[] = {(void*)&t, (void*)&tab, (void*)&ninst, (void*)&ntiles, (void*)&offs[k],
-                    (void*)&itd};
+    void* args[] = {(void*)&t,        (void*)&tab, (void*)&ninst, (void*)&ntiles,
+                    (void*)&offs[k], (void*)&itd, (void*)&queues};
     cudaKernelNodeParams p{};
     p.func = func;
     p.gridDim = dim3(grid);
@@ -722,14 +767,14 @@ int launch_steps_tma(const StepArgs& a, int xchunk, int it0, int nsteps, cudaStr
     rc = make_tma_f64(a, xchunk, &t);
     if (rc != SW_OK) return rc;
     if (t.ts.count == 0) return SW_OK;
-    const int grid = std::min(t.ts.count, 148 * 2);
+    const int grid = std::min(t.ts.count, step_slots());
     int done = 0;
     rc = graph_loop(reinterpret_cast<void*>(step_f64_tma<false>), t, grid, TmaF64::THREADS, smem,
                     1, 32, a.clock, it0, nsteps, s, &done);
     if (rc != SW_OK) return rc;
     for (int it = it0 + done; it < it0 + nsteps; ++it)
       step_f64_tma<false><<<grid, TmaF64::THREADS, smem, s>>>(t, nullptr, 1, t.ts.count, it,
-                                                              nullptr);
+                                                              nullptr, nullptr);
     count_launches((unsigned long long)(nsteps - done));
     SW_CHECK_LAUNCH("step (tma)");
     return SW_OK;
@@ -748,7 +793,7 @@ int launch_steps_tma(const StepArgs& a, int xchunk, int it0, int nsteps, cudaStr
       rc = launch_fused2_prepare();
       if (rc != SW_OK) return rc;
     }
-    const int grid = std::min(t.ts.count, 148 * 2);
+    const int grid = std::min(t.ts.count, step_slots());
     unsigned long long n_launch = 0;
     int done = 0;
     if (fuse && tb.ts.count > 0)
@@ -765,7 +810,7 @@ int launch_steps_tma(const StepArgs& a, int xchunk, int it0, int nsteps, cudaStr
         it += 2;
       } else {
         step_f32_tma<false><<<grid, TmaF32::THREADS, smem, s>>>(t, nullptr, 1, t.ts.count, it,
-                                                                nullptr);
+                                                                nullptr, nullptr);
         it += 1;
       }
       ++n_launch;
@@ -780,20 +825,20 @@ int launch_steps_tma(const StepArgs& a, int xchunk, int it0, int nsteps, cudaStr
 }
 
 int launch_steps_tma_batch(int precision, const void* d_tab, int ninst, int ntiles, int it,
-                           cudaStream_t s) {
+                           int* queues, cudaStream_t s) {
   int rc = set_smem_attr(precision);
   if (rc != SW_OK) return rc;
   if (ntiles == 0) return SW_OK;
   const size_t smem = tma_smem_bytes(precision);
-  const int grid = std::min(ntiles, 148 * 2);
+  const int grid = std::min(ntiles, step_slots());
   if (precision == SW_PLAIN_F64) {
     TmaF64 dummy{};
     step_f64_tma<true><<<grid, TmaF64::THREADS, smem, s>>>(dummy, (const TmaF64*)d_tab, ninst,
-                                                          ntiles, it, nullptr);
+                                                          ntiles, it, nullptr, queues);
   } else {
     TmaF32 dummy{};
     step_f32_tma<true><<<grid, TmaF32::THREADS, smem, s>>>(dummy, (const TmaF32*)d_tab, ninst,
-                                                          ntiles, it, nullptr);
+                                                          ntiles, it, nullptr, queues);
   }
   count_launches(1);
   SW_CHECK_LAUNCH("step (tma, batch)");
@@ -808,23 +853,70 @@ int launch_steps_tma_batch(int precision, const void* d_tab, int ninst, int ntil
 namespace sw {
 namespace {
 
+// Order in which the running solves enter a batched launch's tile range:
+// solves with the longest x columns first, so that the launch-wide tile
+// queue hands out the longest tiles first.
+static std::vector<int> batch_order(const sw_fdtd_desc* descs, const std::vector<int>& run) {
+  std::vector<int> ord(run);
+  std::stable_sort(ord.begin(), ord.end(),
+                   [&](int a, int b) { return descs[a].nx > descs[b].nx; });
+  return ord;
+}
+
+// Target planes per x chunk for a batched launch: about
+// SW_TUNE_BATCH_TILES_PER_CTA (8) tiles per resident CTA over all running
+// solves, at least 8 planes (each chunk re-reads two halo planes).
+static int batch_xchunk(const sw_fdtd_desc* descs, const std::vector<int>& run, int tz, int ty) {
+  long long work = 0;
+  for (int i : run) {
+    const long long cols = (long long)((descs[i].nz + tz - 1) / tz) * ((descs[i].ny + ty - 1) / ty);
+    work += cols * std::max(0, descs[i].nx - 2);
+  }
+  const long long want = (long long)tune_get(SW_TUNE_BATCH_TILES_PER_CTA) * step_slots();
+  return (int)std::max<long long>(8, (work + want - 1) / want);
+}
+
+// A solve's chunk length for target `xc`: the interior planes split into
+// equal chunks no longer than xc.  The solve's own xchunk, then the
+// SW_TUNE_XCHUNK knob, when set, win.
+static int solve_xchunk(const sw_fdtd_desc& d, int xc) {
+  if (d.xchunk > 0) return d.xchunk;
+  if (tune_get(SW_TUNE_XCHUNK) > 0) return tune_get(SW_TUNE_XCHUNK);
+  const int nxi = std::max(1, d.nx - 2);
+  const int nch = (nxi + xc - 1) / xc;
+  return (nxi + nch - 1) / nch;
+}
+
+template <typename Inst>
+int make_inst(const StepArgs& a, int xchunk, Inst* t);
+template <>
+int make_inst<TmaF32>(const StepArgs& a, int xchunk, TmaF32* t) {
+  return make_tma_f32(a, xchunk, t);
+}
+template <>
+int make_inst<TmaF64>(const StepArgs& a, int xchunk, TmaF64* t) {
+  return make_tma_f64(a, xchunk, t);
+}
+
+// Table of the solves running at step `it`, in batch_order, with their tile
+// ranges laid end to end.
 template <typename Inst>
 int build_batch(const sw_fdtd_desc* descs, const int32_t* begins, int n, int it,
-                std::vector<Inst>& tab, int* ntiles);
-
-template <>
-int build_batch<TmaF32>(const sw_fdtd_desc* descs, const int32_t* begins, int n, int it,
-                        std::vector<TmaF32>& tab, int* ntiles) {
+                std::vector<Inst>& tab, int* ntiles) {
   tab.clear();
-  int nt = 0;
+  std::vector<int> run;
   for (int i = 0; i < n; ++i) {
     const int lit = it - (begins ? begins[i] : 0);
-    if (lit < 0 || lit >= descs[i].n_steps) continue;
+    if (lit >= 0 && lit < descs[i].n_steps) run.push_back(i);
+  }
+  const int xc = batch_xchunk(descs, run, Inst::TZ, Inst::TY);
+  int nt = 0;
+  for (int i : batch_order(descs, run)) {
     StepArgs a;
     int rc = make_step_args(&descs[i], &a);
     if (rc != SW_OK) return rc;
-    TmaF32 t;
-    rc = make_tma_f32(a, descs[i].xchunk > 0 ? descs[i].xchunk : 16, &t);
+    Inst t;
+    rc = make_inst<Inst>(a, solve_xchunk(descs[i], xc), &t);
     if (rc != SW_OK) return rc;
     t.it_begin = begins ? begins[i] : 0;
     t.tile_base = nt;
@@ -835,36 +927,20 @@ int build_batch<TmaF32>(const sw_fdtd_desc* descs, const int32_t* begins, int n,
   return SW_OK;
 }
 
-template <>
-int build_batch<TmaF64>(const sw_fdtd_desc* descs, const int32_t* begins, int n, int it,
-                        std::vector<TmaF64>& tab, int* ntiles) {
-  tab.clear();
-  int nt = 0;
-  for (int i = 0; i < n; ++i) {
-    const int lit = it - (begins ? begins[i] : 0);
-    if (lit < 0 || lit >= descs[i].n_steps) continue;
-    StepArgs a;
-    int rc = make_step_args(&descs[i], &a);
-    if (rc != SW_OK) return rc;
-    TmaF64 t;
-    rc = make_tma_f64(a, descs[i].xchunk > 0 ? descs[i].xchunk : 16, &t);
-    if (rc != SW_OK) return rc;
-    t.it_begin = begins ? begins[i] : 0;
-    t.tile_base = nt;
-    nt += t.ts.count;
-    tab.push_back(t);
-  }
-  *ntiles = nt;
-  return SW_OK;
-}
+// A batch table starts with the two launch-wide tile queues (zeroed at the
+// start of every call); the solve arrays follow at kBatchHeader.
+constexpr size_t kBatchHeader = 256;
 
 // Mixed form: two steps per launch whenever every running solve runs both
 // steps of the pair; one-step launches around starts and ends.  The table
 // holds the one-step instance array, then the fused-kernel array.
 int batch_steps_mixed(const sw_fdtd_desc* descs, const int32_t* begins, int n, int it0,
                       int nsteps, void* table, cudaStream_t s) {
-  char* tab_single = (char*)table;
-  char* tab_fused = (char*)table + (size_t)n * sizeof(TmaF32);
+  int* queues = (int*)table;
+  char* tab_single = (char*)table + kBatchHeader;
+  char* tab_fused = tab_single + (size_t)n * sizeof(TmaF32);
+  cudaError_t e0 = cudaMemsetAsync(queues, 0, 2 * sizeof(int), s);
+  if (e0 != cudaSuccess) return cuda_status(e0, "batch queue reset");
   bool fuse_ok = true;
   for (int i = 0; i < n; ++i) fuse_ok &= (descs[i].steps_per_pass == 2);
   auto active = [&](int i, int it) {
@@ -899,13 +975,13 @@ int batch_steps_mixed(const sw_fdtd_desc* descs, const int32_t* begins, int n, i
       tsingle.clear();
       tfused.clear();
       ntiles = 0;
-      for (int i = 0; i < n; ++i) {
-        cur[i] = active(i, it) ? 1 : 0;
-        if (!cur[i]) continue;
-        StepArgs a;
-        int rc = make_step_args(&descs[i], &a);
-        if (rc != SW_OK) return rc;
-        if (kind == 1) {
+      for (int i = 0; i < n; ++i) cur[i] = active(i, it) ? 1 : 0;
+      if (kind == 1) {
+        for (int i = 0; i < n; ++i) {
+          if (!cur[i]) continue;
+          StepArgs a;
+          int rc = make_step_args(&descs[i], &a);
+          if (rc != SW_OK) return rc;
           TmaF32TB t;
           rc = make_tma_f32_tb(a, descs[i].xchunk > 0 ? descs[i].xchunk : 24, &t);
           if (rc != SW_OK) return rc;
@@ -913,15 +989,10 @@ int batch_steps_mixed(const sw_fdtd_desc* descs, const int32_t* begins, int n, i
           t.tile_base = ntiles;
           ntiles += t.ts.count;
           tfused.push_back(t);
-        } else {
-          TmaF32 t;
-          rc = make_tma_f32(a, descs[i].xchunk > 0 ? descs[i].xchunk : 16, &t);
-          if (rc != SW_OK) return rc;
-          t.it_begin = begins ? begins[i] : 0;
-          t.tile_base = ntiles;
-          ntiles += t.ts.count;
-          tsingle.push_back(t);
         }
+      } else {
+        int rc = build_batch<TmaF32>(descs, begins, n, it, tsingle, &ntiles);
+        if (rc != SW_OK) return rc;
       }
       cudaError_t e = kind == 1 ? cudaMemcpyAsync(tab_fused, tfused.data(),
                                                   tfused.size() * sizeof(TmaF32TB),
@@ -937,7 +1008,8 @@ int batch_steps_mixed(const sw_fdtd_desc* descs, const int32_t* begins, int n, i
       rc = launch_fused2_batch(tab_fused, (int)tfused.size(), ntiles, it, s);
       it += 2;
     } else {
-      rc = launch_steps_tma_batch(SW_MIXED_F32, tab_single, (int)tsingle.size(), ntiles, it, s);
+      rc = launch_steps_tma_batch(SW_MIXED_F32, tab_single, (int)tsingle.size(), ntiles, it,
+                                  queues, s);
       it += 1;
     }
     if (rc != SW_OK) return rc;
@@ -947,7 +1019,11 @@ int batch_steps_mixed(const sw_fdtd_desc* descs, const int32_t* begins, int n, i
 
 template <typename Inst>
 int batch_steps(int precision, const sw_fdtd_desc* descs, const int32_t* begins, int n, int it0,
-                int nsteps, void* table, cudaStream_t s) {
+                int nsteps, void* table_base, cudaStream_t s) {
+  int* queues = (int*)table_base;
+  char* table = (char*)table_base + kBatchHeader;
+  cudaError_t e0 = cudaMemsetAsync(queues, 0, 2 * sizeof(int), s);
+  if (e0 != cudaSuccess) return cuda_status(e0, "batch queue reset");
   std::vector<Inst> tab;
   std::vector<int> active(n, -1);
   int ntiles = 0;
@@ -975,7 +1051,7 @@ int batch_steps(int precision, const sw_fdtd_desc* descs, const int32_t* begins,
       have = true;
     }
     if (tab.empty()) continue;
-    int rc = launch_steps_tma_batch(precision, table, (int)tab.size(), ntiles, it, s);
+    int rc = launch_steps_tma_batch(precision, table, (int)tab.size(), ntiles, it, queues, s);
     if (rc != SW_OK) return rc;
   }
   return SW_OK;
@@ -988,7 +1064,7 @@ using namespace sw;
 
 extern "C" size_t sw_fdtd_batch_table_bytes(int n) {
   if (n <= 0) return 0;
-  return (size_t)n * std::max(sizeof(TmaF32) + sizeof(TmaF32TB), sizeof(TmaF64));
+  return kBatchHeader + (size_t)n * std::max(sizeof(TmaF32) + sizeof(TmaF32TB), sizeof(TmaF64));
 }
 
 extern "C" int sw_fdtd_batch_steps(const sw_fdtd_desc* descs, const int32_t* begins, int n,

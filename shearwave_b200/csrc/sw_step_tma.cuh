@@ -138,6 +138,6 @@ int make_tma_f32(const StepArgs& a, int xchunk, TmaF32* t);
 int make_tma_f64(const StepArgs& a, int xchunk, TmaF64* t);
 int launch_steps_tma(const StepArgs& a, int xchunk, int it0, int nsteps, cudaStream_t s);
 int launch_steps_tma_batch(int precision, const void* d_tab, int ninst, int ntiles, int it,
-                           cudaStream_t s);
+                           int* queues, cudaStream_t s);
 
 }  // namespace sw

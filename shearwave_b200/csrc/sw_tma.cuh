@@ -83,13 +83,52 @@ __device__ inline void mbar_arrive(uint64_t* bar) {
 }
 
 // Shared-memory header of the warp-specialised kernels: the mbarriers at
-// offset 0, the abort flag at offset 192, the rings from offset 256.
+// offset 0, the abort flag at offset 192, the tile hand-off slots at 200, the
+// rings from offset 256.
 struct WsHeader {
   uint64_t fullA[6], emptyA[6], fullB[4], emptyB[4];  // 160 bytes
 };
 static_assert(sizeof(WsHeader) <= 192, "header overlaps the abort flag");
 constexpr int kAbortFlagOffset = 192;
+constexpr int kTileSlotOffset = 200;  // int tile[6], then int solve[6]
 constexpr int kRingOffset = 256;
+static_assert(kTileSlotOffset + 48 <= kRingOffset, "tile slots overlap the rings");
+
+// Tile hand-off: the producer picks the CTA's tiles (a fixed stride over the
+// tile range, or the next tile of a launch-wide queue) and writes the tile
+// index and its solve's table index into the slots of the A stage that holds
+// the tile's first plane, before arming that stage's full barrier (the
+// barrier's release / acquire orders the slot write before the consumers'
+// reads).  Tile -1 (a stage armed without a copy) ends the CTA's work.
+__device__ inline volatile int* tile_slots(unsigned char* base) {
+  return reinterpret_cast<volatile int*>(base + kTileSlotOffset);
+}
+__device__ inline volatile int* solve_slots(unsigned char* base) {
+  return reinterpret_cast<volatile int*>(base + kTileSlotOffset + 24);
+}
+
+// Next tile of this CTA: a launch-wide queue (`queue`, batched launches;
+// tiles of the solves with the longest columns come first, so the queue
+// balances like longest-processing-time-first) or the fixed stride
+// blockIdx.x + k gridDim.x.
+__device__ inline int next_tile(int* queue, int& stride_next) {
+  if (queue != nullptr) return atomicAdd(queue, 1);
+  const int t = stride_next;
+  stride_next += gridDim.x;
+  return t;
+}
+
+// Table index of the solve that owns global tile t (tile_base ascending).
+template <typename Inst>
+__device__ inline int find_solve(const Inst* __restrict__ tab, int ninst, int t) {
+  int lo = 0, hi = ninst - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (tab[mid].tile_base <= t) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
 
 // A bounded wait that also gives up as soon as another thread has aborted.
 __device__ inline bool ws_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag) {

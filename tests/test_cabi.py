@@ -9,6 +9,8 @@ from __future__ import annotations
 import ctypes
 import re
 
+import pytest
+
 from conftest import ROOT
 
 import shearwave_b200._native as native
@@ -87,3 +89,40 @@ def test_spectral_basis_diagonalises_the_projection_operator():
         A = a1(n, 0.5e-3)
         assert np.abs(Q.T @ Q - np.eye(m)).max() < 1e-13
         assert np.abs(Q.T @ A @ Q - np.diag(lam)).max() / np.abs(A).max() < 1e-13
+
+
+def test_tune_knobs_roundtrip():
+    """Launch-shape knobs: defaults, set / get, range checks (host only)."""
+    from shearwave_b200 import tune
+
+    old = tune.get_knobs()
+    assert set(old) == {"ctas_per_sm", "batch_tiles_per_cta", "xchunk"}
+    try:
+        with tune.knobs(ctas_per_sm=1, xchunk=32):
+            assert tune.get_knobs()["ctas_per_sm"] == 1
+            assert tune.get_knobs()["xchunk"] == 32
+        assert tune.get_knobs() == old
+        for bad in ({"ctas_per_sm": 3}, {"ctas_per_sm": 0}, {"batch_tiles_per_cta": 0},
+                    {"xchunk": -1}, {"nope": 1}):
+            with pytest.raises(ValueError):
+                tune.set_knobs(**bad)
+        assert tune.get_knobs() == old
+    finally:
+        tune.set_knobs(**old)
+
+
+def test_tune_workload_key_and_shorten():
+    import numpy as np
+
+    from shearwave_b200 import tune
+
+    bz = np.zeros((30, 40, 50), np.float32)
+    p = {"bx": None, "by": None, "bz": bz, "rho": 1.0, "mu": 1.0, "dX": 1, "dY": 1, "dZ": 1,
+         "dT": 1, "n_steps": 100, "opts": {"env_t": np.ones(100), "force_terms": [
+             ((None, None, bz), np.ones(100))]}, "snapshot_stride": 10}
+    assert tune.workload_key(p) == "mixed:single:32x48x48"
+    assert tune.workload_key([p, p], "fp64") == "fp64:batch2:2^17"
+    q = tune._shorten(p, 16)
+    assert q["n_steps"] == 16 and len(q["opts"]["env_t"]) == 16
+    assert len(q["opts"]["force_terms"][0][1]) == 16 and "snapshot_stride" not in q
+    assert p["n_steps"] == 100 and len(p["opts"]["env_t"]) == 100

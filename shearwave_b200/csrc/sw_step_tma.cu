@@ -81,6 +81,86 @@ int encode_tmap_4d(CUtensorMap* map, CUtensorMapDataType dt, void* base, const u
 // ---------------------------------------------------------------------------
 // mixed FP32 step: warp-specialised TMA pipeline
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ float2 lds2(const float* p) {
+  return *reinterpret_cast<const float2*>(p);
+}
+__device__ __forceinline__ float2 ldg2(const float* p) {
+  return __ldg(reinterpret_cast<const float2*>(p));
+}
+__device__ __forceinline__ void stg2(float* p, float a, float b) {
+  *reinterpret_cast<float2*>(p) = make_float2(a, b);
+}
+
+// One plane of the mixed step for one thread's cell pair (z, z+1) of row y:
+// 8-byte shared-memory loads and global stores serve both cells.  `o` is the
+// pair's u component-0 index in the halo box, `ob` its index in the point
+// boxes, `i` its global cell index.  The arithmetic per cell is the same
+// expression as in the direct kernel (sw_step.cu), so the results agree bit
+// for bit.  Cells outside the interior (z = 0, z >= nz-1) get 0, which is
+// what the shell and padding hold in every state buffer.
+template <bool VISC, bool KAHAN>
+__device__ __forceinline__ void f32_pair_plane(
+    const float* __restrict__ Pc, const float* __restrict__ Pn, const float* __restrict__ Bc,
+    const float* __restrict__ Bm, int o, int ob, float2 (&pu)[3], float2 (&pd)[3], bool act_a,
+    bool act_b, float hx, float hy, float hz, bool use_damp, float damp,
+    const TmaF32* __restrict__ in, int j0, int j1, long long nc, long long i,
+    float* __restrict__ D, float2 (&un)[3], bool& bad) {
+  constexpr int W = TmaF32::W, HW = TmaF32::H * TmaF32::W, TZ = TmaF32::TZ, TY = TmaF32::TY;
+  const float2 M = lds2(Bm + ob);
+  const float2 E = VISC ? lds2(Bm + TY * TZ + ob) : make_float2(0.f, 0.f);
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const int oc = o + c * HW, od = oc + 3 * HW;
+    const float2 C = lds2(Pc + oc), L = lds2(Pc + oc - 2), R = lds2(Pc + oc + 2);
+    const float2 N = lds2(Pc + oc + W), S = lds2(Pc + oc - W), X = lds2(Pn + oc);
+    const float lua = ((X.x + pu[c].x) - 2.0f * C.x) * hx + ((N.x + S.x) - 2.0f * C.x) * hy +
+                      ((C.y + L.y) - 2.0f * C.x) * hz;
+    const float lub = ((X.y + pu[c].y) - 2.0f * C.y) * hx + ((N.y + S.y) - 2.0f * C.y) * hy +
+                      ((R.x + C.x) - 2.0f * C.y) * hz;
+    const float2 Cd = lds2(Pc + od);
+    float inca = Cd.x + M.x * lua, incb = Cd.y + M.y * lub;
+    if (VISC) {
+      const float2 Ld = lds2(Pc + od - 2), Rd = lds2(Pc + od + 2);
+      const float2 Nd = lds2(Pc + od + W), Sd = lds2(Pc + od - W), Xd = lds2(Pn + od);
+      const float lda = ((Xd.x + pd[c].x) - 2.0f * Cd.x) * hx +
+                        ((Nd.x + Sd.x) - 2.0f * Cd.x) * hy + ((Cd.y + Ld.y) - 2.0f * Cd.x) * hz;
+      const float ldb = ((Xd.y + pd[c].y) - 2.0f * Cd.y) * hx +
+                        ((Nd.y + Sd.y) - 2.0f * Cd.y) * hy + ((Rd.x + Cd.x) - 2.0f * Cd.y) * hz;
+      inca += E.x * lda;
+      incb += E.y * ldb;
+    }
+    pu[c] = C;
+    pd[c] = Cd;
+    for (int j = j0; j < j1; ++j) {  // push steps only
+      const float2 P = ldg2(in->pat + ((long long)in->term_pat[j] * 3 + c) * nc + i);
+      const float sc = (float)in->term_scale[j];
+      inca += P.x * sc;
+      incb += P.y * sc;
+    }
+    if (use_damp) {
+      inca *= damp;
+      incb *= damp;
+    }
+    float ua, ub;
+    if (KAHAN) {
+      const float2 K = lds2(Bc + c * TY * TZ + ob);
+      const float ya = inca - K.x, yb = incb - K.y;
+      ua = C.x + ya;
+      ub = C.y + yb;
+      stg2(D + (6 + c) * nc + i, act_a ? (ua - C.x) - ya : 0.f, act_b ? (ub - C.y) - yb : 0.f);
+    } else {
+      ua = C.x + inca;  // the compensation planes are neither read nor written
+      ub = C.y + incb;
+    }
+    ua = act_a ? ua : 0.f;
+    ub = act_b ? ub : 0.f;
+    stg2(D + c * nc + i, ua, ub);
+    stg2(D + (3 + c) * nc + i, act_a ? inca : 0.f, act_b ? incb : 0.f);
+    bad |= !isfinite(ua) || !isfinite(ub);
+    un[c] = make_float2(ua, ub);
+  }
+}
+
 template <bool BATCH>
 __global__ void __launch_bounds__(TmaF32::THREADS, 2)
     step_f32_tma(const __grid_constant__ TmaF32 one, const TmaF32* __restrict__ tab, int ninst,
@@ -189,9 +269,11 @@ __global__ void __launch_bounds__(TmaF32::THREADS, 2)
       const float damp = in->damp;
       const int y = tc.y0 + ly;
       const bool yin = (y >= 1 && y <= g.ny - 2);
-      const int z0 = tc.z0 + lane, z1 = z0 + 32;
-      const bool act0 = yin && z0 >= 1 && z0 <= g.nz - 2;
-      const bool act1 = yin && z1 >= 1 && z1 <= g.nz - 2;
+      // this thread's cells: the pair z, z+1 with z = z0 + 2 lane
+      const int lz = 2 * lane, z = tc.z0 + lz;
+      const bool inrow = yin && z < g.pz;  // pz is even: the whole pair is in the row
+      const bool act_a = yin && z >= 1 && z <= g.nz - 2;
+      const bool act_b = yin && z + 1 >= 1 && z + 1 <= g.nz - 2;
       const int j0 = in->term_off ? in->term_off[lit] : 0;
       const int j1 = in->term_off ? in->term_off[lit + 1] : 0;
       const bool snap =
@@ -200,31 +282,29 @@ __global__ void __launch_bounds__(TmaF32::THREADS, 2)
       const long long nc = g.ncell;
       const bool visc = in->ncoef > 1;
       const float hx = in->hx, hy = in->hy, hz = in->hz;
+      const int o = (ly + 1) * W + lz + 4, ob = ly * TZ + lz;
       // Plane x-1 enters only through its centre values (x neighbours of the
       // Laplacians), which each thread keeps in registers from the plane it
       // computed last; so a plane's stage is released as soon as the plane is
       // computed, and the ring holds planes x and x+1 with two more in flight.
-      float pu[2][3], pd[2][3];  // u and d of plane x-1 at this thread's cells
+      float2 pu[3], pd[3];  // u and d of plane x-1 at this thread's cells
       bool ok = true;
       ++ca;  // plane x0-1 (waited for above): centres only
       {
         const float* P0 = ringA + s_cur * AF;
 #pragma unroll
-        for (int k = 0; k < 2; ++k)
-#pragma unroll
-          for (int c = 0; c < 3; ++c) {
-            const int o = (c * H + ly + 1) * W + lane + 32 * k + 4;
-            pu[k][c] = P0[o];
-            pd[k][c] = P0[o + 3 * H * W];
-          }
+        for (int c = 0; c < 3; ++c) {
+          pu[c] = lds2(P0 + o + c * H * W);
+          pd[c] = lds2(P0 + o + (3 + c) * H * W);
+        }
       }
       __syncwarp();
       if (lane == 0) mbar_arrive(&hd->emptyA[s_cur]);
       s_cur = ca % NA;
       ok &= ws_wait(&hd->fullA[s_cur], (ca / NA) & 1u, abort_flag);
       ++ca;
-      long long irow = (long long)tc.x0 * g.sxy + (long long)y * g.pz;
-      for (int x = tc.x0; x < tc.x1 && ok; ++x, irow += g.sxy) {
+      long long i = (long long)tc.x0 * g.sxy + (long long)y * g.pz + z;
+      for (int x = tc.x0; x < tc.x1 && ok; ++x, i += g.sxy) {
         const int s_next = ca % NA;
         ok &= ws_wait(&hd->fullA[s_next], (ca / NA) & 1u, abort_flag);
         ++ca;
@@ -232,62 +312,35 @@ __global__ void __launch_bounds__(TmaF32::THREADS, 2)
         ok &= ws_wait(&hd->fullB[sb], (cb / NB) & 1u, abort_flag);
         ++cb;
         if (!ok) break;
-        const float* Pc = ringA + s_cur * AF;
-        const float* Pn = ringA + s_next * AF;
-        const float* Bc = ringB + sb * BF;
-        const float* Bm = Bc + CF;
-#pragma unroll
-        for (int k = 0; k < 2; ++k) {
-          const int lz = lane + 32 * k;
-          if (!(k == 0 ? act0 : act1)) {  // keep the centres for the next plane
+        if (inrow) {
+          const float* Pc = ringA + s_cur * AF;
+          const float* Pn = ringA + s_next * AF;
+          const float* Bc = ringB + sb * BF;
+          const float* Bm = Bc + CF;
+          float2 un[3];
+          bool bad = false;
+          if (visc) {
+            if (kahan)
+              f32_pair_plane<true, true>(Pc, Pn, Bc, Bm, o, ob, pu, pd, act_a, act_b, hx, hy, hz,
+                                         use_damp, damp, in, j0, j1, nc, i, D, un, bad);
+            else
+              f32_pair_plane<true, false>(Pc, Pn, Bc, Bm, o, ob, pu, pd, act_a, act_b, hx, hy, hz,
+                                          use_damp, damp, in, j0, j1, nc, i, D, un, bad);
+          } else {
+            if (kahan)
+              f32_pair_plane<false, true>(Pc, Pn, Bc, Bm, o, ob, pu, pd, act_a, act_b, hx, hy,
+                                          hz, use_damp, damp, in, j0, j1, nc, i, D, un, bad);
+            else
+              f32_pair_plane<false, false>(Pc, Pn, Bc, Bm, o, ob, pu, pd, act_a, act_b, hx, hy,
+                                           hz, use_damp, damp, in, j0, j1, nc, i, D, un, bad);
+          }
+          if (snap) {
+            float* sp = in->snaps + ((((long long)slot * g.nx + x) * g.ny + y) * g.nz + z) * 3;
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
-              const int o = (c * H + ly + 1) * W + lz + 4;
-              pu[k][c] = Pc[o];
-              pd[k][c] = Pc[o + 3 * H * W];
+              if (act_a) sp[c] = un[c].x;
+              if (act_b) sp[3 + c] = un[c].y;
             }
-            continue;
-          }
-          const int z = tc.z0 + lz;
-          const long long i = irow + z;
-          const float m = Bm[ly * TZ + lz];
-          const float e = visc ? Bm[(TY + ly) * TZ + lz] : 0.0f;
-          bool bad = false;
-#pragma unroll
-          for (int c = 0; c < 3; ++c) {
-            const int o = (c * H + ly + 1) * W + lz + 4;
-            const int od = o + 3 * H * W;
-            const float u0 = Pc[o], d0 = Pc[od];
-            const float lu = ((Pn[o] + pu[k][c]) - 2.0f * u0) * hx +
-                             ((Pc[o + W] + Pc[o - W]) - 2.0f * u0) * hy +
-                             ((Pc[o + 1] + Pc[o - 1]) - 2.0f * u0) * hz;
-            float inc = d0 + m * lu;
-            if (visc) {
-              const float ld = ((Pn[od] + pd[k][c]) - 2.0f * d0) * hx +
-                               ((Pc[od + W] + Pc[od - W]) - 2.0f * d0) * hy +
-                               ((Pc[od + 1] + Pc[od - 1]) - 2.0f * d0) * hz;
-              inc += e * ld;
-            }
-            pu[k][c] = u0;
-            pd[k][c] = d0;
-            for (int j = j0; j < j1; ++j)
-              inc += in->pat[((long long)in->term_pat[j] * 3 + c) * nc + i] *
-                     (float)in->term_scale[j];
-            if (use_damp) inc *= damp;
-            float unew;
-            if (kahan) {
-              const float cc = Bc[(c * TY + ly) * TZ + lz];
-              const float yk = inc - cc;
-              unew = u0 + yk;
-              D[(6 + c) * nc + i] = (unew - u0) - yk;
-            } else {
-              unew = u0 + inc;  // the compensation planes are neither read nor written
-            }
-            D[c * nc + i] = unew;
-            D[(3 + c) * nc + i] = inc;
-            bad |= !isfinite(unew);
-            if (snap)
-              in->snaps[((((long long)slot * g.nx + x) * g.ny + y) * g.nz + z) * 3 + c] = unew;
           }
           if (bad && in->flags) atomicOr(in->flags, 1);
         }

@@ -75,14 +75,16 @@ def measured_hbm():
         return FALLBACK_HBM_GBS, "fallback"
 
 
-def ncu_traffic(kernel: str, workload: str):
-    """dram bytes per launch recorded from an ncu capture (profiles/traffic.txt)."""
+def ncu_bytes_per_cell_step(kernel: str):
+    """DRAM bytes (read + write) per cell-step of a step kernel, from an ncu
+    capture summarised in profiles/traffic.txt (lines ``<kernel>
+    bytes_per_cell_step <B>``); None when absent."""
     p = ROOT / "profiles" / "traffic.txt"
     if not p.exists():
         return None
     for line in p.read_text().splitlines():
         parts = line.split()
-        if len(parts) >= 3 and parts[0] == kernel and parts[1] == workload:
+        if len(parts) >= 3 and parts[0] == kernel and parts[1] == "bytes_per_cell_step":
             try:
                 return float(parts[2])
             except ValueError:
@@ -435,9 +437,14 @@ def main(argv=None) -> int:
     per_launch_ms = step_ms / launches_step
     achieved = alg_bytes / (step_ms / 1e3) / 1e9
     peak, peak_kind = measured_hbm()
-    traffic = ncu_traffic("step_f32", a.workload)
+    bpcs = ncu_bytes_per_cell_step("step_f32_tma")
+    cells_per_launch = sum(math.prod(_shape(p)) * p["n_steps"] for p in probs) / launches_step
+    traffic = None if bpcs is None else bpcs * cells_per_launch
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
+            "traffic_note": ("DRAM bytes per launch: ncu's read+write bytes per cell-step "
+                             "(profiles/traffic.txt) x the cells a launch updates"),
+            "traffic_bytes_per_cell_step": bpcs,
             "kernel": ("step_f32_fused2 (two KV steps per pass, mixed form)" if spl == 2
                        else "step_f32_tma (fused KV step, mixed form)"),
             "steps_per_launch": spl,

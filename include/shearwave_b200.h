@@ -88,7 +88,8 @@ enum sw_tune_knob {
   SW_TUNE_STEP_CTAS_PER_SM = 0,    /* resident step CTAs per SM: 1 or 2 (default 2) */
   SW_TUNE_BATCH_TILES_PER_CTA = 1, /* batched launches: tiles per CTA, 1..64 (8)   */
   SW_TUNE_XCHUNK = 2,              /* planes per x chunk, 0 = automatic (0)          */
-  SW_TUNE_COUNT = 3
+  SW_TUNE_TILE_SHAPE = 3,          /* mixed step tiles: 0 auto, 1 64x8, 2 32x16 (0)  */
+  SW_TUNE_COUNT = 4
 };
 /* SW_EINVAL for an unknown knob or a value out of range. */
 int sw_tune_set(int knob, int value);
@@ -304,6 +305,31 @@ int sw_strain(int dtype, const void* ux, const void* uy, const void* uz, int64_t
 /* Invariants of n Voigt 6-vectors (dense (n, 6) of dtype). */
 int sw_strain_invariants(int dtype, const void* eps, int64_t n, void* vol, void* dev,
                          void* max_shear, double* von_mises, void* stream);
+
+/* ---- acoustic radiation force (radiation_force.py:27-157) ------------- */
+/* Inputs are the reference's (nx, ny, nz, nt) records, time fastest: cell k's
+ * series is p[k*nt .. k*nt+nt-1]; ncell = nx*ny*nz.                        */
+/* Workspace of sw_arf_envelope (FP64 per-block partial sums). */
+size_t sw_arf_workspace_bytes(int64_t ncell, int32_t nt);
+/* Auto-gate envelope (radiation_force.py:63-68): env[t] = mean over cells of
+ * p[., t]^2, accumulated in FP64 in a fixed order; env is nt doubles on the
+ * device.  The caller thresholds it (>= 0.1 max) to pick the gate.         */
+int sw_arf_envelope(int dtype, const void* p, int64_t ncell, int32_t nt, double* env,
+                    void* workspace, size_t workspace_bytes, void* stream);
+/* Radiation force over the gated time indices gate[0..n_gate) (each in
+ * [0, nt); indices outside are skipped).  n_fields 1:
+ * compute_radiation_force (radiation_force.py:71-85),
+ *   out0 = 2 alpha_Np (mean p^2 / (rho c)) / c;
+ * n_fields 3: compute_radiation_force_velocity (radiation_force.py:141-157),
+ *   out_i = (2 alpha_Np / c) mean(p v_i) with v = (vx, vy, vz);
+ * alpha_Np = alpha * (f0 / 1e6) / 8.685889638 * 100.  Maps are FP64 per cell
+ * (map_stride 1) or one value for every cell (map_stride 0); outputs are
+ * ncell values of out_dtype.  Sums run in FP64.                             */
+int sw_arf_force(int dtype, int n_fields, const void* p, const void* vx, const void* vy,
+                 const void* vz, int64_t ncell, int32_t nt, const int32_t* gate, int32_t n_gate,
+                 const double* c_map, const double* rho_map, const double* alpha_map,
+                 int64_t map_stride, double f0, int out_dtype, void* out0, void* out1,
+                 void* out2, void* stream);
 
 #ifdef __cplusplus
 }

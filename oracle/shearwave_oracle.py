@@ -9,6 +9,7 @@ NumPy backend for the path that the CUDA library accelerates:
 * the explicit time loop            (src/shearwave/solver.py:27-243)
 * the static elastic CG solve       (src/shearwave/solver.py:569-625)
 * the strain post-pass              (src/shearwave/strain.py:16-159)
+* the radiation-force producers     (src/shearwave/radiation_force.py:27-157)
 
 It is the CHECKER, never the product: only the test suite, the smoke check and
 the CPU-baseline leg of the benchmark may import it.  The product path lives in
@@ -32,6 +33,8 @@ from __future__ import annotations
 import numpy as np
 
 __all__ = [
+    "compute_radiation_force",
+    "compute_radiation_force_velocity",
     "compute_strain_invariants",
     "compute_strain_tensor",
     "divergence_center",
@@ -478,3 +481,39 @@ def compute_strain_invariants(eps: np.ndarray) -> dict:
         "max_shear": np.sqrt(np.maximum(j2, 0.0)),
         "von_mises": np.sqrt(2.0 / 3.0) * dev,
     }
+
+
+# ---------------------------------------------------------------------------
+# acoustic radiation force (src/shearwave/radiation_force.py)
+# ---------------------------------------------------------------------------
+def _arf_gate(p):
+    """Auto gate (radiation_force.py:63-68): t where mean_cells p^2 >= 0.1 max."""
+    env = (p**2).mean(axis=(0, 1, 2))
+    keep = env >= 0.1 * env.max()
+    return slice(None) if not keep.any() else np.nonzero(keep)[0]
+
+
+def _alpha_np(alpha_coeff_map, f0):
+    """dB/cm/MHz -> Np/m (radiation_force.py:78-80)."""
+    return (alpha_coeff_map * (f0 / 1e6)) / 8.685889638 * 100.0
+
+
+def compute_radiation_force(pressure_4d, c_map, rho_map, alpha_coeff_map, f0, gate=None):
+    """b = 2 alpha_Np Isppa / c, Isppa = mean_gate(p^2) / (rho c)
+    (radiation_force.py:27-85)."""
+    if gate is None:
+        gate = _arf_gate(pressure_4d)
+    isppa = np.mean(pressure_4d[:, :, :, gate] ** 2, axis=3) / (rho_map * c_map)
+    return 2.0 * _alpha_np(alpha_coeff_map, f0) * isppa / c_map
+
+
+def compute_radiation_force_velocity(pressure_4d, velocity_u_4d, velocity_w_4d, velocity_v_4d,
+                                     c_map, rho_map, alpha_coeff_map, f0, gate=None):
+    """b_i = (2 alpha_Np / c) mean_gate(p v_i) (radiation_force.py:88-157)."""
+    if gate is None:
+        gate = _arf_gate(pressure_4d)
+    pg = pressure_4d[:, :, :, gate]
+    flux = [np.mean(pg * v[:, :, :, gate], axis=3)
+            for v in (velocity_u_4d, velocity_w_4d, velocity_v_4d)]
+    coeff = 2.0 * _alpha_np(alpha_coeff_map, f0) / c_map
+    return coeff * flux[0], coeff * flux[1], coeff * flux[2]

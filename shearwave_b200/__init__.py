@@ -11,6 +11,7 @@ from .solver import (
     divergence_center,
     elastic_solve_static,
     gradient_center,
+    hann1d,
     laplacian_center,
     project_body_force_to_shear,
     project_vector_field,
@@ -18,18 +19,22 @@ from .solver import (
     shear_fdtd_batch,
     shear_fdtd_jax,
 )
+from .radiation import compute_radiation_force, compute_radiation_force_velocity
 from .strain import compute_strain_fields, compute_strain_invariants, compute_strain_tensor
 
 __version__ = "0.1.0"
 
 __all__ = [
     "__version__",
+    "compute_radiation_force",
+    "compute_radiation_force_velocity",
     "compute_strain_fields",
     "compute_strain_invariants",
     "compute_strain_tensor",
     "divergence_center",
     "elastic_solve_static",
     "gradient_center",
+    "hann1d",
     "laplacian_center",
     "project_body_force_to_shear",
     "project_vector_field",

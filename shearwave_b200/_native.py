@@ -85,6 +85,11 @@ _SIGNATURES = {
     "sw_pitch": ([C.c_int], C.c_int),
     "sw_fdtd_desc_size": ([], _sz),
     "sw_launch_count": ([], C.c_uint64),
+    "sw_arf_workspace_bytes": ([C.c_int64, C.c_int32], _sz),
+    "sw_arf_envelope": ([C.c_int, _vp, C.c_int64, C.c_int32, _vp, _vp, _sz, _vp], C.c_int),
+    "sw_arf_force": ([C.c_int, C.c_int, _vp, _vp, _vp, _vp, C.c_int64, C.c_int32, _vp, C.c_int32,
+                      _vp, _vp, _vp, C.c_int64, C.c_double, C.c_int, _vp, _vp, _vp, _vp],
+                     C.c_int),
     "sw_tune_set": ([C.c_int, C.c_int], C.c_int),
     "sw_tune_get": ([C.c_int], C.c_int),
     "sw_laplacian": ([C.c_int, _vp, _vp, C.c_int, C.c_int, C.c_int, _f64, _f64, _f64, _vp],

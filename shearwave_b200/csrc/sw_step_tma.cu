@@ -24,6 +24,7 @@
 #include <math.h>
 
 #include <algorithm>
+#include <type_traits>
 #include <vector>
 
 #include "sw_common.cuh"
@@ -101,13 +102,15 @@ __device__ __forceinline__ void stg2(float* p, float a, float b) {
 template <bool VISC, bool KAHAN>
 __device__ __forceinline__ void f32_pair_plane(
     const float* __restrict__ Pc, const float* __restrict__ Pn, const float* __restrict__ Bc,
-    const float* __restrict__ Bm, int o, int ob, float2 (&pu)[3], float2 (&pd)[3], bool act_a,
-    bool act_b, float hx, float hy, float hz, bool use_damp, float damp,
+    const float* __restrict__ Bm, int o, int ob, int W, float2 (&pu)[3], float2 (&pd)[3],
+    bool act_a, bool act_b, float hx, float hy, float hz, bool use_damp, float damp,
     const TmaF32* __restrict__ in, int j0, int j1, long long nc, long long i,
     float* __restrict__ D, float2 (&un)[3], bool& bad) {
-  constexpr int W = TmaF32::W, HW = TmaF32::H * TmaF32::W, TZ = TmaF32::TZ, TY = TmaF32::TY;
+  // the halo box holds W x H = 720 cells per component for both tile shapes,
+  // and a point box tzw x tyh = 512 cells per component
+  constexpr int HW = TmaF32::H * TmaF32::W, PT = TmaF32::TZ * TmaF32::TY;
   const float2 M = lds2(Bm + ob);
-  const float2 E = VISC ? lds2(Bm + TY * TZ + ob) : make_float2(0.f, 0.f);
+  const float2 E = VISC ? lds2(Bm + PT + ob) : make_float2(0.f, 0.f);
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
     const int oc = o + c * HW, od = oc + 3 * HW;
@@ -143,7 +146,7 @@ __device__ __forceinline__ void f32_pair_plane(
     }
     float ua, ub;
     if (KAHAN) {
-      const float2 K = lds2(Bc + c * TY * TZ + ob);
+      const float2 K = lds2(Bc + c * PT + ob);
       const float ya = inca - K.x, yb = incb - K.y;
       ua = C.x + ya;
       ub = C.y + yb;
@@ -161,10 +164,14 @@ __device__ __forceinline__ void f32_pair_plane(
   }
 }
 
-template <bool BATCH>
+template <bool BATCH, int TZW>
 __global__ void __launch_bounds__(TmaF32::THREADS, 2)
     step_f32_tma(const __grid_constant__ TmaF32 one, const TmaF32* __restrict__ tab, int ninst,
                  int ntiles, int it, const int* __restrict__ it_dev, int* queues) {
+  // tile shape: TZW x TYH cells (64 x 8, or 32 x 16); every solve of a
+  // launch uses the launch's shape
+  constexpr int TYH = TmaF32::TZ * TmaF32::TY / TZW;
+  static_assert(TZW == 64 || TZW == 32, "tile widths 64 and 32");
   if (it_dev != nullptr) it += *it_dev;  // step counter kept on the device (graph replays)
   // batched launches take tiles from queue it & 1 and reset the other one
   // for the next launch of the stream
@@ -220,7 +227,7 @@ __global__ void __launch_bounds__(TmaF32::THREADS, 2)
         const int local = BATCH ? t - in->tile_base : t;
         const int lit = it - in->it_begin;
         if (lit < 0 || lit >= in->n_steps) continue;
-        const TileCoord tc = tile_coord_t(in->g, in->ts, local, TZ, TY);
+        const TileCoord tc = tile_coord_t(in->g, in->ts, local, TZW, TYH);
         const CUtensorMap* tma = &in->tm[lit % 3];
         const CUtensorMap* tmc = &in->tmc[lit % 3];
         const uint32_t bbytes = (in->kahan ? TmaF32::C_BYTES : 0) + TZ * TY * 4 * in->ncoef;
@@ -263,14 +270,19 @@ __global__ void __launch_bounds__(TmaF32::THREADS, 2)
       // the stores below could otherwise force reloads of its fields (fields
       // used only on push / snapshot steps are read where they are used)
       const Geom& g = in->g;
-      const TileCoord tc = tile_coord_t(g, in->ts, local, TZ, TY);
+      constexpr int tzw = TZW;
+      const TileCoord tc = tile_coord_t(g, in->ts, local, TZW, TYH);
       float* __restrict__ D = in->state[(lit + 1) % 3];
       const bool kahan = in->kahan != 0, use_damp = in->use_damp != 0;
       const float damp = in->damp;
-      const int y = tc.y0 + ly;
+      // this thread's cells: the pair z, z+1 of tile row `row`; a warp covers
+      // one row of 32 pairs (64 x 8 tiles) or two rows of 16 (32 x 16 tiles)
+      const int row = tzw == 64 ? ly : 2 * ly + (lane >> 4);
+      const int lz = tzw == 64 ? 2 * lane : 2 * (lane & 15);
+      constexpr int Wb = tzw + 8;  // halo box row length
+      const int y = tc.y0 + row;
       const bool yin = (y >= 1 && y <= g.ny - 2);
-      // this thread's cells: the pair z, z+1 with z = z0 + 2 lane
-      const int lz = 2 * lane, z = tc.z0 + lz;
+      const int z = tc.z0 + lz;
       const bool inrow = yin && z < g.pz;  // pz is even: the whole pair is in the row
       const bool act_a = yin && z >= 1 && z <= g.nz - 2;
       const bool act_b = yin && z + 1 >= 1 && z + 1 <= g.nz - 2;
@@ -282,7 +294,7 @@ __global__ void __launch_bounds__(TmaF32::THREADS, 2)
       const long long nc = g.ncell;
       const bool visc = in->ncoef > 1;
       const float hx = in->hx, hy = in->hy, hz = in->hz;
-      const int o = (ly + 1) * W + lz + 4, ob = ly * TZ + lz;
+      const int o = (row + 1) * Wb + lz + 4, ob = row * tzw + lz;
       // Plane x-1 enters only through its centre values (x neighbours of the
       // Laplacians), which each thread keeps in registers from the plane it
       // computed last; so a plane's stage is released as soon as the plane is
@@ -321,17 +333,17 @@ __global__ void __launch_bounds__(TmaF32::THREADS, 2)
           bool bad = false;
           if (visc) {
             if (kahan)
-              f32_pair_plane<true, true>(Pc, Pn, Bc, Bm, o, ob, pu, pd, act_a, act_b, hx, hy, hz,
+              f32_pair_plane<true, true>(Pc, Pn, Bc, Bm, o, ob, Wb, pu, pd, act_a, act_b, hx, hy, hz,
                                          use_damp, damp, in, j0, j1, nc, i, D, un, bad);
             else
-              f32_pair_plane<true, false>(Pc, Pn, Bc, Bm, o, ob, pu, pd, act_a, act_b, hx, hy, hz,
+              f32_pair_plane<true, false>(Pc, Pn, Bc, Bm, o, ob, Wb, pu, pd, act_a, act_b, hx, hy, hz,
                                           use_damp, damp, in, j0, j1, nc, i, D, un, bad);
           } else {
             if (kahan)
-              f32_pair_plane<false, true>(Pc, Pn, Bc, Bm, o, ob, pu, pd, act_a, act_b, hx, hy,
+              f32_pair_plane<false, true>(Pc, Pn, Bc, Bm, o, ob, Wb, pu, pd, act_a, act_b, hx, hy,
                                           hz, use_damp, damp, in, j0, j1, nc, i, D, un, bad);
             else
-              f32_pair_plane<false, false>(Pc, Pn, Bc, Bm, o, ob, pu, pd, act_a, act_b, hx, hy,
+              f32_pair_plane<false, false>(Pc, Pn, Bc, Bm, o, ob, Wb, pu, pd, act_a, act_b, hx, hy,
                                            hz, use_damp, damp, in, j0, j1, nc, i, D, un, bad);
           }
           if (snap) {
@@ -606,11 +618,11 @@ static int set_smem_attr(int precision) {
       e = cudaFuncSetAttribute(step_f64_tma<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                bytes);
   } else {
-    e = cudaFuncSetAttribute(step_f32_tma<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             bytes);
-    if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(step_f32_tma<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               bytes);
+    const void* fns[4] = {(const void*)step_f32_tma<false, 64>, (const void*)step_f32_tma<true, 64>,
+                          (const void*)step_f32_tma<false, 32>, (const void*)step_f32_tma<true, 32>};
+    e = cudaSuccess;
+    for (int i = 0; i < 4 && e == cudaSuccess; ++i)
+      e = cudaFuncSetAttribute(fns[i], cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
   }
   if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(step smem)");
   done[k] = true;
@@ -654,19 +666,36 @@ static int coef_components(const StepArgs& a, size_t es, int* ncoef) {
   return SW_OK;
 }
 
-int make_tma_f32(const StepArgs& a, int xchunk, TmaF32* t) {
+// Tile shape of the mixed step kernel for a grid: 64 x 8 or 32 x 16,
+// whichever covers the (z, y) plane with fewer cells (ties: 64 x 8), unless
+// the SW_TUNE_TILE_SHAPE knob forces one.
+long long f32_tile_cover(const Geom& g, int tzw) {
+  const int tyh = TmaF32::TZ * TmaF32::TY / tzw;
+  return (long long)((g.nz + tzw - 1) / tzw) * tzw * (long long)((g.ny + tyh - 1) / tyh) * tyh;
+}
+
+int f32_tile_width(const Geom& g) {
+  const int knob = tune_get(SW_TUNE_TILE_SHAPE);
+  if (knob == 1) return 64;
+  if (knob == 2) return 32;
+  return f32_tile_cover(g, 32) < f32_tile_cover(g, 64) ? 32 : 64;
+}
+
+int make_tma_f32(const StepArgs& a, int xchunk, TmaF32* t, int tzw) {
   *t = TmaF32{};
   t->g = a.g;
+  t->tzw = tzw > 0 ? tzw : f32_tile_width(a.g);
+  t->tyh = TmaF32::TZ * TmaF32::TY / t->tzw;
   const int xt = xchunk > 0 ? xchunk : tune_get(SW_TUNE_XCHUNK);
-  const int xc = xt > 0 ? xt : tma_xchunk(a.g, TmaF32::TZ, TmaF32::TY, step_slots());
-  t->ts = make_tiles_t(a.g, xc, TmaF32::TZ, TmaF32::TY);
+  const int xc = xt > 0 ? xt : tma_xchunk(a.g, t->tzw, t->tyh, step_slots());
+  t->ts = make_tiles_t(a.g, xc, t->tzw, t->tyh);
   int rc = coef_components(a, 4, &t->ncoef);
   if (rc != SW_OK) return rc;
   const uint64_t dims[4] = {(uint64_t)a.g.pz, (uint64_t)a.g.ny, (uint64_t)a.g.nx, 9};
   const uint64_t strides[3] = {(uint64_t)a.g.pz * 4, (uint64_t)a.g.sxy * 4,
                                (uint64_t)a.g.ncell * 4};
-  const uint32_t box_halo[4] = {TmaF32::W, TmaF32::H, 1, 6};
-  const uint32_t box_pt[4] = {TmaF32::TZ, TmaF32::TY, 1, 3};
+  const uint32_t box_halo[4] = {(uint32_t)t->tzw + 8, (uint32_t)t->tyh + 2, 1, 6};
+  const uint32_t box_pt[4] = {(uint32_t)t->tzw, (uint32_t)t->tyh, 1, 3};
   for (int b = 0; b < 3; ++b) {
     t->state[b] = (float*)a.state[b];
     rc = encode_tmap_4d(&t->tm[b], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, a.state[b], dims, strides,
@@ -678,7 +707,7 @@ int make_tma_f32(const StepArgs& a, int xchunk, TmaF32* t) {
   }
   const uint64_t mdims[4] = {(uint64_t)a.g.pz, (uint64_t)a.g.ny, (uint64_t)a.g.nx,
                              (uint64_t)t->ncoef};
-  const uint32_t box_m[4] = {TmaF32::TZ, TmaF32::TY, 1, (uint32_t)t->ncoef};
+  const uint32_t box_m[4] = {(uint32_t)t->tzw, (uint32_t)t->tyh, 1, (uint32_t)t->ncoef};
   rc = encode_tmap_4d(&t->tmm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, (void*)a.coef_m, mdims, strides,
                       box_m);
   if (rc != SW_OK) return rc;
@@ -836,7 +865,7 @@ int launch_steps_tma(const StepArgs& a, int xchunk, int it0, int nsteps, cudaStr
     // otherwise; 0 (automatic) and 1: one step per launch
     const bool fuse = a.steps_per_pass == 2 && nsteps >= 2;
     TmaF32 t;
-    rc = make_tma_f32(a, xchunk, &t);
+    rc = make_tma_f32(a, xchunk, &t, 0);
     if (rc != SW_OK) return rc;
     if (t.ts.count == 0) return SW_OK;
     TmaF32TB tb;
@@ -854,16 +883,21 @@ int launch_steps_tma(const StepArgs& a, int xchunk, int it0, int nsteps, cudaStr
                       std::min(tb.ts.count, 148), TmaF32TB::THREADS, tb_smem_bytes(), 2, 16,
                       a.clock, it0, nsteps, s, &done);
     else
-      rc = graph_loop(reinterpret_cast<void*>(step_f32_tma<false>), t, grid, TmaF32::THREADS,
-                      smem, 1, 32, a.clock, it0, nsteps, s, &done);
+      rc = graph_loop(t.tzw == 64 ? reinterpret_cast<void*>(step_f32_tma<false, 64>)
+                                  : reinterpret_cast<void*>(step_f32_tma<false, 32>),
+                      t, grid, TmaF32::THREADS, smem, 1, 32, a.clock, it0, nsteps, s, &done);
     if (rc != SW_OK) return rc;
     for (int it = it0 + done; it < it0 + nsteps;) {
       if (fuse && it + 1 < it0 + nsteps) {
         launch_fused2_raw(tb, it, s);
         it += 2;
       } else {
-        step_f32_tma<false><<<grid, TmaF32::THREADS, smem, s>>>(t, nullptr, 1, t.ts.count, it,
-                                                                nullptr, nullptr);
+        if (t.tzw == 64)
+          step_f32_tma<false, 64><<<grid, TmaF32::THREADS, smem, s>>>(t, nullptr, 1, t.ts.count,
+                                                                      it, nullptr, nullptr);
+        else
+          step_f32_tma<false, 32><<<grid, TmaF32::THREADS, smem, s>>>(t, nullptr, 1, t.ts.count,
+                                                                      it, nullptr, nullptr);
         it += 1;
       }
       ++n_launch;
@@ -878,7 +912,7 @@ int launch_steps_tma(const StepArgs& a, int xchunk, int it0, int nsteps, cudaStr
 }
 
 int launch_steps_tma_batch(int precision, const void* d_tab, int ninst, int ntiles, int it,
-                           int* queues, cudaStream_t s) {
+                           int* queues, int tzw, cudaStream_t s) {
   int rc = set_smem_attr(precision);
   if (rc != SW_OK) return rc;
   if (ntiles == 0) return SW_OK;
@@ -890,8 +924,12 @@ int launch_steps_tma_batch(int precision, const void* d_tab, int ninst, int ntil
                                                           ntiles, it, nullptr, queues);
   } else {
     TmaF32 dummy{};
-    step_f32_tma<true><<<grid, TmaF32::THREADS, smem, s>>>(dummy, (const TmaF32*)d_tab, ninst,
-                                                          ntiles, it, nullptr, queues);
+    if (tzw == 32)
+      step_f32_tma<true, 32><<<grid, TmaF32::THREADS, smem, s>>>(dummy, (const TmaF32*)d_tab,
+                                                                ninst, ntiles, it, nullptr, queues);
+    else
+      step_f32_tma<true, 64><<<grid, TmaF32::THREADS, smem, s>>>(dummy, (const TmaF32*)d_tab,
+                                                                ninst, ntiles, it, nullptr, queues);
   }
   count_launches(1);
   SW_CHECK_LAUNCH("step (tma, batch)");
@@ -941,14 +979,33 @@ static int solve_xchunk(const sw_fdtd_desc& d, int xc) {
 }
 
 template <typename Inst>
-int make_inst(const StepArgs& a, int xchunk, Inst* t);
+int make_inst(const StepArgs& a, int xchunk, Inst* t, int shape);
 template <>
-int make_inst<TmaF32>(const StepArgs& a, int xchunk, TmaF32* t) {
-  return make_tma_f32(a, xchunk, t);
+int make_inst<TmaF32>(const StepArgs& a, int xchunk, TmaF32* t, int shape) {
+  return make_tma_f32(a, xchunk, t, shape);
 }
 template <>
-int make_inst<TmaF64>(const StepArgs& a, int xchunk, TmaF64* t) {
+int make_inst<TmaF64>(const StepArgs& a, int xchunk, TmaF64* t, int) {
   return make_tma_f64(a, xchunk, t);
+}
+
+// Tile width shared by every solve of a batched mixed launch: the one that
+// covers the running solves' planes with fewer cells (or the knob's).
+static int batch_tile_width(const sw_fdtd_desc* descs, const std::vector<int>& run) {
+  const int knob = tune_get(SW_TUNE_TILE_SHAPE);
+  if (knob == 1) return 64;
+  if (knob == 2) return 32;
+  long long c64 = 0, c32 = 0;
+  for (int i : run) {
+    Geom g;
+    g.nx = descs[i].nx;
+    g.ny = descs[i].ny;
+    g.nz = descs[i].nz;
+    const long long nxi = std::max(0, descs[i].nx - 2) * (long long)descs[i].n_steps;
+    c64 += f32_tile_cover(g, 64) * nxi;
+    c32 += f32_tile_cover(g, 32) * nxi;
+  }
+  return c32 < c64 ? 32 : 64;
 }
 
 // Table of the solves running at step `it`, in batch_order, with their tile
@@ -962,6 +1019,7 @@ int build_batch(const sw_fdtd_desc* descs, const int32_t* begins, int n, int it,
     const int lit = it - (begins ? begins[i] : 0);
     if (lit >= 0 && lit < descs[i].n_steps) run.push_back(i);
   }
+  const int shape = std::is_same<Inst, TmaF32>::value ? batch_tile_width(descs, run) : 0;
   const int xc = batch_xchunk(descs, run, Inst::TZ, Inst::TY);
   int nt = 0;
   for (int i : batch_order(descs, run)) {
@@ -969,7 +1027,7 @@ int build_batch(const sw_fdtd_desc* descs, const int32_t* begins, int n, int it,
     int rc = make_step_args(&descs[i], &a);
     if (rc != SW_OK) return rc;
     Inst t;
-    rc = make_inst<Inst>(a, solve_xchunk(descs[i], xc), &t);
+    rc = make_inst<Inst>(a, solve_xchunk(descs[i], xc), &t, shape);
     if (rc != SW_OK) return rc;
     t.it_begin = begins ? begins[i] : 0;
     t.tile_base = nt;
@@ -1062,7 +1120,7 @@ int batch_steps_mixed(const sw_fdtd_desc* descs, const int32_t* begins, int n, i
       it += 2;
     } else {
       rc = launch_steps_tma_batch(SW_MIXED_F32, tab_single, (int)tsingle.size(), ntiles, it,
-                                  queues, s);
+                                  queues, tsingle.empty() ? 64 : tsingle[0].tzw, s);
       it += 1;
     }
     if (rc != SW_OK) return rc;
@@ -1104,7 +1162,7 @@ int batch_steps(int precision, const sw_fdtd_desc* descs, const int32_t* begins,
       have = true;
     }
     if (tab.empty()) continue;
-    int rc = launch_steps_tma_batch(precision, table, (int)tab.size(), ntiles, it, queues, s);
+    int rc = launch_steps_tma_batch(precision, table, (int)tab.size(), ntiles, it, queues, 0, s);
     if (rc != SW_OK) return rc;
   }
   return SW_OK;

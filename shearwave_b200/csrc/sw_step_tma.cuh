@@ -11,14 +11,18 @@ namespace sw {
 constexpr int round128(int bytes) { return (bytes + 127) / 128 * 128; }
 
 // Kernel-side view of one mixed-form solve (state after t steps in buffer t mod 3).
+// The output tile is tzw x tyh cells of the (z, y) plane, 64 x 8 or 32 x 16
+// (per solve, whichever wastes fewer lanes on its grid); both shapes give
+// boxes of the same byte sizes.
 //   tm[b]  : state buffer b as a 4-D tensor (pz, ny, nx, 9 components);
-//            box (W, H, 1, 6) = the halo'd u and d of one plane
-//   tmc[b] : the same tensor, box (TZ, TY, 1, 3) = the Kahan compensation
-//   tmm    : material coefficients (pz, ny, nx, ncoef), box (TZ, TY, 1, ncoef)
+//            box (tzw + 8, tyh + 2, 1, 6) = the halo'd u and d of one plane
+//   tmc[b] : the same tensor, box (tzw, tyh, 1, 3) = the Kahan compensation
+//   tmm    : material coefficients (pz, ny, nx, ncoef), box (tzw, tyh, 1, ncoef)
 struct TmaF32 {
-  static constexpr int TZ = 64, TY = 8;  // output tile (z, y)
+  static constexpr int TZ = 64, TY = 8;  // the 64 x 8 shape; tzw * tyh == TZ * TY always
   static constexpr int W = TZ + 8;       // halo box width: 4 cells each side in z
   static constexpr int H = TY + 2;       // halo box height: 1 row each side in y
+  static_assert((32 + 8) * (16 + 2) == W * H, "the 32 x 16 box must match the 64 x 8 box");
   static constexpr int NA = 4;           // halo ring stages (planes x-1, x, x+1 + 1 ahead)
   static constexpr int NB = 3;           // point ring stages
   static constexpr int A_BYTES = W * H * 6 * 4;
@@ -41,6 +45,7 @@ struct TmaF32 {
   float hx, hy, hz, damp;
   int ncoef;  // 1: mu only, 2: mu and eta
   int use_damp, kahan, n_steps, snap_stride;
+  int tzw, tyh;   // output tile shape: 64 x 8 or 32 x 16
   float* snaps;
   int* flags;
   int it_begin;   // launch step index of this solve's step 0
@@ -134,10 +139,15 @@ void launch_fused2_raw(const TmaF32TB& t, int it, cudaStream_t s);  // enqueue o
 const void* step_f32_fused2_ptr();  // the single-solve fused kernel (for graph nodes)
 int launch_fused2_batch(const void* d_tab, int ninst, int ntiles, int it, cudaStream_t s);
 int tma_xchunk(const Geom& g, int tz, int ty, long long want_tiles);
-int make_tma_f32(const StepArgs& a, int xchunk, TmaF32* t);
+// Mixed-step tile width for a grid (64 or 32; the SW_TUNE_TILE_SHAPE knob
+// can force one) and the plane cells a tile width covers.
+int f32_tile_width(const Geom& g);
+long long f32_tile_cover(const Geom& g, int tzw);
+// tzw 0: f32_tile_width(a.g)
+int make_tma_f32(const StepArgs& a, int xchunk, TmaF32* t, int tzw);
 int make_tma_f64(const StepArgs& a, int xchunk, TmaF64* t);
 int launch_steps_tma(const StepArgs& a, int xchunk, int it0, int nsteps, cudaStream_t s);
 int launch_steps_tma_batch(int precision, const void* d_tab, int ninst, int ntiles, int it,
-                           int* queues, cudaStream_t s);
+                           int* queues, int tzw, cudaStream_t s);
 
 }  // namespace sw

@@ -45,6 +45,7 @@ __all__ = [
     "divergence_center",
     "elastic_solve_static",
     "gradient_center",
+    "hann1d",
     "laplacian_center",
     "project_body_force_to_shear",
     "project_vector_field",
@@ -263,6 +264,14 @@ def project_body_force_to_shear(bz, dX, dY, dZ, tol=5e-5, max_iters=400):
 # ---------------------------------------------------------------------------
 # shear_fdtd (solver.py:27-243) and the shear_fdtd_jax extras (246-566)
 # ---------------------------------------------------------------------------
+def hann1d(n):
+    """1-D Hann window of length n as float32 (solver.py:1053-1057); host helper
+    used to taper synthetic sources."""
+    if n <= 1:
+        return np.ones((n,), dtype=np.float32)
+    return np.hanning(n).astype(np.float32)
+
+
 def _check_jax_kwargs(n_steps, trace_indices, return_traces, snapshot_stride):
     """Validation of solver.py:290-303 and 396-408."""
     if return_traces and trace_indices is None:

@@ -1,7 +1,7 @@
 """Autotuner for the launch shape of the step kernels.
 
 The step kernels' results do not depend on how the grid is cut into tiles
-(every cell runs the same arithmetic), only their speed does.  Three
+(every cell runs the same arithmetic), only their speed does.  Four
 process-wide knobs of the CUDA library set the cut (enum ``sw_tune_knob``):
 
 * ``ctas_per_sm`` — resident step CTAs per SM (1 or 2): one CTA per SM
@@ -9,7 +9,10 @@ process-wide knobs of the CUDA library set the cut (enum ``sw_tune_knob``):
 * ``batch_tiles_per_cta`` — batched launches cut x into chunks so that
   about this many tiles fall to each CTA (more tiles balance better, each
   chunk re-reads two halo planes);
-* ``xchunk`` — planes per x chunk for every launch (0 = automatic).
+* ``xchunk`` — planes per x chunk for every launch (0 = automatic);
+* ``tile_shape`` — the mixed step kernel's (z, y) tile: 0 picks, per grid,
+  whichever of 64 x 8 and 32 x 16 covers the plane with fewer cells; 1 and
+  2 force one.
 
 :func:`autotune` times a shortened copy of a workload (one problem through
 ``shear_fdtd``, or a batch through ``shear_fdtd_batch``) under each
@@ -29,7 +32,7 @@ from pathlib import Path
 
 from . import _native
 
-KNOBS = {"ctas_per_sm": 0, "batch_tiles_per_cta": 1, "xchunk": 2}
+KNOBS = {"ctas_per_sm": 0, "batch_tiles_per_cta": 1, "xchunk": 2, "tile_shape": 3}
 
 __all__ = ["KNOBS", "get_knobs", "set_knobs", "knobs", "workload_key", "autotune",
            "apply_cached", "default_cache_path"]

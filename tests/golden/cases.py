@@ -63,7 +63,45 @@ CASES: dict[str, dict] = {
     "fdtd_initial": {"kind": "fdtd", "shape": (12, 14, 10), "dX": 0.5e-3, "dY": 0.5e-3,
                      "dZ": 0.5e-3, "dT": 10e-6, "n_steps": 15, "stride": 5, "seed": 7,
                      "physics": "initial"},
+    # radiation force: a focused tone burst recorded on a small grid; the
+    # auto gate (None), an explicit slice and an index array
+    "arf_auto": {"kind": "radiation", "shape": (10, 9, 12), "nt": 48, "f0": 1.0e6, "seed": 11,
+                 "gate": None},
+    "arf_slice": {"kind": "radiation", "shape": (7, 8, 9), "nt": 40, "f0": 0.5e6, "seed": 12,
+                  "gate": (6, 30, 2)},
+    "arf_index": {"kind": "radiation", "shape": (6, 5, 11), "nt": 70, "f0": 2.0e6, "seed": 13,
+                  "gate": [3, 4, 5, 9, 17, 33, 34, 60]},
+    # validate_wavespeed.py at its default size (float32 reference run only:
+    # the script runs the reference as shipped)
+    "wavespeed_default": {"kind": "wavespeed", "f32_only": True},
 }
+
+
+def radiation_inputs(case, dtype):
+    """Pressure and particle-velocity records (nx, ny, nz, nt), sound speed,
+    density and attenuation maps, and the gate of one radiation-force case."""
+    nx, ny, nz = case["shape"]
+    nt = case["nt"]
+    rng = np.random.default_rng(case["seed"])
+    x, y, z = np.meshgrid(np.linspace(-1, 1, nx), np.linspace(-1, 1, ny), np.linspace(-1, 1, nz),
+                          indexing="ij")
+    t = np.arange(nt)
+    burst = np.sin(2 * np.pi * 0.11 * t) * np.exp(-0.5 * ((t - 0.45 * nt) / (0.15 * nt)) ** 2)
+    focus = np.exp(-2.0 * (x**2 + y**2) - 0.7 * z**2)[..., None]
+    delay = (0.8 * z[..., None] * 4.0).astype(np.int64)
+    p = 1e5 * focus * np.take(burst, np.clip(t[None, None, None, :] - delay, 0, nt - 1))
+    p = p * (1.0 + 0.05 * rng.standard_normal(p.shape))
+    rc = 1500.0 * (1.0 + 0.03 * rng.uniform(-1, 1, (nx, ny, nz)))
+    rho = 1000.0 * (1.0 + 0.05 * rng.uniform(-1, 1, (nx, ny, nz)))
+    alpha = 0.5 + 0.3 * rng.uniform(0, 1, (nx, ny, nz))
+    v = [p / (rho * rc)[..., None] * w for w in (0.2 * x[..., None], 0.1 * y[..., None],
+                                                  np.ones_like(z)[..., None])]
+    v = [a * (1.0 + 0.05 * rng.standard_normal(a.shape)) for a in v]
+    c = lambda a: _f32(a).astype(dtype)  # noqa: E731
+    g = case["gate"]
+    gate = None if g is None else (slice(*g) if isinstance(g, tuple) else np.asarray(g))
+    return {"p": c(p), "vx": c(v[0]), "vy": c(v[1]), "vz": c(v[2]), "c": c(rc), "rho": c(rho),
+            "alpha": c(alpha), "f0": case["f0"], "gate": gate}
 
 
 def operator_inputs(case, dtype):

@@ -3,7 +3,7 @@
 Run in a container that has the pinton-lab/shearwave sources at
 ``/root/reference`` (override with ``SHEARWAVE_REF_SRC``):
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [case ...]
 
 Each case is run twice through the reference's own NumPy code:
 
@@ -32,6 +32,7 @@ import cases  # noqa: E402
 
 REF_SRC = os.environ.get("SHEARWAVE_REF_SRC", "/root/reference/src")
 sys.path.insert(0, REF_SRC)
+import shearwave.radiation_force as ref_arf  # noqa: E402
 import shearwave.solver as ref_solver  # noqa: E402
 import shearwave.strain as ref_strain  # noqa: E402
 
@@ -145,19 +146,57 @@ def _run_static(case: dict, wide: bool):
     return {"u": u, "apply_calls": np.int64(cnt.calls)}
 
 
+def _run_radiation(case: dict, wide: bool):
+    """radiation_force.py has no float32 casts: f32 runs float32 records and
+    maps, f64 the same values in float64."""
+    r = cases.radiation_inputs(case, np.float64 if wide else np.float32)
+    b = ref_arf.compute_radiation_force(r["p"], r["c"], r["rho"], r["alpha"], r["f0"],
+                                        gate=r["gate"])
+    bx, by, bz = ref_arf.compute_radiation_force_velocity(
+        r["p"], r["vx"], r["vy"], r["vz"], r["c"], r["rho"], r["alpha"], r["f0"], gate=r["gate"])
+    return {"b": b, "bx": bx, "by": by, "bz": bz}
+
+
+def _run_wavespeed(case: dict, wide: bool):
+    """validation/validate_wavespeed.py:21-205 at its defaults, through the
+    reference's shear_fdtd with a per-step callback recording u_z at the
+    sensors; the arrival analysis is shearwave_b200.validation's restatement
+    of the script's (the script itself needs matplotlib)."""
+    sys.path.insert(0, str(HERE.parents[1]))
+    from shearwave_b200 import validation as V
+
+    s = V.wavespeed_setup()
+    traces = np.zeros((len(s["sensor_offsets"]), s["n_steps"]), np.float32)
+    ix, iy, iz = s["trace_indices"]
+
+    def cb(it, u):
+        traces[:, it] = u[ix, iy, iz, 2]
+
+    ref_solver.shear_fdtd(None, None, s["bz"], s["rho"], s["mu"], s["dX"], s["dX"], s["dX"],
+                          s["dT"], s["n_steps"], opts=s["opts"], callback=cb)
+    r = V.arrival_analysis(traces, s["dT"], s["sensor_distances"], s["cs_target"])
+    return {"traces": traces, "arrival_idx": r["arrival_idx"], "c_fit": np.float64(r["c_fit"])}
+
+
 RUNNERS = {
     "fdtd": _run_fdtd,
     "projection": _run_projection,
     "operators": _run_operators,
     "strain": _run_strain,
     "static": _run_static,
+    "radiation": _run_radiation,
+    "wavespeed": _run_wavespeed,
 }
 
 
-def main() -> None:
+def main(names=None) -> None:
+    """Regenerate every fixture, or only the named cases."""
     for name, case in cases.CASES.items():
+        if names and name not in names:
+            continue
         payload = {"case": np.array(repr(case))}
-        for tag, wide in (("f32", False), ("f64", True)):
+        for tag, wide in (("f32", False),) + ((("f64", True),) if not case.get("f32_only")
+                                               else ()):
             out = RUNNERS[case["kind"]](case, wide)
             for k, v in out.items():
                 payload[f"{tag}_{k}"] = np.asarray(v)
@@ -167,4 +206,4 @@ def main() -> None:
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])

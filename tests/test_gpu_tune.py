@@ -7,10 +7,11 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 
-SETTINGS = [dict(ctas_per_sm=1, batch_tiles_per_cta=1, xchunk=0),
-            dict(ctas_per_sm=2, batch_tiles_per_cta=16, xchunk=0),
-            dict(ctas_per_sm=1, batch_tiles_per_cta=8, xchunk=5),
-            dict(ctas_per_sm=2, batch_tiles_per_cta=8, xchunk=64)]
+SETTINGS = [dict(ctas_per_sm=1, batch_tiles_per_cta=1, xchunk=0, tile_shape=0),
+            dict(ctas_per_sm=2, batch_tiles_per_cta=16, xchunk=0, tile_shape=1),
+            dict(ctas_per_sm=1, batch_tiles_per_cta=8, xchunk=5, tile_shape=2),
+            dict(ctas_per_sm=2, batch_tiles_per_cta=8, xchunk=64, tile_shape=2),
+            dict(ctas_per_sm=2, batch_tiles_per_cta=4, xchunk=0, tile_shape=1)]
 
 
 def _problems():

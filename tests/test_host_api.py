@@ -115,3 +115,30 @@ def test_no_cpu_fallback_without_a_gpu():
         pytest.skip("a CUDA device is present")
     with pytest.raises(RuntimeError, match="CUDA device"):
         _call(opts={"env_t": np.ones(4)})
+
+
+def test_hann1d_matches_reference_definition():
+    """hann1d (solver.py:1053-1057): numpy's Hann window as float32, ones for n <= 1."""
+    import numpy as np
+
+    from shearwave_b200 import hann1d
+
+    assert hann1d(0).shape == (0,) and hann1d(1).tolist() == [1.0]
+    w = hann1d(9)
+    assert w.dtype == np.float32
+    assert np.array_equal(w, np.hanning(9).astype(np.float32))
+
+
+def test_arrival_analysis_recovers_a_known_speed():
+    """Synthetic traces with pulses arriving at distance / c: the fit returns c."""
+    import numpy as np
+
+    from shearwave_b200.validation import arrival_analysis
+
+    dT, c = 1e-5, 2.5
+    dist = np.array([3e-3, 5e-3, 7e-3, 9e-3])
+    t = np.arange(800) * dT
+    traces = np.stack([np.tanh((t - d / c) / 4e-5) for d in dist])  # velocity peaks at d/c
+    r = arrival_analysis(traces, dT, dist, c)
+    assert abs(r["c_fit"] - c) / c < 0.02
+    assert np.all(np.abs(r["speeds"] - c) / c < 0.05)

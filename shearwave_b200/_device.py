@@ -47,7 +47,10 @@ def is_tensor(a) -> bool:
 def to_device(a, dtype: torch.dtype, dev: torch.device) -> torch.Tensor:
     """Contiguous device tensor of ``dtype`` holding ``a`` (copied if needed)."""
     if isinstance(a, torch.Tensor):
-        return a.to(device=dev, dtype=dtype).contiguous()
+        # page-locked host tensors copy asynchronously (stream-ordered before
+        # the kernels that read them; the caller keeps the source alive)
+        pinned = a.device.type == "cpu" and a.is_pinned()
+        return a.to(device=dev, dtype=dtype, non_blocking=pinned).contiguous()
     arr = np.ascontiguousarray(np.asarray(a), dtype=_NP[dtype])
     return torch.from_numpy(arr).to(dev)
 

@@ -646,6 +646,14 @@ class _Solve:
             self.tev[1].record()
 
     def finish(self, return_device: bool):
+        """Outputs of a finished solve (finish_enqueue + finish_collect)."""
+        return self.finish_collect(self.finish_enqueue(return_device))
+
+    def finish_enqueue(self, return_device: bool, copy_stream=None):
+        """Enqueue the output conversion (and, for host outputs, copies into
+        pinned host buffers on ``copy_stream``, which waits for the
+        conversion); nothing here waits for the GPU.  Returns the handle that
+        finish_collect turns into the result once the copies are done."""
         run, dt, dev = self.run, self.dt, self.dev
         nx, ny, nz = self.shape
         if self.tev is not None:
@@ -653,10 +661,42 @@ class _Solve:
         u = torch.empty((nx, ny, nz, 3), dtype=dt, device=dev)
         v = torch.empty((nx, ny, nz, 3), dtype=dt, device=dev)
         _native.call("sw_fdtd_finish", run.p(), self.n_steps, ptr(u), ptr(v), stream_handle())
-        nonfinite = bool(run.flags.item())
+        outs = [u, v]
+        if self.snaps is not None:
+            outs.append(self.snaps)
+        elif self.traces is not None:
+            outs.append(self.traces)
+        if self.tev is not None:
+            self.tev[3].record()
+        flag = torch.empty(1, dtype=torch.int32, pin_memory=True)
+        if return_device:
+            flag.copy_(run.flags, non_blocking=True)
+            return {"outs": outs, "flag": flag, "event": None, "device": True}
+        done = torch.cuda.Event()
+        done.record()
+        cs = copy_stream if copy_stream is not None else torch.cuda.current_stream()
+        cs.wait_event(done)
+        host = []
+        with torch.cuda.stream(cs):
+            for t in outs:
+                h = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
+                h.copy_(t, non_blocking=True)
+                t.record_stream(cs)  # the device buffer lives until the copy ran
+                host.append(h)
+            flag.copy_(run.flags, non_blocking=True)
+        ev = torch.cuda.Event()
+        ev.record(cs)
+        return {"outs": host, "flag": flag, "event": ev, "device": False}
+
+    def finish_collect(self, handle):
+        """Wait for a finish_enqueue handle and return the solve's result."""
+        if handle["event"] is not None:
+            handle["event"].synchronize()
+        else:
+            torch.cuda.current_stream().synchronize()
+        nonfinite = bool(int(handle["flag"][0]))
         if self.info is not None:
             tev = self.tev
-            tev[3].record()
             tev[3].synchronize()
             self.info.update(
                 cg=self.cg_log, nonfinite=nonfinite,
@@ -669,12 +709,9 @@ class _Solve:
         if nonfinite:
             warnings.warn("shear_fdtd: non-finite displacement encountered (unstable dT?)",
                           RuntimeWarning, stacklevel=3)
-        out = [to_host(u, return_device), to_host(v, return_device)]
-        if self.snaps is not None:
-            out.append(to_host(self.snaps, return_device))
-        elif self.traces is not None:
-            out.append(to_host(self.traces, return_device))
-        return tuple(out)
+        if handle["device"]:
+            return tuple(handle["outs"])
+        return tuple(h.numpy() for h in handle["outs"])
 
     def run_loop(self, callback, ws: "_Workspace"):
         """The time loop of solver.py:194-239 for this solve alone."""
@@ -826,15 +863,22 @@ def shear_fdtd_batch(problems, *, precision=None, return_device=False):
         return results
     precs = {sv.prec for _, sv in solves}
     groups = [[(i, sv) for i, sv in solves if sv.prec == pr] for pr in sorted(precs)]
+    copy_stream = None if return_device else torch.cuda.Stream(device=solves[0][1].dev)
     for group in groups:
-        _run_batch_group([sv for _, sv in group])
-        for i, sv in group:
-            results[i] = sv.finish(return_device)
+        handles = _run_batch_group([sv for _, sv in group], return_device, copy_stream)
+        for (i, sv), h in zip(group, handles):
+            results[i] = sv.finish_collect(h)
     return results
 
 
-def _run_batch_group(solves):
-    """Batched projection + batched time loop for solves of one precision."""
+def _run_batch_group(solves, return_device, copy_stream):
+    """Batched projection + batched time loop for solves of one precision.
+
+    The loop is enqueued in segments that end where a solve ends; each
+    finished solve's output conversion and copy to pinned host memory
+    (``copy_stream``) are enqueued right there, so they run while the
+    longer solves are still stepping.  Returns one finish handle per solve.
+    """
     lib = _native.load()
     dev = solves[0].dev
     strm = stream_handle()
@@ -888,8 +932,16 @@ def _run_batch_group(solves):
     tb = int(lib.sw_fdtd_batch_table_bytes(n))
     table = torch.empty(tb + 64, dtype=torch.uint8, device=dev)
     base = (table.data_ptr() + 63) // 64 * 64
-    steps = max(sv.n_steps for sv in solves)
-    _native.call("sw_fdtd_batch_steps", descs, None, n, 0, steps, base, tb, strm)
+    handles = [None] * n
+    it = 0
+    for end in sorted({sv.n_steps for sv in solves}):
+        if end > it:
+            _native.call("sw_fdtd_batch_steps", descs, None, n, it, end - it, base, tb, strm)
+            it = end
+        for k, sv in enumerate(solves):
+            if sv.n_steps == end:
+                handles[k] = sv.finish_enqueue(return_device, copy_stream)
+    return handles
 
 
 def shear_fdtd_jax(bx, by, bz, rho, mu, dX, dY, dZ, dT, n_steps, opts=None, callback=None,

@@ -261,6 +261,7 @@ __global__ void __launch_bounds__(TILE_THREADS) step_f32(const __grid_constant__
   const bool snap = a.snap_stride > 0 && a.snaps != nullptr && ((it + 1) % a.snap_stride) == 0;
   const int slot = snap ? (it + 1) / a.snap_stride - 1 : 0;
   const float hx = (float)a.ihx2, hy = (float)a.ihy2, hz = (float)a.ihz2;
+  const float hc = lap7_centre_coef(hx, hy, hz);
   const float damp = (float)a.damp;
   const long long sx = g.sxy, sy = g.pz, nc = g.ncell;
   for (int t = blockIdx.x; t < a.ts.count; t += gridDim.x) {
@@ -277,14 +278,12 @@ __global__ void __launch_bounds__(TILE_THREADS) step_f32(const __grid_constant__
         const float* U = S + c * nc;
         const float* Dd = S + (3 + c) * nc;
         const float u0 = U[i], d0 = Dd[i];
-        const float lu = ((U[i + sx] + U[i - sx]) - 2.0f * u0) * hx +
-                         ((U[i + sy] + U[i - sy]) - 2.0f * u0) * hy +
-                         ((U[i + 1] + U[i - 1]) - 2.0f * u0) * hz;
+        const float lu = lap7f(U[i + sx] + U[i - sx], U[i + sy] + U[i - sy], U[i + 1] + U[i - 1],
+                               u0, hx, hy, hz, hc);
         float inc = d0 + m * lu;
         if (er) {
-          const float ld = ((Dd[i + sx] + Dd[i - sx]) - 2.0f * d0) * hx +
-                           ((Dd[i + sy] + Dd[i - sy]) - 2.0f * d0) * hy +
-                           ((Dd[i + 1] + Dd[i - 1]) - 2.0f * d0) * hz;
+          const float ld = lap7f(Dd[i + sx] + Dd[i - sx], Dd[i + sy] + Dd[i - sy],
+                                 Dd[i + 1] + Dd[i - 1], d0, hx, hy, hz, hc);
           inc += e * ld;
         }
         for (int j = j0; j < j1; ++j)
@@ -332,9 +331,14 @@ __global__ void trace_kernel(const __grid_constant__ StepArgs a, int it) {
 // ---------------------------------------------------------------------------
 // outputs (solver.py:241-243)
 // ---------------------------------------------------------------------------
+// Also raises bit 0 of the solve's flag word when the final state holds a
+// non-finite value: a NaN or an infinity, once in u or d, stays there, so
+// the end state tells whether any step produced one (the mixed step kernels
+// leave this check to here).
 __global__ void finish_kernel(StepArgs a, int done, void* uo, void* vo) {
   const Geom g = a.g;
   const long long n = (long long)g.nx * g.ny * g.nz;
+  bool bad = false;
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n;
        q += (long long)gridDim.x * blockDim.x) {
     const int z = (int)(q % g.nz);
@@ -345,15 +349,20 @@ __global__ void finish_kernel(StepArgs a, int done, void* uo, void* vo) {
         const double* up = (const double*)a.state[done % 3];
         const double* uc = (const double*)a.state[(done + 1) % 3];
         const double cu = uc[c * g.ncell + i];
+        const double cv = (cu - up[c * g.ncell + i]) / a.dT;
         if (uo) ((double*)uo)[3 * q + c] = cu;
-        if (vo) ((double*)vo)[3 * q + c] = (cu - up[c * g.ncell + i]) / a.dT;
+        if (vo) ((double*)vo)[3 * q + c] = cv;
+        bad |= !isfinite(cu) || !isfinite(cv);
       } else {
         const float* S = (const float*)a.state[done % 3];
-        if (uo) ((float*)uo)[3 * q + c] = S[c * g.ncell + i];
-        if (vo) ((float*)vo)[3 * q + c] = S[(3 + c) * g.ncell + i] / (float)a.dT;
+        const float cu = S[c * g.ncell + i], cd = S[(3 + c) * g.ncell + i];
+        if (uo) ((float*)uo)[3 * q + c] = cu;
+        if (vo) ((float*)vo)[3 * q + c] = cd / (float)a.dT;
+        bad |= !isfinite(cu) || !isfinite(cd);
       }
     }
   }
+  if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0 && a.flags) atomicOr(a.flags, 1);
 }
 
 // dst = src * scale / rho  (see sw_convert)

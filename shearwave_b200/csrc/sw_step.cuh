@@ -33,6 +33,19 @@ struct StepArgs {
   int* clock;          // device step counter for graph replays (or null)
 };
 
+// 7-point Laplacian of the mixed form from the three neighbour-pair sums
+// (x+ + x-, y+ + y-, z+ + z-) and the centre value:
+//   hx sx + hy sy + hz sz + hc c,  hc = -2 ((hx + hy) + hz),
+// as one fixed chain of fused multiply-adds.  Every mixed-form kernel uses
+// these two functions, so all of them agree bit for bit.
+__device__ __forceinline__ float lap7_centre_coef(float hx, float hy, float hz) {
+  return -2.0f * ((hx + hy) + hz);
+}
+__device__ __forceinline__ float lap7f(float sx, float sy, float sz, float c, float hx, float hy,
+                                       float hz, float hc) {
+  return fmaf(hz, sz, fmaf(hy, sy, fmaf(hx, sx, hc * c)));
+}
+
 int make_step_args(const sw_fdtd_desc* d, StepArgs* a);
 int launch_steps(const StepArgs& a, int it0, int nsteps, cudaStream_t s);
 

@@ -193,7 +193,7 @@ __global__ void __launch_bounds__(TmaF32TB::THREADS, 1)
       const int slot1 = snap1 ? (lit + 1) / in->snap_stride - 1 : 0;
       const int slot2 = snap2 ? (lit + 2) / in->snap_stride - 1 : 0;
       const bool visc = in->ncoef > 1, kahan = in->kahan != 0;
-      const float hx = in->hx, hy = in->hy, hz = in->hz;
+      const float hx = in->hx, hy = in->hy, hz = in->hz, hc = lap7_centre_coef(hx, hy, hz);
       float mp[2] = {0.f, 0.f}, ep[2] = {0.f, 0.f}, cp[2][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
       bool ok = true;
       int s_prev = ca % NA;
@@ -235,14 +235,12 @@ __global__ void __launch_bounds__(TmaF32TB::THREADS, 1)
                 const int o = (comp * H + w + 1) * W + c + offA;
                 const int od = o + 3 * H * W;
                 const float u0 = Pc[o], d0 = Pc[od];
-                const float lu = ((Pn[o] + Pp[o]) - 2.0f * u0) * hx +
-                                 ((Pc[o + W] + Pc[o - W]) - 2.0f * u0) * hy +
-                                 ((Pc[o + 1] + Pc[o - 1]) - 2.0f * u0) * hz;
+                const float lu = lap7f(Pn[o] + Pp[o], Pc[o + W] + Pc[o - W],
+                                       Pc[o + 1] + Pc[o - 1], u0, hx, hy, hz, hc);
                 inc = d0 + mc[k] * lu;
                 if (visc) {
-                  const float ld = ((Pn[od] + Pp[od]) - 2.0f * d0) * hx +
-                                   ((Pc[od + W] + Pc[od - W]) - 2.0f * d0) * hy +
-                                   ((Pc[od + 1] + Pc[od - 1]) - 2.0f * d0) * hz;
+                  const float ld = lap7f(Pn[od] + Pp[od], Pc[od + W] + Pc[od - W],
+                                         Pc[od + 1] + Pc[od - 1], d0, hx, hy, hz, hc);
                   inc += ec[k] * ld;
                 }
                 for (int j = ja0; j < ja1; ++j)
@@ -296,14 +294,12 @@ __global__ void __launch_bounds__(TmaF32TB::THREADS, 1)
               const int o = (comp * LY + w) * LZ + c;
               const int od = o + 3 * LY * LZ;
               const float u0 = Lc[o], d0 = Lc[od];
-              const float lu = ((Ln[o] + Lp[o]) - 2.0f * u0) * hx +
-                               ((Lc[o + LZ] + Lc[o - LZ]) - 2.0f * u0) * hy +
-                               ((Lc[o + 1] + Lc[o - 1]) - 2.0f * u0) * hz;
+              const float lu = lap7f(Ln[o] + Lp[o], Lc[o + LZ] + Lc[o - LZ],
+                                     Lc[o + 1] + Lc[o - 1], u0, hx, hy, hz, hc);
               float inc = d0 + mp[k] * lu;
               if (visc) {
-                const float ld = ((Ln[od] + Lp[od]) - 2.0f * d0) * hx +
-                                 ((Lc[od + LZ] + Lc[od - LZ]) - 2.0f * d0) * hy +
-                                 ((Lc[od + 1] + Lc[od - 1]) - 2.0f * d0) * hz;
+                const float ld = lap7f(Ln[od] + Lp[od], Lc[od + LZ] + Lc[od - LZ],
+                                       Lc[od + 1] + Lc[od - 1], d0, hx, hy, hz, hc);
                 inc += ep[k] * ld;
               }
               for (int j = jb0; j < jb1; ++j)

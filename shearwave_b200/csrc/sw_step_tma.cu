@@ -98,14 +98,15 @@ __device__ __forceinline__ void stg2(float* p, float a, float b) {
 // boxes, `i` its global cell index.  The arithmetic per cell is the same
 // expression as in the direct kernel (sw_step.cu), so the results agree bit
 // for bit.  Cells outside the interior (z = 0, z >= nz-1) get 0, which is
-// what the shell and padding hold in every state buffer.
+// what the shell and padding hold in every state buffer.  Non-finite values
+// are detected once, in the finish kernel.
 template <bool VISC, bool KAHAN>
 __device__ __forceinline__ void f32_pair_plane(
     const float* __restrict__ Pc, const float* __restrict__ Pn, const float* __restrict__ Bc,
     const float* __restrict__ Bm, int o, int ob, int W, float2 (&pu)[3], float2 (&pd)[3],
-    bool act_a, bool act_b, float hx, float hy, float hz, bool use_damp, float damp,
+    bool act_a, bool act_b, float hx, float hy, float hz, float hc, bool use_damp, float damp,
     const TmaF32* __restrict__ in, int j0, int j1, long long nc, long long i,
-    float* __restrict__ D, float2 (&un)[3], bool& bad) {
+    float* __restrict__ D, float2 (&un)[3]) {
   // the halo box holds W x H = 720 cells per component for both tile shapes,
   // and a point box tzw x tyh = 512 cells per component
   constexpr int HW = TmaF32::H * TmaF32::W, PT = TmaF32::TZ * TmaF32::TY;
@@ -116,19 +117,15 @@ __device__ __forceinline__ void f32_pair_plane(
     const int oc = o + c * HW, od = oc + 3 * HW;
     const float2 C = lds2(Pc + oc), L = lds2(Pc + oc - 2), R = lds2(Pc + oc + 2);
     const float2 N = lds2(Pc + oc + W), S = lds2(Pc + oc - W), X = lds2(Pn + oc);
-    const float lua = ((X.x + pu[c].x) - 2.0f * C.x) * hx + ((N.x + S.x) - 2.0f * C.x) * hy +
-                      ((C.y + L.y) - 2.0f * C.x) * hz;
-    const float lub = ((X.y + pu[c].y) - 2.0f * C.y) * hx + ((N.y + S.y) - 2.0f * C.y) * hy +
-                      ((R.x + C.x) - 2.0f * C.y) * hz;
+    const float lua = lap7f(X.x + pu[c].x, N.x + S.x, C.y + L.y, C.x, hx, hy, hz, hc);
+    const float lub = lap7f(X.y + pu[c].y, N.y + S.y, R.x + C.x, C.y, hx, hy, hz, hc);
     const float2 Cd = lds2(Pc + od);
     float inca = Cd.x + M.x * lua, incb = Cd.y + M.y * lub;
     if (VISC) {
       const float2 Ld = lds2(Pc + od - 2), Rd = lds2(Pc + od + 2);
       const float2 Nd = lds2(Pc + od + W), Sd = lds2(Pc + od - W), Xd = lds2(Pn + od);
-      const float lda = ((Xd.x + pd[c].x) - 2.0f * Cd.x) * hx +
-                        ((Nd.x + Sd.x) - 2.0f * Cd.x) * hy + ((Cd.y + Ld.y) - 2.0f * Cd.x) * hz;
-      const float ldb = ((Xd.y + pd[c].y) - 2.0f * Cd.y) * hx +
-                        ((Nd.y + Sd.y) - 2.0f * Cd.y) * hy + ((Rd.x + Cd.x) - 2.0f * Cd.y) * hz;
+      const float lda = lap7f(Xd.x + pd[c].x, Nd.x + Sd.x, Cd.y + Ld.y, Cd.x, hx, hy, hz, hc);
+      const float ldb = lap7f(Xd.y + pd[c].y, Nd.y + Sd.y, Rd.x + Cd.x, Cd.y, hx, hy, hz, hc);
       inca += E.x * lda;
       incb += E.y * ldb;
     }
@@ -159,12 +156,24 @@ __device__ __forceinline__ void f32_pair_plane(
     ub = act_b ? ub : 0.f;
     stg2(D + c * nc + i, ua, ub);
     stg2(D + (3 + c) * nc + i, act_a ? inca : 0.f, act_b ? incb : 0.f);
-    bad |= !isfinite(ua) || !isfinite(ub);
     un[c] = make_float2(ua, ub);
   }
 }
 
-template <bool BATCH, int TZW>
+// Ring layout of the mixed step kernel.  With room for the compensation
+// planes (KR) a point stage holds c then the coefficients and the halo ring
+// has 4 stages; without, a point stage holds the coefficients only and the
+// space goes to a fifth halo stage (three planes in flight instead of two).
+template <bool KR>
+struct F32Ring {
+  static constexpr int NA = KR ? 4 : 5, NB = 3;
+  static constexpr int C_OFF = KR ? round128(TmaF32::C_BYTES) : 0;  // coefficients, bytes
+  static constexpr int B_STAGE = C_OFF + round128(TmaF32::M_BYTES);
+  static constexpr size_t SMEM = 128 + 256 + (size_t)NA * TmaF32::A_STAGE + (size_t)NB * B_STAGE;
+};
+static_assert(F32Ring<false>::SMEM <= F32Ring<true>::SMEM, "the compact ring must not be larger");
+
+template <bool BATCH, int TZW, bool KR>
 __global__ void __launch_bounds__(TmaF32::THREADS, 2)
     step_f32_tma(const __grid_constant__ TmaF32 one, const TmaF32* __restrict__ tab, int ninst,
                  int ntiles, int it, const int* __restrict__ it_dev, int* queues) {
@@ -177,10 +186,10 @@ __global__ void __launch_bounds__(TmaF32::THREADS, 2)
   // for the next launch of the stream
   int* queue = (BATCH && queues != nullptr) ? queues + (it & 1) : nullptr;
   if (queue != nullptr && blockIdx.x == 0 && threadIdx.x == 0) queues[(it + 1) & 1] = 0;
-  constexpr int NA = TmaF32::NA, NB = TmaF32::NB, W = TmaF32::W, H = TmaF32::H;
+  constexpr int NA = F32Ring<KR>::NA, NB = F32Ring<KR>::NB, W = TmaF32::W, H = TmaF32::H;
   constexpr int TZ = TmaF32::TZ, TY = TmaF32::TY;
-  constexpr int AF = TmaF32::A_STAGE / 4, BF = TmaF32::B_STAGE / 4;  // floats per stage
-  constexpr int CF = round128(TmaF32::C_BYTES) / 4;                  // offset of coefficients
+  constexpr int AF = TmaF32::A_STAGE / 4, BF = F32Ring<KR>::B_STAGE / 4;  // floats per stage
+  constexpr int CF = F32Ring<KR>::C_OFF / 4;  // offset of the coefficients in a point stage
   extern __shared__ unsigned char smem_raw[];
   unsigned char* base = smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u);
   WsHeader* hd = reinterpret_cast<WsHeader*>(base);
@@ -230,7 +239,8 @@ __global__ void __launch_bounds__(TmaF32::THREADS, 2)
         const TileCoord tc = tile_coord_t(in->g, in->ts, local, TZW, TYH);
         const CUtensorMap* tma = &in->tm[lit % 3];
         const CUtensorMap* tmc = &in->tmc[lit % 3];
-        const uint32_t bbytes = (in->kahan ? TmaF32::C_BYTES : 0) + TZ * TY * 4 * in->ncoef;
+        const bool kahan = KR && in->kahan;  // the compact ring never carries c
+        const uint32_t bbytes = (kahan ? TmaF32::C_BYTES : 0) + TZ * TY * 4 * in->ncoef;
         for (int p = tc.x0 - 1; p <= tc.x1 && !*abort_flag; ++p) {
           const int sa = pa % NA;
           if (!ws_wait(&hd->emptyA[sa], ((pa / NA) & 1u) ^ 1u, abort_flag)) break;
@@ -247,7 +257,7 @@ __global__ void __launch_bounds__(TmaF32::THREADS, 2)
             if (!ws_wait(&hd->emptyB[sb], ((pb / NB) & 1u) ^ 1u, abort_flag)) break;
             fence_proxy_async_smem();
             mbar_arrive_expect_tx(&hd->fullB[sb], bbytes);
-            if (in->kahan) tma_load_4d(ringB + sb * BF, tmc, &hd->fullB[sb], tc.z0, tc.y0, p, 6);
+            if (kahan) tma_load_4d(ringB + sb * BF, tmc, &hd->fullB[sb], tc.z0, tc.y0, p, 6);
             tma_load_4d(ringB + sb * BF + CF, &in->tmm, &hd->fullB[sb], tc.z0, tc.y0, p, 0);
             ++pb;
           }
@@ -273,7 +283,7 @@ __global__ void __launch_bounds__(TmaF32::THREADS, 2)
       constexpr int tzw = TZW;
       const TileCoord tc = tile_coord_t(g, in->ts, local, TZW, TYH);
       float* __restrict__ D = in->state[(lit + 1) % 3];
-      const bool kahan = in->kahan != 0, use_damp = in->use_damp != 0;
+      const bool kahan = KR && in->kahan != 0, use_damp = in->use_damp != 0;
       const float damp = in->damp;
       // this thread's cells: the pair z, z+1 of tile row `row`; a warp covers
       // one row of 32 pairs (64 x 8 tiles) or two rows of 16 (32 x 16 tiles)
@@ -293,7 +303,7 @@ __global__ void __launch_bounds__(TmaF32::THREADS, 2)
       const int slot = snap ? (lit + 1) / in->snap_stride - 1 : 0;
       const long long nc = g.ncell;
       const bool visc = in->ncoef > 1;
-      const float hx = in->hx, hy = in->hy, hz = in->hz;
+      const float hx = in->hx, hy = in->hy, hz = in->hz, hc = lap7_centre_coef(hx, hy, hz);
       const int o = (row + 1) * Wb + lz + 4, ob = row * tzw + lz;
       // Plane x-1 enters only through its centre values (x neighbours of the
       // Laplacians), which each thread keeps in registers from the plane it
@@ -330,21 +340,20 @@ __global__ void __launch_bounds__(TmaF32::THREADS, 2)
           const float* Bc = ringB + sb * BF;
           const float* Bm = Bc + CF;
           float2 un[3];
-          bool bad = false;
           if (visc) {
             if (kahan)
               f32_pair_plane<true, true>(Pc, Pn, Bc, Bm, o, ob, Wb, pu, pd, act_a, act_b, hx, hy, hz,
-                                         use_damp, damp, in, j0, j1, nc, i, D, un, bad);
+                                         hc, use_damp, damp, in, j0, j1, nc, i, D, un);
             else
               f32_pair_plane<true, false>(Pc, Pn, Bc, Bm, o, ob, Wb, pu, pd, act_a, act_b, hx, hy, hz,
-                                          use_damp, damp, in, j0, j1, nc, i, D, un, bad);
+                                          hc, use_damp, damp, in, j0, j1, nc, i, D, un);
           } else {
             if (kahan)
               f32_pair_plane<false, true>(Pc, Pn, Bc, Bm, o, ob, Wb, pu, pd, act_a, act_b, hx, hy,
-                                          hz, use_damp, damp, in, j0, j1, nc, i, D, un, bad);
+                                          hz, hc, use_damp, damp, in, j0, j1, nc, i, D, un);
             else
               f32_pair_plane<false, false>(Pc, Pn, Bc, Bm, o, ob, Wb, pu, pd, act_a, act_b, hx, hy,
-                                           hz, use_damp, damp, in, j0, j1, nc, i, D, un, bad);
+                                           hz, hc, use_damp, damp, in, j0, j1, nc, i, D, un);
           }
           if (snap) {
             float* sp = in->snaps + ((((long long)slot * g.nx + x) * g.ny + y) * g.nz + z) * 3;
@@ -354,7 +363,6 @@ __global__ void __launch_bounds__(TmaF32::THREADS, 2)
               if (act_b) sp[3 + c] = un[c].y;
             }
           }
-          if (bad && in->flags) atomicOr(in->flags, 1);
         }
         __syncwarp();
         if (lane == 0) {
@@ -602,7 +610,29 @@ __global__ void __launch_bounds__(TmaF64::THREADS, 2)
 size_t tma_smem_bytes(int precision) {
   if (precision == SW_PLAIN_F64)
     return 128 + 256 + (size_t)TmaF64::NA * TmaF64::A_STAGE + (size_t)TmaF64::NB * TmaF64::B_STAGE;
-  return 128 + 256 + (size_t)TmaF32::NA * TmaF32::A_STAGE + (size_t)TmaF32::NB * TmaF32::B_STAGE;
+  return F32Ring<true>::SMEM;  // the larger of the two mixed layouts
+}
+
+// The mixed step kernel for a launch: batched or not, tile width, ring layout.
+static const void* f32_kernel(bool batch, int tzw, bool kr) {
+  if (batch) {
+    if (tzw == 32) return kr ? (const void*)step_f32_tma<true, 32, true>
+                             : (const void*)step_f32_tma<true, 32, false>;
+    return kr ? (const void*)step_f32_tma<true, 64, true> : (const void*)step_f32_tma<true, 64, false>;
+  }
+  if (tzw == 32) return kr ? (const void*)step_f32_tma<false, 32, true>
+                           : (const void*)step_f32_tma<false, 32, false>;
+  return kr ? (const void*)step_f32_tma<false, 64, true> : (const void*)step_f32_tma<false, 64, false>;
+}
+
+static size_t f32_smem(bool kr) { return kr ? F32Ring<true>::SMEM : F32Ring<false>::SMEM; }
+
+static void launch_f32(const void* fn, int grid, size_t smem, cudaStream_t s, const TmaF32& one,
+                       const TmaF32* tab, int ninst, int ntiles, int it, int* queues) {
+  const int* itd = nullptr;
+  void* args[] = {(void*)&one, (void*)&tab, (void*)&ninst, (void*)&ntiles, (void*)&it,
+                  (void*)&itd, (void*)&queues};
+  cudaLaunchKernel(fn, dim3(grid), dim3(TmaF32::THREADS), args, smem, s);
 }
 
 static int set_smem_attr(int precision) {
@@ -618,11 +648,12 @@ static int set_smem_attr(int precision) {
       e = cudaFuncSetAttribute(step_f64_tma<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                bytes);
   } else {
-    const void* fns[4] = {(const void*)step_f32_tma<false, 64>, (const void*)step_f32_tma<true, 64>,
-                          (const void*)step_f32_tma<false, 32>, (const void*)step_f32_tma<true, 32>};
     e = cudaSuccess;
-    for (int i = 0; i < 4 && e == cudaSuccess; ++i)
-      e = cudaFuncSetAttribute(fns[i], cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    for (int i = 0; i < 8 && e == cudaSuccess; ++i) {
+      const bool kr = i & 1;
+      e = cudaFuncSetAttribute(f32_kernel(i & 4, (i & 2) ? 32 : 64, kr),
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)f32_smem(kr));
+    }
   }
   if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(step smem)");
   done[k] = true;
@@ -883,21 +914,17 @@ int launch_steps_tma(const StepArgs& a, int xchunk, int it0, int nsteps, cudaStr
                       std::min(tb.ts.count, 148), TmaF32TB::THREADS, tb_smem_bytes(), 2, 16,
                       a.clock, it0, nsteps, s, &done);
     else
-      rc = graph_loop(t.tzw == 64 ? reinterpret_cast<void*>(step_f32_tma<false, 64>)
-                                  : reinterpret_cast<void*>(step_f32_tma<false, 32>),
-                      t, grid, TmaF32::THREADS, smem, 1, 32, a.clock, it0, nsteps, s, &done);
+      rc = graph_loop(const_cast<void*>(f32_kernel(false, t.tzw, t.kahan != 0)), t, grid,
+                      TmaF32::THREADS, f32_smem(t.kahan != 0), 1, 32, a.clock, it0, nsteps, s,
+                      &done);
     if (rc != SW_OK) return rc;
     for (int it = it0 + done; it < it0 + nsteps;) {
       if (fuse && it + 1 < it0 + nsteps) {
         launch_fused2_raw(tb, it, s);
         it += 2;
       } else {
-        if (t.tzw == 64)
-          step_f32_tma<false, 64><<<grid, TmaF32::THREADS, smem, s>>>(t, nullptr, 1, t.ts.count,
-                                                                      it, nullptr, nullptr);
-        else
-          step_f32_tma<false, 32><<<grid, TmaF32::THREADS, smem, s>>>(t, nullptr, 1, t.ts.count,
-                                                                      it, nullptr, nullptr);
+        launch_f32(f32_kernel(false, t.tzw, t.kahan != 0), grid, f32_smem(t.kahan != 0), s, t,
+                   nullptr, 1, t.ts.count, it, nullptr);
         it += 1;
       }
       ++n_launch;
@@ -912,7 +939,7 @@ int launch_steps_tma(const StepArgs& a, int xchunk, int it0, int nsteps, cudaStr
 }
 
 int launch_steps_tma_batch(int precision, const void* d_tab, int ninst, int ntiles, int it,
-                           int* queues, int tzw, cudaStream_t s) {
+                           int* queues, int tzw, bool kahan_ring, cudaStream_t s) {
   int rc = set_smem_attr(precision);
   if (rc != SW_OK) return rc;
   if (ntiles == 0) return SW_OK;
@@ -924,12 +951,8 @@ int launch_steps_tma_batch(int precision, const void* d_tab, int ninst, int ntil
                                                           ntiles, it, nullptr, queues);
   } else {
     TmaF32 dummy{};
-    if (tzw == 32)
-      step_f32_tma<true, 32><<<grid, TmaF32::THREADS, smem, s>>>(dummy, (const TmaF32*)d_tab,
-                                                                ninst, ntiles, it, nullptr, queues);
-    else
-      step_f32_tma<true, 64><<<grid, TmaF32::THREADS, smem, s>>>(dummy, (const TmaF32*)d_tab,
-                                                                ninst, ntiles, it, nullptr, queues);
+    launch_f32(f32_kernel(true, tzw, kahan_ring), grid, f32_smem(kahan_ring), s, dummy,
+               (const TmaF32*)d_tab, ninst, ntiles, it, queues);
   }
   count_launches(1);
   SW_CHECK_LAUNCH("step (tma, batch)");
@@ -1119,8 +1142,10 @@ int batch_steps_mixed(const sw_fdtd_desc* descs, const int32_t* begins, int n, i
       rc = launch_fused2_batch(tab_fused, (int)tfused.size(), ntiles, it, s);
       it += 2;
     } else {
+      bool kr = false;  // the compensation ring layout if any running solve needs it
+      for (const TmaF32& t : tsingle) kr |= t.kahan != 0;
       rc = launch_steps_tma_batch(SW_MIXED_F32, tab_single, (int)tsingle.size(), ntiles, it,
-                                  queues, tsingle.empty() ? 64 : tsingle[0].tzw, s);
+                                  queues, tsingle.empty() ? 64 : tsingle[0].tzw, kr, s);
       it += 1;
     }
     if (rc != SW_OK) return rc;
@@ -1162,7 +1187,8 @@ int batch_steps(int precision, const sw_fdtd_desc* descs, const int32_t* begins,
       have = true;
     }
     if (tab.empty()) continue;
-    int rc = launch_steps_tma_batch(precision, table, (int)tab.size(), ntiles, it, queues, 0, s);
+    int rc = launch_steps_tma_batch(precision, table, (int)tab.size(), ntiles, it, queues, 0,
+                                    false, s);
     if (rc != SW_OK) return rc;
   }
   return SW_OK;

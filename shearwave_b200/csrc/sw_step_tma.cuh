@@ -23,8 +23,6 @@ struct TmaF32 {
   static constexpr int W = TZ + 8;       // halo box width: 4 cells each side in z
   static constexpr int H = TY + 2;       // halo box height: 1 row each side in y
   static_assert((32 + 8) * (16 + 2) == W * H, "the 32 x 16 box must match the 64 x 8 box");
-  static constexpr int NA = 4;           // halo ring stages (planes x-1, x, x+1 + 1 ahead)
-  static constexpr int NB = 3;           // point ring stages
   static constexpr int A_BYTES = W * H * 6 * 4;
   static constexpr int C_BYTES = TZ * TY * 3 * 4;
   static constexpr int M_BYTES = TZ * TY * 2 * 4;
@@ -148,6 +146,6 @@ int make_tma_f32(const StepArgs& a, int xchunk, TmaF32* t, int tzw);
 int make_tma_f64(const StepArgs& a, int xchunk, TmaF64* t);
 int launch_steps_tma(const StepArgs& a, int xchunk, int it0, int nsteps, cudaStream_t s);
 int launch_steps_tma_batch(int precision, const void* d_tab, int ninst, int ntiles, int it,
-                           int* queues, int tzw, cudaStream_t s);
+                           int* queues, int tzw, bool kahan_ring, cudaStream_t s);
 
 }  // namespace sw

@@ -137,3 +137,41 @@ def test_cuda_graph_replay_matches_direct_launches(cuda, precision, spp):
 
     for x, y in zip(run(True), run(False)):
         assert np.array_equal(x, y)
+
+
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_unstable_run_is_flagged(cuda, precision):
+    """An unstable dT (viscous number 240, limit 2) overflows within 300 steps
+    in both forms; the solve reports it (info["nonfinite"] and a
+    RuntimeWarning), alone and batched."""
+    import warnings
+
+    import numpy as np
+
+    import shearwave_b200 as sw
+    from shearwave_b200 import workloads as W
+
+    shape = (20, 18, 22)
+    bz = W.gaussian_push(shape, [(n - 1) / 2 * W.H for n in shape])
+    n = 300
+    env = np.zeros(n, np.float32)
+    env[:5] = 1
+    opts = {"eta": 5.0, "env_t": env, "poisson_tol": 1e-8, "poisson_max_iters": 200,
+            "precision": precision}
+    for batched in (False, True):
+        info = {}
+        o = dict(opts, info=info)
+        with warnings.catch_warnings(record=True) as rec:
+            warnings.simplefilter("always")
+            if batched:
+                p = dict(bx=None, by=None, bz=bz, rho=1000.0, mu=3e3, dX=W.H, dY=W.H, dZ=W.H,
+                         dT=1e-3, n_steps=n, opts=o)
+                sw.shear_fdtd_batch([p, dict(p, opts=dict(opts))])
+            else:
+                sw.shear_fdtd(None, None, bz, 1000.0, 3e3, W.H, W.H, W.H, 1e-3, n, o)
+        assert info["nonfinite"], batched
+        assert any(issubclass(w.category, RuntimeWarning) for w in rec), batched
+    # and a stable run is not flagged
+    info = {}
+    sw.shear_fdtd(None, None, bz, 1000.0, 3e3, W.H, W.H, W.H, 1e-6, n, dict(opts, info=info))
+    assert not info["nonfinite"]

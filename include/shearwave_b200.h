@@ -85,10 +85,10 @@ uint64_t sw_launch_count(void);
  * change how the grid is cut into tiles, never the results.  Process-wide;
  * set them between solves, not while one is running.                      */
 enum sw_tune_knob {
-  SW_TUNE_STEP_CTAS_PER_SM = 0,    /* resident step CTAs per SM: 1 or 2 (default 2) */
+  SW_TUNE_STEP_CTAS_PER_SM = 0,    /* step CTAs per SM a launch is sized for: 1 or 2 (2) */
   SW_TUNE_BATCH_TILES_PER_CTA = 1, /* batched launches: tiles per CTA, 1..64 (8)   */
   SW_TUNE_XCHUNK = 2,              /* planes per x chunk, 0 = automatic (0)          */
-  SW_TUNE_TILE_SHAPE = 3,          /* mixed step tiles: 0 auto, 1 64x8, 2 32x16 (0)  */
+  SW_TUNE_TILE_SHAPE = 3,          /* mixed step tiles: 0 auto, 1 64-wide, 2 32-wide */
   SW_TUNE_COUNT = 4
 };
 /* SW_EINVAL for an unknown knob or a value out of range. */

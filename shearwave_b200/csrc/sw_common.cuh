@@ -186,8 +186,12 @@ void set_error(const char* fmt, ...);
 // Launch-shape knob (enum sw_tune_knob), process-wide.
 int tune_get(int knob);
 constexpr int kNumSMs = 148;  // B200
-// Resident CTA slots of the step kernels (SMs x CTAs per SM).
-inline int step_slots() { return kNumSMs * tune_get(SW_TUNE_STEP_CTAS_PER_SM); }
+// CTA slots a step launch is sized for (SMs x CTAs per SM): the mixed
+// kernel follows the SW_TUNE_STEP_CTAS_PER_SM knob, the plain FP64 kernel
+// always fits two CTAs per SM.
+inline int step_slots(bool mixed = true) {
+  return kNumSMs * (mixed ? tune_get(SW_TUNE_STEP_CTAS_PER_SM) : 2);
+}
 int cuda_status(cudaError_t e, const char* what);
 // Count kernel launches issued by this library (exported as sw_launch_count).
 void count_launches(unsigned long long n);

@@ -100,16 +100,15 @@ __device__ __forceinline__ void stg2(float* p, float a, float b) {
 // for bit.  Cells outside the interior (z = 0, z >= nz-1) get 0, which is
 // what the shell and padding hold in every state buffer.  Non-finite values
 // are detected once, in the finish kernel.
-template <bool VISC, bool KAHAN>
+template <bool VISC, bool KAHAN, int HW>
 __device__ __forceinline__ void f32_pair_plane(
     const float* __restrict__ Pc, const float* __restrict__ Pn, const float* __restrict__ Bc,
     const float* __restrict__ Bm, int o, int ob, int W, float2 (&pu)[3], float2 (&pd)[3],
     bool act_a, bool act_b, float hx, float hy, float hz, float hc, bool use_damp, float damp,
     const TmaF32* __restrict__ in, int j0, int j1, long long nc, long long i,
     float* __restrict__ D, float2 (&un)[3]) {
-  // the halo box holds W x H = 720 cells per component for both tile shapes,
-  // and a point box tzw x tyh = 512 cells per component
-  constexpr int HW = TmaF32::H * TmaF32::W, PT = TmaF32::TZ * TmaF32::TY;
+  // HW: halo-box cells per component; a point box holds PT cells per component
+  constexpr int PT = TmaF32::PT;
   const float2 M = lds2(Bm + ob);
   const float2 E = VISC ? lds2(Bm + PT + ob) : make_float2(0.f, 0.f);
 #pragma unroll
@@ -166,7 +165,7 @@ __device__ __forceinline__ void f32_pair_plane(
 // space goes to a fifth halo stage (three planes in flight instead of two).
 template <bool KR>
 struct F32Ring {
-  static constexpr int NA = KR ? 4 : 5, NB = 3;
+  static constexpr int NA = TmaF32::MIN_CTAS == 2 ? (KR ? 4 : 5) : (KR ? 5 : 6), NB = 3;
   static constexpr int C_OFF = KR ? round128(TmaF32::C_BYTES) : 0;  // coefficients, bytes
   static constexpr int B_STAGE = C_OFF + round128(TmaF32::M_BYTES);
   static constexpr size_t SMEM = 128 + 256 + (size_t)NA * TmaF32::A_STAGE + (size_t)NB * B_STAGE;
@@ -174,7 +173,7 @@ struct F32Ring {
 static_assert(F32Ring<false>::SMEM <= F32Ring<true>::SMEM, "the compact ring must not be larger");
 
 template <bool BATCH, int TZW, bool KR>
-__global__ void __launch_bounds__(TmaF32::THREADS, 2)
+__global__ void __launch_bounds__(TmaF32::THREADS, TmaF32::MIN_CTAS)
     step_f32_tma(const __grid_constant__ TmaF32 one, const TmaF32* __restrict__ tab, int ninst,
                  int ntiles, int it, const int* __restrict__ it_dev, int* queues) {
   // tile shape: TZW x TYH cells (64 x 8, or 32 x 16); every solve of a
@@ -186,7 +185,9 @@ __global__ void __launch_bounds__(TmaF32::THREADS, 2)
   // for the next launch of the stream
   int* queue = (BATCH && queues != nullptr) ? queues + (it & 1) : nullptr;
   if (queue != nullptr && blockIdx.x == 0 && threadIdx.x == 0) queues[(it + 1) & 1] = 0;
-  constexpr int NA = F32Ring<KR>::NA, NB = F32Ring<KR>::NB, W = TmaF32::W, H = TmaF32::H;
+  constexpr int NA = F32Ring<KR>::NA, NB = F32Ring<KR>::NB;
+  constexpr int HWB = TmaF32::box_cells(TZW);                   // halo-box cells per component
+  constexpr uint32_t A_BYTES = (uint32_t)HWB * 6 * 4;          // one plane's u and d
   constexpr int TZ = TmaF32::TZ, TY = TmaF32::TY;
   constexpr int AF = TmaF32::A_STAGE / 4, BF = F32Ring<KR>::B_STAGE / 4;  // floats per stage
   constexpr int CF = F32Ring<KR>::C_OFF / 4;  // offset of the coefficients in a point stage
@@ -249,7 +250,7 @@ __global__ void __launch_bounds__(TmaF32::THREADS, 2)
             solve_slots(base)[sa] = k;
           }
           fence_proxy_async_smem();
-          mbar_arrive_expect_tx(&hd->fullA[sa], TmaF32::A_BYTES);
+          mbar_arrive_expect_tx(&hd->fullA[sa], A_BYTES);
           tma_load_4d(ringA + sa * AF, tma, &hd->fullA[sa], tc.z0 - 4, tc.y0 - 1, p, 0);
           ++pa;
           if (p >= tc.x0 && p < tc.x1) {
@@ -316,8 +317,8 @@ __global__ void __launch_bounds__(TmaF32::THREADS, 2)
         const float* P0 = ringA + s_cur * AF;
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-          pu[c] = lds2(P0 + o + c * H * W);
-          pd[c] = lds2(P0 + o + (3 + c) * H * W);
+          pu[c] = lds2(P0 + o + c * HWB);
+          pd[c] = lds2(P0 + o + (3 + c) * HWB);
         }
       }
       __syncwarp();
@@ -342,17 +343,17 @@ __global__ void __launch_bounds__(TmaF32::THREADS, 2)
           float2 un[3];
           if (visc) {
             if (kahan)
-              f32_pair_plane<true, true>(Pc, Pn, Bc, Bm, o, ob, Wb, pu, pd, act_a, act_b, hx, hy, hz,
+              f32_pair_plane<true, true, HWB>(Pc, Pn, Bc, Bm, o, ob, Wb, pu, pd, act_a, act_b, hx, hy, hz,
                                          hc, use_damp, damp, in, j0, j1, nc, i, D, un);
             else
-              f32_pair_plane<true, false>(Pc, Pn, Bc, Bm, o, ob, Wb, pu, pd, act_a, act_b, hx, hy, hz,
+              f32_pair_plane<true, false, HWB>(Pc, Pn, Bc, Bm, o, ob, Wb, pu, pd, act_a, act_b, hx, hy, hz,
                                           hc, use_damp, damp, in, j0, j1, nc, i, D, un);
           } else {
             if (kahan)
-              f32_pair_plane<false, true>(Pc, Pn, Bc, Bm, o, ob, Wb, pu, pd, act_a, act_b, hx, hy,
+              f32_pair_plane<false, true, HWB>(Pc, Pn, Bc, Bm, o, ob, Wb, pu, pd, act_a, act_b, hx, hy,
                                           hz, hc, use_damp, damp, in, j0, j1, nc, i, D, un);
             else
-              f32_pair_plane<false, false>(Pc, Pn, Bc, Bm, o, ob, Wb, pu, pd, act_a, act_b, hx, hy,
+              f32_pair_plane<false, false, HWB>(Pc, Pn, Bc, Bm, o, ob, Wb, pu, pd, act_a, act_b, hx, hy,
                                            hz, hc, use_damp, damp, in, j0, j1, nc, i, D, un);
           }
           if (snap) {
@@ -765,7 +766,7 @@ int make_tma_f64(const StepArgs& a, int xchunk, TmaF64* t) {
   *t = TmaF64{};
   t->g = a.g;
   const int xt = xchunk > 0 ? xchunk : tune_get(SW_TUNE_XCHUNK);
-  const int xc = xt > 0 ? xt : tma_xchunk(a.g, TmaF64::TZ, TmaF64::TY, step_slots());
+  const int xc = xt > 0 ? xt : tma_xchunk(a.g, TmaF64::TZ, TmaF64::TY, step_slots(false));
   t->ts = make_tiles_t(a.g, xc, TmaF64::TZ, TmaF64::TY);
   int rc = coef_components(a, 8, &t->ncoef);
   if (rc != SW_OK) return rc;
@@ -880,7 +881,7 @@ int launch_steps_tma(const StepArgs& a, int xchunk, int it0, int nsteps, cudaStr
     rc = make_tma_f64(a, xchunk, &t);
     if (rc != SW_OK) return rc;
     if (t.ts.count == 0) return SW_OK;
-    const int grid = std::min(t.ts.count, step_slots());
+    const int grid = std::min(t.ts.count, step_slots(false));
     int done = 0;
     rc = graph_loop(reinterpret_cast<void*>(step_f64_tma<false>), t, grid, TmaF64::THREADS, smem,
                     1, 32, a.clock, it0, nsteps, s, &done);
@@ -944,7 +945,7 @@ int launch_steps_tma_batch(int precision, const void* d_tab, int ninst, int ntil
   if (rc != SW_OK) return rc;
   if (ntiles == 0) return SW_OK;
   const size_t smem = tma_smem_bytes(precision);
-  const int grid = std::min(ntiles, step_slots());
+  const int grid = std::min(ntiles, step_slots(precision != SW_PLAIN_F64));
   if (precision == SW_PLAIN_F64) {
     TmaF64 dummy{};
     step_f64_tma<true><<<grid, TmaF64::THREADS, smem, s>>>(dummy, (const TmaF64*)d_tab, ninst,
@@ -980,13 +981,14 @@ static std::vector<int> batch_order(const sw_fdtd_desc* descs, const std::vector
 // Target planes per x chunk for a batched launch: about
 // SW_TUNE_BATCH_TILES_PER_CTA (8) tiles per resident CTA over all running
 // solves, at least 8 planes (each chunk re-reads two halo planes).
-static int batch_xchunk(const sw_fdtd_desc* descs, const std::vector<int>& run, int tz, int ty) {
+static int batch_xchunk(const sw_fdtd_desc* descs, const std::vector<int>& run, int tz, int ty,
+                        bool mixed) {
   long long work = 0;
   for (int i : run) {
     const long long cols = (long long)((descs[i].nz + tz - 1) / tz) * ((descs[i].ny + ty - 1) / ty);
     work += cols * std::max(0, descs[i].nx - 2);
   }
-  const long long want = (long long)tune_get(SW_TUNE_BATCH_TILES_PER_CTA) * step_slots();
+  const long long want = (long long)tune_get(SW_TUNE_BATCH_TILES_PER_CTA) * step_slots(mixed);
   return (int)std::max<long long>(8, (work + want - 1) / want);
 }
 
@@ -1043,7 +1045,7 @@ int build_batch(const sw_fdtd_desc* descs, const int32_t* begins, int n, int it,
     if (lit >= 0 && lit < descs[i].n_steps) run.push_back(i);
   }
   const int shape = std::is_same<Inst, TmaF32>::value ? batch_tile_width(descs, run) : 0;
-  const int xc = batch_xchunk(descs, run, Inst::TZ, Inst::TY);
+  const int xc = batch_xchunk(descs, run, Inst::TZ, Inst::TY, std::is_same<Inst, TmaF32>::value);
   int nt = 0;
   for (int i : batch_order(descs, run)) {
     StepArgs a;

@@ -11,25 +11,30 @@ namespace sw {
 constexpr int round128(int bytes) { return (bytes + 127) / 128 * 128; }
 
 // Kernel-side view of one mixed-form solve (state after t steps in buffer t mod 3).
-// The output tile is tzw x tyh cells of the (z, y) plane, 64 x 8 or 32 x 16
-// (per solve, whichever wastes fewer lanes on its grid); both shapes give
-// boxes of the same byte sizes.
+// The output tile is tzw x tyh cells of the (z, y) plane: 64 x TY or
+// 32 x 2TY (per launch, whichever wastes fewer lanes on the grids); a CTA
+// has TY consumer warps, one tile row of 32 z pairs each (64-wide) or two
+// rows of 16 (32-wide).
 //   tm[b]  : state buffer b as a 4-D tensor (pz, ny, nx, 9 components);
 //            box (tzw + 8, tyh + 2, 1, 6) = the halo'd u and d of one plane
 //   tmc[b] : the same tensor, box (tzw, tyh, 1, 3) = the Kahan compensation
 //   tmm    : material coefficients (pz, ny, nx, ncoef), box (tzw, tyh, 1, ncoef)
+constexpr int kF32TileRows = 8;  // TY: rows of a 64-wide tile = consumer warps
+// halo-box cells per component of a mixed-step tile of width tzw
+constexpr int f32_box_cells(int tzw) { return (tzw + 8) * (64 * kF32TileRows / tzw + 2); }
+
 struct TmaF32 {
-  static constexpr int TZ = 64, TY = 8;  // the 64 x 8 shape; tzw * tyh == TZ * TY always
-  static constexpr int W = TZ + 8;       // halo box width: 4 cells each side in z
-  static constexpr int H = TY + 2;       // halo box height: 1 row each side in y
-  static_assert((32 + 8) * (16 + 2) == W * H, "the 32 x 16 box must match the 64 x 8 box");
-  static constexpr int A_BYTES = W * H * 6 * 4;
-  static constexpr int C_BYTES = TZ * TY * 3 * 4;
-  static constexpr int M_BYTES = TZ * TY * 2 * 4;
-  static constexpr int A_STAGE = round128(A_BYTES);
-  static constexpr int B_STAGE = round128(C_BYTES) + round128(M_BYTES);
+  static constexpr int TZ = 64, TY = kF32TileRows;  // the 64-wide shape; tzw * tyh == TZ * TY
+  static constexpr int PT = TZ * TY;                // cells of a point box (per component)
+  static constexpr int box_cells(int tzw) { return f32_box_cells(tzw); }
+  static constexpr int A_BYTES_MAX =
+      (f32_box_cells(64) > f32_box_cells(32) ? f32_box_cells(64) : f32_box_cells(32)) * 6 * 4;
+  static constexpr int C_BYTES = PT * 3 * 4;
+  static constexpr int M_BYTES = PT * 2 * 4;
+  static constexpr int A_STAGE = round128(A_BYTES_MAX);
   static constexpr int CONSUMER_WARPS = TY;
   static constexpr int THREADS = 32 * (CONSUMER_WARPS + 1);
+  static constexpr int MIN_CTAS = TY <= 8 ? 2 : 1;  // resident CTAs per SM the layout allows
   CUtensorMap tm[3];
   CUtensorMap tmc[3];
   CUtensorMap tmm;
@@ -43,7 +48,7 @@ struct TmaF32 {
   float hx, hy, hz, damp;
   int ncoef;  // 1: mu only, 2: mu and eta
   int use_damp, kahan, n_steps, snap_stride;
-  int tzw, tyh;   // output tile shape: 64 x 8 or 32 x 16
+  int tzw, tyh;   // output tile shape: 64 x TY or 32 x 2 TY
   float* snaps;
   int* flags;
   int it_begin;   // launch step index of this solve's step 0
@@ -57,7 +62,7 @@ struct TmaF64 {
   static constexpr int TZ = 32, TY = 8;
   static constexpr int W = TZ + 4;  // 2 cells of halo each side in z (16-byte aligned)
   static constexpr int H = TY + 2;
-  static constexpr int NA = 4, NB = 3;
+  static constexpr int NA = 5, NB = 3;  // planes x, x+1 held, three in flight
   static constexpr int BOX_BYTES = W * H * 3 * 8;        // one buffer's box
   static constexpr int HALF = round128(BOX_BYTES);        // u_prev box, then u_curr box
   static constexpr int A_STAGE = 2 * HALF;

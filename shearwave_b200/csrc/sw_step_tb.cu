@@ -1,31 +1,38 @@
-// Mixed-form step kernel that advances two time steps per pass over HBM.
+// Mixed-form step kernel that advances two time steps per pass over HBM
+// (opts steps_per_pass=2; runs without the compensated sum).
 //
 // Same per-cell update as the one-step kernels (src/shearwave/solver.py:
-// 195-226 in increment form with a compensated displacement), applied twice:
+// 195-226 in increment form), applied twice in one pass:
 //
-//   level 0  the state at step t, streamed by TMA: u and d of a plane with two
-//            cells of halo around the 62 x 6 output tile (one 72 x 10 x 1 x 6
-//            box per plane, 6-stage ring: three planes in use, three in
-//            flight), and the point-wise data of the 64 x 8 level-1 region
-//            (Kahan c, material coefficients; 4-stage ring);
-//   level 1  step t+1 on the 64 x 8 region (the output tile plus one cell of
-//            halo), written to a 4-slot shared-memory ring of planes;
+//   level 0  the state at step t, streamed by TMA: u and d of a plane around
+//            the 60 x 13 output tile (one 68 x 17 x 1 x 6 box per plane;
+//            4-stage ring: planes q and q+1 held, two in flight) and the
+//            material coefficients of the 64 x 15 level-1 region (3 stages);
+//   level 1  step t+1 on the 64 x 15 region (the tile, one cell of halo, one
+//            more column each side in z so z pairs stay aligned), written to
+//            a 3-slot shared-memory ring of planes;
 //   level 2  step t+2 on the output tile, read from the level-1 ring and
 //            written to global memory.
 //
 // The CTA marches along x: when level-0 plane q+1 lands, level 1 computes
-// plane q and level 2 plane q-1.  Level-1 cells outside the grid interior
-// are the zero shell.  Each consumer thread owns the same two columns at
-// both levels, so the level-1 Kahan compensation and the material
-// coefficients carry over in registers.  One named barrier per plane (with
-// an or-reduction of the failure flag, so an abort is decided by all
-// consumers together) separates the level-1 writes from the level-2 reads;
-// four level-1 slots make a second barrier unnecessary.  A step reads the
-// state in buffer t mod 3 and writes buffer (t+2) mod 3.
+// plane q and level 2 plane q-1.  Fifteen consumer warps each own one
+// level-1 row of 32 z pairs (8-byte shared loads and stores for both cells)
+// and the same pairs at level 2, so the coefficients carry over in
+// registers; the x neighbours at x-1 of both levels come from registers too
+// (the centre values of the plane computed before), which frees a level-0
+// stage as soon as level 1 has used it.  The level-1 ring has a full and an
+// empty mbarrier per slot (one arrival per warp): level 2 of plane q-1 waits
+// until every warp has written plane q-1 (it reads the rows above and
+// below), and level 1 reuses a slot once every warp has read it, so warps
+// drift up to a plane apart instead of meeting at a barrier; every wait is
+// bounded and an abort stops each warp on its own.  Level-1 cells outside
+// the grid interior are the zero shell.  Both levels use lap7f, so
+// two steps here equal two one-step launches bit for bit.  A pass reads
+// buffer t mod 3 and writes buffer (t+2) mod 3.
 //
-// Per output cell and pair of steps the kernel moves about 78 bytes of DRAM
-// traffic (u, d, c in and out, coefficients once) instead of 160 for two
-// one-step passes.
+// Per output cell and pair of steps it moves about 35 bytes of DRAM traffic
+// per step (u, d in and out once per two steps, coefficients, halos),
+// against 66 for one-step launches.
 #include <math.h>
 
 #include <algorithm>
@@ -40,15 +47,15 @@ namespace sw {
 namespace {
 
 struct TbCoord {
-  int z_start, y_start, x0, x1;
+  int z0, y0, x0, x1;  // output tile: z in [z0, z0+OZ), y in [y0, y0+OY), x in [x0, x1)
 };
 
 __host__ __device__ inline TileSpace make_tiles_tb(const Geom& g, int xc) {
   TileSpace t;
-  const int nzi = g.nz > 2 ? g.nz - 2 : 0, nyi = g.ny > 2 ? g.ny - 2 : 0;
+  // tiles [60 k, 60 k + 60) and [13 k, 13 k + 13) cover the interior 1..n-2
+  t.ntz = g.nz > 2 ? (g.nz - 2) / TmaF32TB::OZ + 1 : 0;
+  t.nty = g.ny > 2 ? (g.ny - 2) / TmaF32TB::OY + 1 : 0;
   const int nxi = g.nx > 2 ? g.nx - 2 : 0;
-  t.ntz = (nzi + TmaF32TB::OZ - 1) / TmaF32TB::OZ;
-  t.nty = (nyi + TmaF32TB::OY - 1) / TmaF32TB::OY;
   t.xc = xc < 1 ? 1 : xc;
   t.nxc = nxi > 0 ? (nxi + t.xc - 1) / t.xc : 0;
   t.count = t.ntz * t.nty * t.nxc;
@@ -61,26 +68,88 @@ __device__ inline TbCoord tb_coord(const Geom& g, const TileSpace& t, int local)
   const int rest = local / t.ntz;
   const int yt = rest % t.nty;
   const int xt = rest / t.nty;
-  c.z_start = 1 + TmaF32TB::OZ * zt;
-  c.y_start = 1 + TmaF32TB::OY * yt;
+  c.z0 = TmaF32TB::OZ * zt;
+  c.y0 = TmaF32TB::OY * yt;
   c.x0 = 1 + xt * t.xc;
   c.x1 = min(c.x0 + t.xc, g.nx - 1);
   return c;
 }
 
-__device__ inline int floor4(int v) { return v & ~3; }  // floor to a multiple of 4 (v >= -4)
+__device__ __forceinline__ float2 tb_ld2(const float* p) {
+  return *reinterpret_cast<const float2*>(p);
+}
+__device__ __forceinline__ void tb_st2(float* p, float a, float b) {
+  *reinterpret_cast<float2*>(p) = make_float2(a, b);
+}
+
+// One level of the two-step pass for one thread's z pair: the step from the
+// plane whose centre pair is at `P + o` (row stride `RS`, component stride
+// `CS`), with the plane after it at `Pn` and the centre values of the plane
+// before it in (pu, pd).  Writes the new u and the increment of each
+// component to `out + c * ocs` and `out + (3 + c) * ocs` (inactive cells:
+// 0) and, when `snap` is set, the new u of active cells to snap[3 c'] of the
+// AoS snapshot.  (pu, pd) become this plane's centres.
+template <bool VISC, int RS, int CS>
+__device__ __forceinline__ void tb_pair_step(const float* __restrict__ P,
+                                             const float* __restrict__ Pn, int o, float2 M,
+                                             float2 E, float2 (&pu)[3], float2 (&pd)[3],
+                                             bool act_a, bool act_b, float hx, float hy, float hz,
+                                             float hc, bool use_damp, float damp,
+                                             const TmaF32TB* __restrict__ in, int j0, int j1,
+                                             long long nc, long long i, float* __restrict__ out,
+                                             long long ocs, float* __restrict__ snap) {
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const int oc = o + c * CS, od = oc + 3 * CS;
+    const float2 C = tb_ld2(P + oc), L = tb_ld2(P + oc - 2), R = tb_ld2(P + oc + 2);
+    const float2 N = tb_ld2(P + oc + RS), S = tb_ld2(P + oc - RS), X = tb_ld2(Pn + oc);
+    const float lua = lap7f(X.x + pu[c].x, N.x + S.x, C.y + L.y, C.x, hx, hy, hz, hc);
+    const float lub = lap7f(X.y + pu[c].y, N.y + S.y, R.x + C.x, C.y, hx, hy, hz, hc);
+    const float2 Cd = tb_ld2(P + od);
+    float inca = Cd.x + M.x * lua, incb = Cd.y + M.y * lub;
+    if (VISC) {
+      const float2 Ld = tb_ld2(P + od - 2), Rd = tb_ld2(P + od + 2);
+      const float2 Nd = tb_ld2(P + od + RS), Sd = tb_ld2(P + od - RS), Xd = tb_ld2(Pn + od);
+      const float lda = lap7f(Xd.x + pd[c].x, Nd.x + Sd.x, Cd.y + Ld.y, Cd.x, hx, hy, hz, hc);
+      const float ldb = lap7f(Xd.y + pd[c].y, Nd.y + Sd.y, Rd.x + Cd.x, Cd.y, hx, hy, hz, hc);
+      inca += E.x * lda;
+      incb += E.y * ldb;
+    }
+    pu[c] = C;
+    pd[c] = Cd;
+    for (int j = j0; j < j1; ++j) {  // push steps only
+      const float2 Pt = __ldg(reinterpret_cast<const float2*>(
+          in->pat + ((long long)in->term_pat[j] * 3 + c) * nc + i));
+      const float sc = (float)in->term_scale[j];
+      inca += Pt.x * sc;
+      incb += Pt.y * sc;
+    }
+    if (use_damp) {
+      inca *= damp;
+      incb *= damp;
+    }
+    const float ua = C.x + inca, ub = C.y + incb;
+    tb_st2(out + c * ocs, act_a ? ua : 0.f, act_b ? ub : 0.f);
+    tb_st2(out + (3 + c) * ocs, act_a ? inca : 0.f, act_b ? incb : 0.f);
+    if (snap != nullptr) {
+      if (act_a) snap[c] = ua;
+      if (act_b) snap[3 + c] = ub;
+    }
+  }
+}
 
 template <bool BATCH>
 __global__ void __launch_bounds__(TmaF32TB::THREADS, 1)
     step_f32_fused2(const __grid_constant__ TmaF32TB one, const TmaF32TB* __restrict__ tab,
-                    int ninst, int ntiles, int it, const int* __restrict__ it_dev,
-                    int* /*queues: unused; keeps the step kernels' parameters alike*/) {
+                    int ninst, int ntiles, int it, const int* __restrict__ it_dev, int* queues) {
   if (it_dev != nullptr) it += *it_dev;  // step counter kept on the device (graph replays)
+  // batched launches take tiles from a launch-wide queue (see step_f32_tma)
+  int* queue = (BATCH && queues != nullptr) ? queues : nullptr;
   using T = TmaF32TB;
   constexpr int NA = T::NA, NB = T::NB, NL = T::NL, W = T::W, H = T::H, WB = T::WB, HB = T::HB;
   constexpr int LZ = T::LZ, LY = T::LY, NC = T::CONSUMER_WARPS * 32;
   constexpr int AF = T::A_STAGE / 4, BF = T::B_STAGE / 4, LF = T::L_STAGE / 4;
-  constexpr int CF = round128(T::C_BYTES) / 4;
+  constexpr int LP = LZ * LY;  // level-1 cells per component
   extern __shared__ unsigned char smem_raw[];
   unsigned char* base = smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u);
   WsHeader* hd = reinterpret_cast<WsHeader*>(base);
@@ -88,10 +157,13 @@ __global__ void __launch_bounds__(TmaF32TB::THREADS, 1)
   float* ringA = reinterpret_cast<float*>(base + kRingOffset);
   float* ringB = ringA + NA * AF;
   float* ringL = ringB + NB * BF;
+  uint64_t* Lfull = reinterpret_cast<uint64_t*>(ringL + NL * LF);  // after the rings
+  uint64_t* Lempty = Lfull + NL;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if ((smem_addr(ringA) & 127u) != 0u) {
     int* fl = BATCH ? (ninst > 0 ? tab[0].flags : nullptr) : one.flags;
     if (threadIdx.x == 0 && fl) atomicOr(fl, 4);
+    queue_cta_done(queue);
     return;
   }
   if (threadIdx.x == 0) {
@@ -103,6 +175,10 @@ __global__ void __launch_bounds__(TmaF32TB::THREADS, 1)
       mbar_init(&hd->fullB[s], 1);
       mbar_init(&hd->emptyB[s], T::CONSUMER_WARPS);
     }
+    for (int s = 0; s < NL; ++s) {
+      mbar_init(&Lfull[s], T::CONSUMER_WARPS);
+      mbar_init(&Lempty[s], T::CONSUMER_WARPS);
+    }
     *abort_flag = 0;
     mbar_fence_init();
   }
@@ -111,38 +187,53 @@ __global__ void __launch_bounds__(TmaF32TB::THREADS, 1)
   if (warp == T::CONSUMER_WARPS) {
     // ------------------------------- producer -----------------------------
     if (lane == 0) {
-      uint32_t pa = 0, pb = 0;
-      for (int t = blockIdx.x; t < ntiles && !*abort_flag; t += gridDim.x) {
-        const T* in;
-        int local, lit;
-        if (!resolve_tile<T, BATCH>(one, tab, ninst, t, it, in, local, lit)) continue;
+      RingPos<NA> pa;
+      RingPos<NB> pb;
+      int stride_next = blockIdx.x;
+      bool ok = true;
+      while (ok && !*abort_flag) {
+        const int t = next_tile(queue, stride_next);
+        if (t >= ntiles) {  // end of this CTA's work: arm one stage without a copy
+          if (!ws_wait(&hd->emptyA[pa.s], pa.ph ^ 1u, abort_flag)) break;
+          tile_slots(base)[pa.s] = -1;
+          mbar_arrive(&hd->fullA[pa.s]);
+          pa.next();
+          break;
+        }
+        const int k = BATCH ? find_solve(tab, ninst, t) : 0;
+        const T* in = BATCH ? &tab[k] : &one;
+        const int local = BATCH ? t - in->tile_base : t;
+        const int lit = it - in->it_begin;
+        if (lit < 0 || lit + 1 >= in->n_steps) continue;
         const Geom& g = in->g;
         const TbCoord tc = tb_coord(g, in->ts, local);
-        const int zA0 = floor4(tc.z_start - 2), zB0 = floor4(tc.z_start - 1);
         const CUtensorMap* tma = &in->tm[lit % 3];
-        const CUtensorMap* tmc = &in->tmc[lit % 3];
-        const uint32_t bbytes = (in->kahan ? T::C_BYTES : 0) + WB * HB * 4 * in->ncoef;
-        bool ok = true;
+        const uint32_t bbytes = WB * HB * 4 * in->ncoef;
+        bool first = true;
         auto issueA = [&](int p) {
-          const int sa = pa % NA;
-          ok = ok && ws_wait(&hd->emptyA[sa], ((pa / NA) & 1u) ^ 1u, abort_flag);
+          const int sa = pa.s;
+          ok = ok && ws_wait(&hd->emptyA[sa], pa.ph ^ 1u, abort_flag);
           if (!ok) return;
-          const int pl = min(max(p, 0), g.nx - 1);  // planes outside the grid are never read
+          if (first) {
+            tile_slots(base)[sa] = t;
+            solve_slots(base)[sa] = k;
+            first = false;
+          }
+          const int pl = min(max(p, 0), g.nx - 1);  // planes outside the grid feed only the shell
           fence_proxy_async_smem();
           mbar_arrive_expect_tx(&hd->fullA[sa], T::A_BYTES);
-          tma_load_4d(ringA + sa * AF, tma, &hd->fullA[sa], zA0, tc.y_start - 2, pl, 0);
-          ++pa;
+          tma_load_4d(ringA + sa * AF, tma, &hd->fullA[sa], tc.z0 - 4, tc.y0 - 2, pl, 0);
+          pa.next();
         };
         auto issueB = [&](int q) {
-          const int sb = pb % NB;
-          ok = ok && ws_wait(&hd->emptyB[sb], ((pb / NB) & 1u) ^ 1u, abort_flag);
+          const int sb = pb.s;
+          ok = ok && ws_wait(&hd->emptyB[sb], pb.ph ^ 1u, abort_flag);
           if (!ok) return;
           const int ql = min(max(q, 0), g.nx - 1);
           fence_proxy_async_smem();
           mbar_arrive_expect_tx(&hd->fullB[sb], bbytes);
-          if (in->kahan) tma_load_4d(ringB + sb * BF, tmc, &hd->fullB[sb], zB0, tc.y_start - 1, ql, 6);
-          tma_load_4d(ringB + sb * BF + CF, &in->tmm, &hd->fullB[sb], zB0, tc.y_start - 1, ql, 0);
-          ++pb;
+          tma_load_4d(ringB + sb * BF, &in->tmm, &hd->fullB[sb], tc.z0 - 4, tc.y0 - 1, ql, 0);
+          pb.next();
         };
         issueA(tc.x0 - 2);
         issueA(tc.x0 - 1);
@@ -150,195 +241,148 @@ __global__ void __launch_bounds__(TmaF32TB::THREADS, 1)
           issueA(q + 1);
           issueB(q);
         }
-        if (!ok) break;
       }
     }
   } else {
     // ------------------------------- consumers ----------------------------
     const int w = warp;
-    uint32_t ca = 0, cb = 0, lcount = 0;
-    bool failed = false;
-    for (int t = blockIdx.x; t < ntiles && !failed; t += gridDim.x) {
-      const T* in;
-      int local, lit;
-      if (!resolve_tile<T, BATCH>(one, tab, ninst, t, it, in, local, lit)) continue;
-      const Geom& g = in->g;  // hot switches in registers (see step_f32_tma)
+    RingPos<NA> ca;  // next level-0 plane to consume
+    RingPos<NB> cb;  // next point plane
+    RingPos<NL> lw;  // slot of the next level-1 plane
+    while (true) {
+      // the tile's first plane, x0-2: centres only
+      if (!ws_wait(&hd->fullA[ca.s], ca.ph, abort_flag)) break;
+      const int t = tile_slots(base)[ca.s];
+      if (t < 0) break;
+      const T* in = BATCH ? &tab[solve_slots(base)[ca.s]] : &one;
+      const int local = BATCH ? t - in->tile_base : t;
+      const int lit = it - in->it_begin;
+      const Geom& g = in->g;
       const TbCoord tc = tb_coord(g, in->ts, local);
-      const bool use_damp = in->use_damp != 0;
-      const float damp = in->damp;
-      const int zA0 = floor4(tc.z_start - 2), zB0 = floor4(tc.z_start - 1);
-      const int offA = tc.z_start - 1 - zA0;  // level-1 column 0 in the level-0 box
-      const int offB = tc.z_start - 1 - zB0;  // level-1 column 0 in the point box
       float* __restrict__ D = in->state[(lit + 2) % 3];
       const long long nc = g.ncell;
-      const int y = tc.y_start - 1 + w;  // this warp's level-1 row
-      const bool yin = (y >= 1 && y <= g.ny - 2);
-      int zc[2];
-      bool inyz[2], own[2];
-#pragma unroll
-      for (int k = 0; k < 2; ++k) {
-        const int c = lane + 32 * k;
-        zc[k] = tc.z_start - 1 + c;
-        inyz[k] = yin && zc[k] >= 1 && zc[k] <= g.nz - 2;
-        own[k] = inyz[k] && w >= 1 && w <= T::OY && c >= 1 && c <= T::OZ;
-      }
-      const int ja0 = in->term_off ? in->term_off[lit] : 0;
-      const int ja1 = in->term_off ? in->term_off[lit + 1] : 0;
-      const int jb0 = in->term_off ? in->term_off[lit + 1] : 0;
-      const int jb1 = in->term_off ? in->term_off[lit + 2] : 0;
+      const bool use_damp = in->use_damp != 0, visc = in->ncoef > 1;
+      const float damp = in->damp;
+      const float hx = in->hx, hy = in->hy, hz = in->hz, hc = lap7_centre_coef(hx, hy, hz);
+      // this thread: level-1 row w (y = y0-1+w), z pair zp, zp+1 (zp = z0-2+2 lane)
+      const int y = tc.y0 - 1 + w, zp = tc.z0 - 2 + 2 * lane;
+      const bool yin = y >= 1 && y <= g.ny - 2;
+      const bool zin_a = zp >= 1 && zp <= g.nz - 2, zin_b = zp + 1 >= 1 && zp + 1 <= g.nz - 2;
+      // level 2: rows 1..OY and pairs 1..30 are the output tile
+      const bool out_rc = w >= 1 && w <= T::OY && lane >= 1 && lane <= 30;
+      const bool store = out_rc && yin && zp < g.pz;  // pz is even: the pair is in the row
+      const int o = (w + 1) * W + 2 + 2 * lane, ob = w * WB + 2 + 2 * lane, ol = w * LZ + 2 * lane;
+      const int j10 = in->term_off ? in->term_off[lit] : 0;
+      const int j11 = in->term_off ? in->term_off[lit + 1] : 0;
+      const int j20 = j11;
+      const int j21 = in->term_off ? in->term_off[lit + 2] : 0;
       const bool snap1 =
           in->snap_stride > 0 && in->snaps != nullptr && ((lit + 1) % in->snap_stride) == 0;
       const bool snap2 =
           in->snap_stride > 0 && in->snaps != nullptr && ((lit + 2) % in->snap_stride) == 0;
       const int slot1 = snap1 ? (lit + 1) / in->snap_stride - 1 : 0;
       const int slot2 = snap2 ? (lit + 2) / in->snap_stride - 1 : 0;
-      const bool visc = in->ncoef > 1, kahan = in->kahan != 0;
-      const float hx = in->hx, hy = in->hy, hz = in->hz, hc = lap7_centre_coef(hx, hy, hz);
-      float mp[2] = {0.f, 0.f}, ep[2] = {0.f, 0.f}, cp[2][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
-      bool ok = true;
-      int s_prev = ca % NA;
-      ok = ok && ws_wait(&hd->fullA[s_prev], (ca / NA) & 1u, abort_flag);
-      ++ca;
-      int s_cur = ca % NA;
-      ok = ok && ws_wait(&hd->fullA[s_cur], (ca / NA) & 1u, abort_flag);
-      ++ca;
-      for (int q = tc.x0 - 1; q <= tc.x1; ++q) {
-        const int s_next = ca % NA;
-        ok = ok && ws_wait(&hd->fullA[s_next], (ca / NA) & 1u, abort_flag);
-        ++ca;
-        const int sb = cb % NB;
-        ok = ok && ws_wait(&hd->fullB[sb], (cb / NB) & 1u, abort_flag);
-        ++cb;
-        // ---- level 1: step lit+1 at plane q on the 64 x 8 region ----
-        float* Lw = ringL + (lcount % NL) * LF;
-        float mc[2] = {0.f, 0.f}, ec[2] = {0.f, 0.f}, cc[2][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
-        if (ok) {
-          const float* Pp = ringA + s_prev * AF;
-          const float* Pc = ringA + s_cur * AF;
-          const float* Pn = ringA + s_next * AF;
-          const float* Bc = ringB + sb * BF;
-          const float* Bm = Bc + CF;
-          const bool qin = (q >= 1 && q <= g.nx - 2);
-          bool bad = false;
+      float2 pu[3], pd[3];  // level-0 centres of the plane before
+      float2 qu[3], qd[3];  // level-1 centres of the plane before
+      float2 Mp = make_float2(0.f, 0.f), Ep = Mp;  // coefficients of the previous plane
+      {
+        const float* P0 = ringA + ca.s * AF;
 #pragma unroll
-          for (int k = 0; k < 2; ++k) {
-            const int c = lane + 32 * k;
-            const int ob = w * WB + c + offB;
-            mc[k] = Bm[ob];
-            ec[k] = visc ? Bm[HB * WB + ob] : 0.0f;
-            const bool act = qin && inyz[k];
-            const long long i = (long long)q * g.sxy + (long long)y * g.pz + zc[k];
-#pragma unroll
-            for (int comp = 0; comp < 3; ++comp) {
-              float unew = 0.f, inc = 0.f, cnew = 0.f;
-              if (act) {
-                const int o = (comp * H + w + 1) * W + c + offA;
-                const int od = o + 3 * H * W;
-                const float u0 = Pc[o], d0 = Pc[od];
-                const float lu = lap7f(Pn[o] + Pp[o], Pc[o + W] + Pc[o - W],
-                                       Pc[o + 1] + Pc[o - 1], u0, hx, hy, hz, hc);
-                inc = d0 + mc[k] * lu;
-                if (visc) {
-                  const float ld = lap7f(Pn[od] + Pp[od], Pc[od + W] + Pc[od - W],
-                                         Pc[od + 1] + Pc[od - 1], d0, hx, hy, hz, hc);
-                  inc += ec[k] * ld;
-                }
-                for (int j = ja0; j < ja1; ++j)
-                  inc += in->pat[((long long)in->term_pat[j] * 3 + comp) * nc + i] *
-                         (float)in->term_scale[j];
-                if (use_damp) inc *= damp;
-                if (kahan) {
-                  const float c0 = Bc[comp * HB * WB + ob];
-                  const float yk = inc - c0;
-                  unew = u0 + yk;
-                  cnew = (unew - u0) - yk;
-                } else {
-                  unew = u0 + inc;
-                }
-                bad |= !isfinite(unew);
-                if (snap1 && own[k] && q >= tc.x0 && q < tc.x1)
-                  in->snaps[((((long long)slot1 * g.nx + q) * g.ny + y) * g.nz + zc[k]) * 3 +
-                            comp] = unew;
-              }
-              Lw[(comp * LY + w) * LZ + c] = unew;
-              Lw[((3 + comp) * LY + w) * LZ + c] = inc;
-              cc[k][comp] = cnew;
-            }
-          }
-          if (bad && in->flags) atomicOr(in->flags, 1);
+        for (int c = 0; c < 3; ++c) {
+          pu[c] = tb_ld2(P0 + o + c * H * W);
+          pd[c] = tb_ld2(P0 + o + (3 + c) * H * W);
+          qu[c] = qd[c] = make_float2(0.f, 0.f);
+        }
+      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&hd->emptyA[ca.s]);
+      ca.next();
+      RingPos<NA> cur = ca;  // plane q
+      bool ok = ws_wait(&hd->fullA[cur.s], cur.ph, abort_flag);
+      ca.next();
+      RingPos<NL> lprev = lw;  // slot of level-1 plane q-1 (meaningful from q = x0)
+      for (int q = tc.x0 - 1; q <= tc.x1 && ok; ++q) {
+        const RingPos<NA> nxt = ca;  // plane q+1
+        ok = ok && ws_wait(&hd->fullA[nxt.s], nxt.ph, abort_flag);
+        ca.next();
+        const RingPos<NB> pt = cb;
+        ok = ok && ws_wait(&hd->fullB[pt.s], pt.ph, abort_flag);
+        cb.next();
+        // the slot is free once every warp has read what it held before
+        ok = ok && ws_wait(&Lempty[lw.s], lw.ph ^ 1u, abort_flag);
+        if (!ok) break;
+        float* Lw = ringL + lw.s * LF;
+        // ---- level 1: step lit+1 at plane q on the level-1 region ----
+        const float* Bm = ringB + pt.s * BF;
+        const float2 Mc = tb_ld2(Bm + ob);
+        const float2 Ec = visc ? tb_ld2(Bm + HB * WB + ob) : make_float2(0.f, 0.f);
+        {
+          const float* Pc = ringA + cur.s * AF;
+          const float* Pn = ringA + nxt.s * AF;
+          const bool xin = q >= 1 && q <= g.nx - 2;
+          const bool aa = xin && yin && zin_a, ab = xin && yin && zin_b;
+          const long long i = (long long)min(max(q, 0), g.nx - 1) * g.sxy +
+                              (long long)min(max(y, 0), g.ny - 1) * g.pz + max(zp, 0);
+          const int jl0 = (aa || ab) ? j10 : 0, jl1 = (aa || ab) ? j11 : 0;
+          float* sp = (snap1 && store && q >= tc.x0 && q < tc.x1)
+                          ? in->snaps + ((((long long)slot1 * g.nx + q) * g.ny + y) * g.nz + zp) * 3
+                          : nullptr;
+          if (visc)
+            tb_pair_step<true, W, H * W>(Pc, Pn, o, Mc, Ec, pu, pd, aa, ab, hx, hy, hz, hc,
+                                         use_damp, damp, in, jl0, jl1, nc, i, Lw + ol, LP, sp);
+          else
+            tb_pair_step<false, W, H * W>(Pc, Pn, o, Mc, Ec, pu, pd, aa, ab, hx, hy, hz, hc,
+                                          use_damp, damp, in, jl0, jl1, nc, i, Lw + ol, LP, sp);
         }
         __syncwarp();
-        if (lane == 0 && ok) {
-          mbar_arrive(&hd->emptyA[s_prev]);  // level-0 plane q-1 is no longer needed
-          mbar_arrive(&hd->emptyB[sb]);
+        if (lane == 0) {
+          mbar_arrive(&hd->emptyA[cur.s]);  // level-0 plane q is no longer needed
+          mbar_arrive(&hd->emptyB[pt.s]);
+          mbar_arrive(&Lfull[lw.s]);        // this warp's row of level-1 plane q is written
         }
-        ++lcount;
-        if (consumer_sync_or(!ok, NC)) {  // level-1 plane q visible to all consumers
-          failed = true;
-          break;
-        }
-        // ---- level 2: step lit+2 at plane x = q-1 on the output tile ----
-        const int x = q - 1;
-        if (x >= tc.x0) {
-          const float* Lp = ringL + ((lcount - 3) % NL) * LF;
-          const float* Lc = ringL + ((lcount - 2) % NL) * LF;
-          const float* Ln = ringL + ((lcount - 1) % NL) * LF;
-          bool bad = false;
+        if (q >= tc.x0) {
+          const float* Lc = ringL + lprev.s * LF;  // level-1 plane q-1
+          if (q == tc.x0) {  // level-1 centres of plane x0-1 (own pair) for the first level 2
 #pragma unroll
-          for (int k = 0; k < 2; ++k) {
-            if (!own[k]) continue;
-            const int c = lane + 32 * k;
-            const long long i = (long long)x * g.sxy + (long long)y * g.pz + zc[k];
-#pragma unroll
-            for (int comp = 0; comp < 3; ++comp) {
-              const int o = (comp * LY + w) * LZ + c;
-              const int od = o + 3 * LY * LZ;
-              const float u0 = Lc[o], d0 = Lc[od];
-              const float lu = lap7f(Ln[o] + Lp[o], Lc[o + LZ] + Lc[o - LZ],
-                                     Lc[o + 1] + Lc[o - 1], u0, hx, hy, hz, hc);
-              float inc = d0 + mp[k] * lu;
-              if (visc) {
-                const float ld = lap7f(Ln[od] + Lp[od], Lc[od + LZ] + Lc[od - LZ],
-                                       Lc[od + 1] + Lc[od - 1], d0, hx, hy, hz, hc);
-                inc += ep[k] * ld;
-              }
-              for (int j = jb0; j < jb1; ++j)
-                inc += in->pat[((long long)in->term_pat[j] * 3 + comp) * nc + i] *
-                       (float)in->term_scale[j];
-              if (use_damp) inc *= damp;
-              float unew;
-              if (kahan) {
-                const float yk = inc - cp[k][comp];
-                unew = u0 + yk;
-                D[(6 + comp) * nc + i] = (unew - u0) - yk;
-              } else {
-                unew = u0 + inc;  // compensation planes unused
-              }
-              D[comp * nc + i] = unew;
-              D[(3 + comp) * nc + i] = inc;
-              bad |= !isfinite(unew);
-              if (snap2)
-                in->snaps[((((long long)slot2 * g.nx + x) * g.ny + y) * g.nz + zc[k]) * 3 +
-                          comp] = unew;
+            for (int c = 0; c < 3; ++c) {
+              qu[c] = tb_ld2(Lc + ol + c * LP);
+              qd[c] = tb_ld2(Lc + ol + (3 + c) * LP);
+            }
+          } else {
+            // ---- level 2: step lit+2 at plane x = q-1 on the output tile ----
+            // (reads rows w-1..w+1 of plane q-1: wait until every warp wrote it)
+            ok = ws_wait(&Lfull[lprev.s], lprev.ph, abort_flag);
+            if (!ok) break;
+            if (store) {
+              const int x = q - 1;
+              const long long i = (long long)x * g.sxy + (long long)y * g.pz + zp;
+              float* sp =
+                  snap2 ? in->snaps + ((((long long)slot2 * g.nx + x) * g.ny + y) * g.nz + zp) * 3
+                        : nullptr;
+              if (visc)
+                tb_pair_step<true, LZ, LP>(Lc, Lw, ol, Mp, Ep, qu, qd, zin_a, zin_b, hx, hy, hz,
+                                           hc, use_damp, damp, in, j20, j21, nc, i, D + i, nc,
+                                           sp);
+              else
+                tb_pair_step<false, LZ, LP>(Lc, Lw, ol, Mp, Ep, qu, qd, zin_a, zin_b, hx, hy, hz,
+                                            hc, use_damp, damp, in, j20, j21, nc, i, D + i, nc,
+                                            sp);
             }
           }
-          if (bad && in->flags) atomicOr(in->flags, 1);
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&Lempty[lprev.s]);  // this warp is done with plane q-1
         }
-#pragma unroll
-        for (int k = 0; k < 2; ++k) {
-          mp[k] = mc[k];
-          ep[k] = ec[k];
-#pragma unroll
-          for (int comp = 0; comp < 3; ++comp) cp[k][comp] = cc[k][comp];
-        }
-        s_prev = s_cur;
-        s_cur = s_next;
+        Mp = Mc;
+        Ep = Ec;
+        lprev = lw;
+        lw.next();
+        cur = nxt;
       }
-      if (failed) break;
+      if (!ok) break;
       __syncwarp();
-      if (lane == 0) {  // level-0 planes x1 and x1+1
-        mbar_arrive(&hd->emptyA[s_prev]);
-        mbar_arrive(&hd->emptyA[s_cur]);
+      if (lane == 0) {
+        mbar_arrive(&hd->emptyA[cur.s]);   // the closing halo plane x1+1
+        mbar_arrive(&Lempty[lprev.s]);     // the tile's last level-1 plane x1
       }
     }
   }
@@ -350,6 +394,7 @@ __global__ void __launch_bounds__(TmaF32TB::THREADS, 1)
     while (clock64() - t0 < 200000000LL) {
     }
   }
+  queue_cta_done(queue);
 }
 
 }  // namespace
@@ -357,9 +402,11 @@ __global__ void __launch_bounds__(TmaF32TB::THREADS, 1)
 // ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
+// alignment slack + header + rings + the level-1 ring's full / empty barriers
 size_t tb_smem_bytes() {
   return 128 + 256 + (size_t)TmaF32TB::NA * TmaF32TB::A_STAGE +
-         (size_t)TmaF32TB::NB * TmaF32TB::B_STAGE + (size_t)TmaF32TB::NL * TmaF32TB::L_STAGE;
+         (size_t)TmaF32TB::NB * TmaF32TB::B_STAGE + (size_t)TmaF32TB::NL * TmaF32TB::L_STAGE +
+         2 * TmaF32TB::NL * sizeof(uint64_t);
 }
 
 static int tb_set_attr() {
@@ -378,12 +425,11 @@ static int tb_set_attr() {
 
 // planes per x chunk: minimise waves x (level-1 planes per tile) on 148 SMs
 static int tb_xchunk(const Geom& g) {
-  const long long nzi = g.nz > 2 ? g.nz - 2 : 0, nyi = g.ny > 2 ? g.ny - 2 : 0;
   const long long nxi = g.nx > 2 ? g.nx - 2 : 0;
-  if (nxi == 0 || nzi == 0 || nyi == 0) return 1;
-  const long long cols = ((nzi + TmaF32TB::OZ - 1) / TmaF32TB::OZ) *
-                         ((nyi + TmaF32TB::OY - 1) / TmaF32TB::OY);
-  const long long slots = 148;
+  if (nxi == 0 || g.nz <= 2 || g.ny <= 2) return 1;
+  const TileSpace one = make_tiles_tb(g, (int)nxi);
+  const long long cols = (long long)one.ntz * one.nty;
+  const long long slots = kNumSMs;
   long long best_nc = 1, best = -1;
   for (long long nc = 1; nc <= nxi; ++nc) {
     const long long xc = (nxi + nc - 1) / nc;
@@ -409,18 +455,18 @@ int make_tma_f32_tb(const StepArgs& a, int xchunk, TmaF32TB* t) {
     set_error("the fused step kernel needs coef_e == coef_m + ncell");
     return SW_EINVAL;
   }
+  if (a.kahan) {
+    set_error("the two-steps-per-pass kernel runs without the compensated sum");
+    return SW_EINVAL;
+  }
   const uint64_t dims[4] = {(uint64_t)a.g.pz, (uint64_t)a.g.ny, (uint64_t)a.g.nx, 9};
   const uint64_t strides[3] = {(uint64_t)a.g.pz * 4, (uint64_t)a.g.sxy * 4,
                                (uint64_t)a.g.ncell * 4};
   const uint32_t boxA[4] = {TmaF32TB::W, TmaF32TB::H, 1, 6};
-  const uint32_t boxC[4] = {TmaF32TB::WB, TmaF32TB::HB, 1, 3};
   for (int b = 0; b < 3; ++b) {
     t->state[b] = (float*)a.state[b];
     int rc = encode_tmap_4d(&t->tm[b], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, a.state[b], dims, strides,
                             boxA);
-    if (rc == SW_OK)
-      rc = encode_tmap_4d(&t->tmc[b], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, a.state[b], dims, strides,
-                          boxC);
     if (rc != SW_OK) return rc;
   }
   const uint64_t mdims[4] = {(uint64_t)a.g.pz, (uint64_t)a.g.ny, (uint64_t)a.g.nx,
@@ -438,7 +484,6 @@ int make_tma_f32_tb(const StepArgs& a, int xchunk, TmaF32TB* t) {
   t->hz = (float)a.ihz2;
   t->damp = (float)a.damp;
   t->use_damp = a.use_damp;
-  t->kahan = a.kahan;
   t->n_steps = a.n_steps;
   t->snap_stride = a.snap_stride;
   t->snaps = (float*)a.snaps;
@@ -454,8 +499,8 @@ const void* step_f32_fused2_ptr() { return reinterpret_cast<const void*>(step_f3
 
 void launch_fused2_raw(const TmaF32TB& t, int it, cudaStream_t s) {
   if (t.ts.count == 0) return;
-  step_f32_fused2<false><<<std::min(t.ts.count, 148), TmaF32TB::THREADS, tb_smem_bytes(), s>>>(
-      t, nullptr, 1, t.ts.count, it, nullptr, nullptr);
+  step_f32_fused2<false><<<std::min(t.ts.count, kNumSMs), TmaF32TB::THREADS, tb_smem_bytes(),
+                           s>>>(t, nullptr, 1, t.ts.count, it, nullptr, nullptr);
 }
 
 int launch_fused2(const StepArgs& a, int xchunk, int it, cudaStream_t s) {
@@ -465,7 +510,7 @@ int launch_fused2(const StepArgs& a, int xchunk, int it, cudaStream_t s) {
   rc = make_tma_f32_tb(a, xchunk, &t);
   if (rc != SW_OK) return rc;
   if (t.ts.count == 0) return SW_OK;
-  const int grid = std::min(t.ts.count, 148);
+  const int grid = std::min(t.ts.count, kNumSMs);
   step_f32_fused2<false><<<grid, TmaF32TB::THREADS, tb_smem_bytes(), s>>>(
       t, nullptr, 1, t.ts.count, it, nullptr, nullptr);
   count_launches(1);
@@ -473,13 +518,14 @@ int launch_fused2(const StepArgs& a, int xchunk, int it, cudaStream_t s) {
   return SW_OK;
 }
 
-int launch_fused2_batch(const void* d_tab, int ninst, int ntiles, int it, cudaStream_t s) {
+int launch_fused2_batch(const void* d_tab, int ninst, int ntiles, int it, int* queues,
+                        cudaStream_t s) {
   int rc = tb_set_attr();
   if (rc != SW_OK) return rc;
   if (ntiles == 0) return SW_OK;
   TmaF32TB dummy{};
-  step_f32_fused2<true><<<std::min(ntiles, 148), TmaF32TB::THREADS, tb_smem_bytes(), s>>>(
-      dummy, (const TmaF32TB*)d_tab, ninst, ntiles, it, nullptr, nullptr);
+  step_f32_fused2<true><<<std::min(ntiles, kNumSMs), TmaF32TB::THREADS, tb_smem_bytes(), s>>>(
+      dummy, (const TmaF32TB*)d_tab, ninst, ntiles, it, nullptr, queues);
   count_launches(1);
   SW_CHECK_LAUNCH("fused two-step kernel (batch)");
   return SW_OK;

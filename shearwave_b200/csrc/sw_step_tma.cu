@@ -181,10 +181,9 @@ __global__ void __launch_bounds__(TmaF32::THREADS, TmaF32::MIN_CTAS)
   constexpr int TYH = TmaF32::TZ * TmaF32::TY / TZW;
   static_assert(TZW == 64 || TZW == 32, "tile widths 64 and 32");
   if (it_dev != nullptr) it += *it_dev;  // step counter kept on the device (graph replays)
-  // batched launches take tiles from queue it & 1 and reset the other one
-  // for the next launch of the stream
-  int* queue = (BATCH && queues != nullptr) ? queues + (it & 1) : nullptr;
-  if (queue != nullptr && blockIdx.x == 0 && threadIdx.x == 0) queues[(it + 1) & 1] = 0;
+  // batched launches take tiles from a launch-wide queue, which the last CTA
+  // to finish resets for the next launch
+  int* queue = (BATCH && queues != nullptr) ? queues : nullptr;
   constexpr int NA = F32Ring<KR>::NA, NB = F32Ring<KR>::NB;
   constexpr int HWB = TmaF32::box_cells(TZW);                   // halo-box cells per component
   constexpr uint32_t A_BYTES = (uint32_t)HWB * 6 * 4;          // one plane's u and d
@@ -201,6 +200,7 @@ __global__ void __launch_bounds__(TmaF32::THREADS, TmaF32::MIN_CTAS)
   if ((smem_addr(ringA) & 127u) != 0u) {  // never issue a TMA to a misaligned destination
     int* fl = BATCH ? (ninst > 0 ? tab[0].flags : nullptr) : one.flags;
     if (threadIdx.x == 0 && fl) atomicOr(fl, 4);
+    queue_cta_done(queue);
     return;
   }
   if (threadIdx.x == 0) {
@@ -386,6 +386,7 @@ __global__ void __launch_bounds__(TmaF32::THREADS, TmaF32::MIN_CTAS)
     while (clock64() - t0 < 200000000LL) {
     }
   }
+  queue_cta_done(queue);
 }
 
 // ---------------------------------------------------------------------------
@@ -396,8 +397,7 @@ __global__ void __launch_bounds__(TmaF64::THREADS, 2)
     step_f64_tma(const __grid_constant__ TmaF64 one, const TmaF64* __restrict__ tab, int ninst,
                  int ntiles, int it, const int* __restrict__ it_dev, int* queues) {
   if (it_dev != nullptr) it += *it_dev;  // step counter kept on the device (graph replays)
-  int* queue = (BATCH && queues != nullptr) ? queues + (it & 1) : nullptr;  // see step_f32_tma
-  if (queue != nullptr && blockIdx.x == 0 && threadIdx.x == 0) queues[(it + 1) & 1] = 0;
+  int* queue = (BATCH && queues != nullptr) ? queues : nullptr;  // see step_f32_tma
   constexpr int NA = TmaF64::NA, NB = TmaF64::NB, W = TmaF64::W, H = TmaF64::H;
   constexpr int TZ = TmaF64::TZ, TY = TmaF64::TY;
   constexpr int AD = TmaF64::A_STAGE / 8, BD = TmaF64::B_STAGE / 8, HALF = TmaF64::HALF / 8;
@@ -411,6 +411,7 @@ __global__ void __launch_bounds__(TmaF64::THREADS, 2)
   if ((smem_addr(ringA) & 127u) != 0u) {
     int* fl = BATCH ? (ninst > 0 ? tab[0].flags : nullptr) : one.flags;
     if (threadIdx.x == 0 && fl) atomicOr(fl, 4);
+    queue_cta_done(queue);
     return;
   }
   if (threadIdx.x == 0) {
@@ -602,6 +603,7 @@ __global__ void __launch_bounds__(TmaF64::THREADS, 2)
     while (clock64() - t0 < 200000000LL) {
     }
   }
+  queue_cta_done(queue);
 }
 
 // ---------------------------------------------------------------------------
@@ -895,7 +897,7 @@ int launch_steps_tma(const StepArgs& a, int xchunk, int it0, int nsteps, cudaStr
   } else {
     // steps_per_pass 2: two steps per launch where two remain, one step
     // otherwise; 0 (automatic) and 1: one step per launch
-    const bool fuse = a.steps_per_pass == 2 && nsteps >= 2;
+    const bool fuse = a.steps_per_pass == 2 && !a.kahan && nsteps >= 2;
     TmaF32 t;
     rc = make_tma_f32(a, xchunk, &t, 0);
     if (rc != SW_OK) return rc;
@@ -912,7 +914,7 @@ int launch_steps_tma(const StepArgs& a, int xchunk, int it0, int nsteps, cudaStr
     int done = 0;
     if (fuse && tb.ts.count > 0)
       rc = graph_loop(const_cast<void*>(step_f32_fused2_ptr()), tb,
-                      std::min(tb.ts.count, 148), TmaF32TB::THREADS, tb_smem_bytes(), 2, 16,
+                      std::min(tb.ts.count, kNumSMs), TmaF32TB::THREADS, tb_smem_bytes(), 2, 16,
                       a.clock, it0, nsteps, s, &done);
     else
       rc = graph_loop(const_cast<void*>(f32_kernel(false, t.tzw, t.kahan != 0)), t, grid,
@@ -1078,7 +1080,7 @@ int batch_steps_mixed(const sw_fdtd_desc* descs, const int32_t* begins, int n, i
   cudaError_t e0 = cudaMemsetAsync(queues, 0, 2 * sizeof(int), s);
   if (e0 != cudaSuccess) return cuda_status(e0, "batch queue reset");
   bool fuse_ok = true;
-  for (int i = 0; i < n; ++i) fuse_ok &= (descs[i].steps_per_pass == 2);
+  for (int i = 0; i < n; ++i) fuse_ok &= (descs[i].steps_per_pass == 2 && !descs[i].kahan);
   auto active = [&](int i, int it) {
     const int lit = it - (begins ? begins[i] : 0);
     return lit >= 0 && lit < descs[i].n_steps;
@@ -1113,13 +1115,15 @@ int batch_steps_mixed(const sw_fdtd_desc* descs, const int32_t* begins, int n, i
       ntiles = 0;
       for (int i = 0; i < n; ++i) cur[i] = active(i, it) ? 1 : 0;
       if (kind == 1) {
-        for (int i = 0; i < n; ++i) {
-          if (!cur[i]) continue;
+        std::vector<int> run;
+        for (int i = 0; i < n; ++i)
+          if (cur[i]) run.push_back(i);
+        for (int i : batch_order(descs, run)) {
           StepArgs a;
           int rc = make_step_args(&descs[i], &a);
           if (rc != SW_OK) return rc;
           TmaF32TB t;
-          rc = make_tma_f32_tb(a, descs[i].xchunk > 0 ? descs[i].xchunk : 24, &t);
+          rc = make_tma_f32_tb(a, descs[i].xchunk > 0 ? descs[i].xchunk : 32, &t);
           if (rc != SW_OK) return rc;
           t.it_begin = begins ? begins[i] : 0;
           t.tile_base = ntiles;
@@ -1141,7 +1145,7 @@ int batch_steps_mixed(const sw_fdtd_desc* descs, const int32_t* begins, int n, i
     }
     int rc;
     if (kind == 1) {
-      rc = launch_fused2_batch(tab_fused, (int)tfused.size(), ntiles, it, s);
+      rc = launch_fused2_batch(tab_fused, (int)tfused.size(), ntiles, it, queues, s);
       it += 2;
     } else {
       bool kr = false;  // the compensation ring layout if any running solve needs it

@@ -89,33 +89,35 @@ struct TmaF64 {
   int tile_base;
 };
 
-// Kernel-side view of one mixed-form solve for the two-steps-per-pass kernel.
-// Step t+1 is computed on an LZ x LY region (the output tile plus one cell of
-// halo), step t+2 on the OZ x OY output tile.  Output tiles start at z = 1 +
-// 62 k and y = 1 + 6 k; the TMA boxes start at the 16-byte aligned z at or
-// below the region they cover, and the kernel indexes from that offset.
-//   tm[b]  : state buffer b (pz, ny, nx, 9), box (W, H, 1, 6): u and d with
-//            two cells of halo around the output tile
-//   tmc[b] : state buffer b, box (WB, HB, 1, 3) at component 6: Kahan c on
-//            the step-(t+1) region
-//   tmm    : coefficients (pz, ny, nx, ncoef), box (WB, HB, 1, ncoef)
+// Kernel-side view of one mixed-form solve for the two-steps-per-pass kernel
+// (no compensated sum).  Output tiles are OZ x OY cells starting at
+// z = 60 kz, y = 13 ky; step t+1 is computed on the LZ x LY region around
+// the tile (z from z0-2, y from y0-1: the tile plus one cell of halo, and one
+// more column each side in z so that z pairs stay 8-byte aligned), step t+2
+// on the tile.  A CTA has LY consumer warps, one level-1 row of 32 z pairs
+// each.
+//   tm[b]  : state buffer b (pz, ny, nx, 9), box (W, H, 1, 6) from (z0-4,
+//            y0-2): u and d with two cells of halo (and alignment) around
+//            the tile
+//   tmm    : coefficients (pz, ny, nx, ncoef), box (WB, HB, 1, ncoef) from
+//            (z0-4, y0-1): the level-1 rows
 struct TmaF32TB {
-  static constexpr int OZ = 62, OY = 6;   // output tile (z, y)
-  static constexpr int LZ = 64, LY = 8;   // step-(t+1) region
-  static constexpr int W = 72, H = OY + 4;
-  static constexpr int WB = 72, HB = LY;
-  // ring stages: level 0 (3 planes in use, 3 in flight), point data, level 1
-  static constexpr int NA = 6, NB = 4, NL = 4;
+  // 15 consumer warps + the producer = 16 warps: four per scheduler, which
+  // leaves each thread up to 128 registers (17 warps would cap it at 96)
+  static constexpr int OZ = 60, OY = 13;  // output tile (z, y)
+  static constexpr int LZ = 64, LY = 15;  // step-(t+1) region
+  static constexpr int W = 68, H = OY + 4;
+  static constexpr int WB = 68, HB = LY;
+  // ring stages: level 0 (planes q, q+1 held, two in flight), points, level 1
+  static constexpr int NA = 4, NB = 3, NL = 3;
   static constexpr int A_BYTES = W * H * 6 * 4;
-  static constexpr int C_BYTES = WB * HB * 3 * 4;
   static constexpr int M_BYTES = WB * HB * 2 * 4;
   static constexpr int A_STAGE = round128(A_BYTES);
-  static constexpr int B_STAGE = round128(C_BYTES) + round128(M_BYTES);
+  static constexpr int B_STAGE = round128(M_BYTES);
   static constexpr int L_STAGE = round128(LZ * LY * 6 * 4);
   static constexpr int CONSUMER_WARPS = LY;
   static constexpr int THREADS = 32 * (CONSUMER_WARPS + 1);
   CUtensorMap tm[3];
-  CUtensorMap tmc[3];
   CUtensorMap tmm;
   Geom g;
   TileSpace ts;  // z tiles of OZ, y tiles of OY, x chunks
@@ -126,7 +128,7 @@ struct TmaF32TB {
   const double* term_scale;
   float hx, hy, hz, damp;
   int ncoef;
-  int use_damp, kahan, n_steps, snap_stride;
+  int use_damp, n_steps, snap_stride;
   float* snaps;
   int* flags;
   int it_begin;
@@ -140,7 +142,8 @@ int launch_fused2(const StepArgs& a, int xchunk, int it, cudaStream_t s);
 int launch_fused2_prepare();                                   // kernel attributes, once
 void launch_fused2_raw(const TmaF32TB& t, int it, cudaStream_t s);  // enqueue one launch
 const void* step_f32_fused2_ptr();  // the single-solve fused kernel (for graph nodes)
-int launch_fused2_batch(const void* d_tab, int ninst, int ntiles, int it, cudaStream_t s);
+int launch_fused2_batch(const void* d_tab, int ninst, int ntiles, int it, int* queues,
+                        cudaStream_t s);
 int tma_xchunk(const Geom& g, int tz, int ty, long long want_tiles);
 // Mixed-step tile width for a grid (64 or 32; the SW_TUNE_TILE_SHAPE knob
 // can force one) and the plane cells a tile width covers.

@@ -121,6 +121,32 @@ __device__ inline int next_tile(int* queue, int& stride_next) {
   return t;
 }
 
+// End of a CTA of a queue-fed launch: the last CTA to finish resets the
+// launch-wide queue (queues[0]) and the finish count (queues[1]) for the next
+// launch of the stream.  Every CTA has taken its last tile by then.
+__device__ inline void queue_cta_done(int* queues) {
+  if (queues == nullptr || threadIdx.x != 0) return;
+  __threadfence();
+  if (atomicAdd(queues + 1, 1) == (int)gridDim.x - 1) {
+    atomicExch(queues, 0);
+    atomicExch(queues + 1, 0);
+  }
+}
+
+// Position in a ring of N stages: the stage index and the phase parity of
+// its barriers, advanced without divisions.
+template <int N>
+struct RingPos {
+  int s = 0;
+  uint32_t ph = 0;
+  __device__ inline void next() {
+    if (++s == N) {
+      s = 0;
+      ph ^= 1u;
+    }
+  }
+};
+
 // Table index of the solve that owns global tile t (tile_base ascending).
 template <typename Inst>
 __device__ inline int find_solve(const Inst* __restrict__ tab, int ninst, int t) {

@@ -220,16 +220,16 @@ __global__ void __launch_bounds__(TmaF32::THREADS, TmaF32::MIN_CTAS)
   if (warp == TmaF32::CONSUMER_WARPS) {
     // ------------------------------- producer -----------------------------
     if (lane == 0) {
-      uint32_t pa = 0, pb = 0;  // loads issued into ring A / ring B
+      RingPos<NA> pa;  // next stage of ring A / ring B to load
+      RingPos<NB> pb;
       int stride_next = blockIdx.x;
       while (!*abort_flag) {
         const int t = next_tile(queue, stride_next);
         if (t >= ntiles) {  // end of this CTA's work: arm one stage without a copy
-          const int sa = pa % NA;
-          if (!ws_wait(&hd->emptyA[sa], ((pa / NA) & 1u) ^ 1u, abort_flag)) break;
-          tile_slots(base)[sa] = -1;
-          mbar_arrive(&hd->fullA[sa]);
-          ++pa;
+          if (!ws_wait(&hd->emptyA[pa.s], pa.ph ^ 1u, abort_flag)) break;
+          tile_slots(base)[pa.s] = -1;
+          mbar_arrive(&hd->fullA[pa.s]);
+          pa.next();
           break;
         }
         const int k = BATCH ? find_solve(tab, ninst, t) : 0;
@@ -243,8 +243,8 @@ __global__ void __launch_bounds__(TmaF32::THREADS, TmaF32::MIN_CTAS)
         const bool kahan = KR && in->kahan;  // the compact ring never carries c
         const uint32_t bbytes = (kahan ? TmaF32::C_BYTES : 0) + TZ * TY * 4 * in->ncoef;
         for (int p = tc.x0 - 1; p <= tc.x1 && !*abort_flag; ++p) {
-          const int sa = pa % NA;
-          if (!ws_wait(&hd->emptyA[sa], ((pa / NA) & 1u) ^ 1u, abort_flag)) break;
+          const int sa = pa.s;
+          if (!ws_wait(&hd->emptyA[sa], pa.ph ^ 1u, abort_flag)) break;
           if (p == tc.x0 - 1) {
             tile_slots(base)[sa] = t;
             solve_slots(base)[sa] = k;
@@ -252,15 +252,15 @@ __global__ void __launch_bounds__(TmaF32::THREADS, TmaF32::MIN_CTAS)
           fence_proxy_async_smem();
           mbar_arrive_expect_tx(&hd->fullA[sa], A_BYTES);
           tma_load_4d(ringA + sa * AF, tma, &hd->fullA[sa], tc.z0 - 4, tc.y0 - 1, p, 0);
-          ++pa;
+          pa.next();
           if (p >= tc.x0 && p < tc.x1) {
-            const int sb = pb % NB;
-            if (!ws_wait(&hd->emptyB[sb], ((pb / NB) & 1u) ^ 1u, abort_flag)) break;
+            const int sb = pb.s;
+            if (!ws_wait(&hd->emptyB[sb], pb.ph ^ 1u, abort_flag)) break;
             fence_proxy_async_smem();
             mbar_arrive_expect_tx(&hd->fullB[sb], bbytes);
             if (kahan) tma_load_4d(ringB + sb * BF, tmc, &hd->fullB[sb], tc.z0, tc.y0, p, 6);
             tma_load_4d(ringB + sb * BF + CF, &in->tmm, &hd->fullB[sb], tc.z0, tc.y0, p, 0);
-            ++pb;
+            pb.next();
           }
         }
       }
@@ -268,13 +268,14 @@ __global__ void __launch_bounds__(TmaF32::THREADS, TmaF32::MIN_CTAS)
   } else {
     // ------------------------------- consumers ----------------------------
     const int ly = warp;
-    uint32_t ca = 0, cb = 0;  // planes consumed from ring A / ring B
+    RingPos<NA> ca;  // next plane to consume from ring A / ring B
+    RingPos<NB> cb;
     while (true) {
-      int s_cur = ca % NA;  // the tile's first plane (its halo plane x0-1)
-      if (!ws_wait(&hd->fullA[s_cur], (ca / NA) & 1u, abort_flag)) break;
-      const int t = tile_slots(base)[s_cur];
+      // the tile's first plane (its halo plane x0-1)
+      if (!ws_wait(&hd->fullA[ca.s], ca.ph, abort_flag)) break;
+      const int t = tile_slots(base)[ca.s];
       if (t < 0) break;
-      const TmaF32* in = BATCH ? &tab[solve_slots(base)[s_cur]] : &one;
+      const TmaF32* in = BATCH ? &tab[solve_slots(base)[ca.s]] : &one;
       const int local = BATCH ? t - in->tile_base : t;
       const int lit = it - in->it_begin;
       // the per-cell switches in registers: the table lives in global memory and
@@ -312,9 +313,8 @@ __global__ void __launch_bounds__(TmaF32::THREADS, TmaF32::MIN_CTAS)
       // computed, and the ring holds planes x and x+1 with two more in flight.
       float2 pu[3], pd[3];  // u and d of plane x-1 at this thread's cells
       bool ok = true;
-      ++ca;  // plane x0-1 (waited for above): centres only
-      {
-        const float* P0 = ringA + s_cur * AF;
+      {  // plane x0-1 (waited for above): centres only
+        const float* P0 = ringA + ca.s * AF;
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
           pu[c] = lds2(P0 + o + c * HWB);
@@ -322,18 +322,19 @@ __global__ void __launch_bounds__(TmaF32::THREADS, TmaF32::MIN_CTAS)
         }
       }
       __syncwarp();
-      if (lane == 0) mbar_arrive(&hd->emptyA[s_cur]);
-      s_cur = ca % NA;
-      ok &= ws_wait(&hd->fullA[s_cur], (ca / NA) & 1u, abort_flag);
-      ++ca;
+      if (lane == 0) mbar_arrive(&hd->emptyA[ca.s]);
+      ca.next();
+      int s_cur = ca.s;
+      ok &= ws_wait(&hd->fullA[s_cur], ca.ph, abort_flag);
+      ca.next();
       long long i = (long long)tc.x0 * g.sxy + (long long)y * g.pz + z;
       for (int x = tc.x0; x < tc.x1 && ok; ++x, i += g.sxy) {
-        const int s_next = ca % NA;
-        ok &= ws_wait(&hd->fullA[s_next], (ca / NA) & 1u, abort_flag);
-        ++ca;
-        const int sb = cb % NB;
-        ok &= ws_wait(&hd->fullB[sb], (cb / NB) & 1u, abort_flag);
-        ++cb;
+        const int s_next = ca.s;
+        ok &= ws_wait(&hd->fullA[s_next], ca.ph, abort_flag);
+        ca.next();
+        const int sb = cb.s;
+        ok &= ws_wait(&hd->fullB[sb], cb.ph, abort_flag);
+        cb.next();
         if (!ok) break;
         if (inrow) {
           const float* Pc = ringA + s_cur * AF;
@@ -430,16 +431,16 @@ __global__ void __launch_bounds__(TmaF64::THREADS, 2)
 
   if (warp == TmaF64::CONSUMER_WARPS) {
     if (lane == 0) {
-      uint32_t pa = 0, pb = 0;
+      RingPos<NA> pa;
+      RingPos<NB> pb;
       int stride_next = blockIdx.x;
       while (!*abort_flag) {
         const int t = next_tile(queue, stride_next);
         if (t >= ntiles) {  // end of this CTA's work: arm one stage without a copy
-          const int sa = pa % NA;
-          if (!ws_wait(&hd->emptyA[sa], ((pa / NA) & 1u) ^ 1u, abort_flag)) break;
-          tile_slots(base)[sa] = -1;
-          mbar_arrive(&hd->fullA[sa]);
-          ++pa;
+          if (!ws_wait(&hd->emptyA[pa.s], pa.ph ^ 1u, abort_flag)) break;
+          tile_slots(base)[pa.s] = -1;
+          mbar_arrive(&hd->fullA[pa.s]);
+          pa.next();
           break;
         }
         const int k = BATCH ? find_solve(tab, ninst, t) : 0;
@@ -452,8 +453,8 @@ __global__ void __launch_bounds__(TmaF64::THREADS, 2)
         const CUtensorMap* tmc = &in->tm[(lit + 1) % 3];
         const uint32_t bbytes = TZ * TY * 8 * in->ncoef;
         for (int p = tc.x0 - 1; p <= tc.x1 && !*abort_flag; ++p) {
-          const int sa = pa % NA;
-          if (!ws_wait(&hd->emptyA[sa], ((pa / NA) & 1u) ^ 1u, abort_flag)) break;
+          const int sa = pa.s;
+          if (!ws_wait(&hd->emptyA[sa], pa.ph ^ 1u, abort_flag)) break;
           if (p == tc.x0 - 1) {
             tile_slots(base)[sa] = t;
             solve_slots(base)[sa] = k;
@@ -462,24 +463,25 @@ __global__ void __launch_bounds__(TmaF64::THREADS, 2)
           mbar_arrive_expect_tx(&hd->fullA[sa], 2 * TmaF64::BOX_BYTES);
           tma_load_4d(ringA + sa * AD, tmp, &hd->fullA[sa], tc.z0 - 2, tc.y0 - 1, p, 0);
           tma_load_4d(ringA + sa * AD + HALF, tmc, &hd->fullA[sa], tc.z0 - 2, tc.y0 - 1, p, 0);
-          ++pa;
+          pa.next();
           if (p >= tc.x0 && p < tc.x1) {
-            const int sb = pb % NB;
-            if (!ws_wait(&hd->emptyB[sb], ((pb / NB) & 1u) ^ 1u, abort_flag)) break;
+            const int sb = pb.s;
+            if (!ws_wait(&hd->emptyB[sb], pb.ph ^ 1u, abort_flag)) break;
             fence_proxy_async_smem();
             mbar_arrive_expect_tx(&hd->fullB[sb], bbytes);
             tma_load_4d(ringB + sb * BD, &in->tmm, &hd->fullB[sb], tc.z0, tc.y0, p, 0);
-            ++pb;
+            pb.next();
           }
         }
       }
     }
   } else {
     const int ly = warp;
-    uint32_t ca = 0, cb = 0;
+    RingPos<NA> ca;
+    RingPos<NB> cb;
     while (true) {
-      int s_cur = ca % NA;  // the tile's first plane (its halo plane x0-1)
-      if (!ws_wait(&hd->fullA[s_cur], (ca / NA) & 1u, abort_flag)) break;
+      int s_cur = ca.s;  // the tile's first plane (its halo plane x0-1)
+      if (!ws_wait(&hd->fullA[s_cur], ca.ph, abort_flag)) break;
       const int t = tile_slots(base)[s_cur];
       if (t < 0) break;
       const TmaF64* in = BATCH ? &tab[solve_slots(base)[s_cur]] : &one;
@@ -505,7 +507,7 @@ __global__ void __launch_bounds__(TmaF64::THREADS, 2)
       // soon as the plane is computed (see step_f32_tma)
       double qc[3], qp[3];
       bool ok = true;
-      ++ca;  // plane x0-1 (waited for above): centres only
+      ca.next();  // plane x0-1 (waited for above): centres only
       {
         const double* P0 = ringA + s_cur * AD;
 #pragma unroll
@@ -517,17 +519,17 @@ __global__ void __launch_bounds__(TmaF64::THREADS, 2)
       }
       __syncwarp();
       if (lane == 0) mbar_arrive(&hd->emptyA[s_cur]);
-      s_cur = ca % NA;
-      ok &= ws_wait(&hd->fullA[s_cur], (ca / NA) & 1u, abort_flag);
-      ++ca;
+      s_cur = ca.s;
+      ok &= ws_wait(&hd->fullA[s_cur], ca.ph, abort_flag);
+      ca.next();
       long long i = (long long)tc.x0 * g.sxy + (long long)y * g.pz + z;
       for (int x = tc.x0; x < tc.x1 && ok; ++x, i += g.sxy) {
-        const int s_next = ca % NA;
-        ok &= ws_wait(&hd->fullA[s_next], (ca / NA) & 1u, abort_flag);
-        ++ca;
-        const int sb = cb % NB;
-        ok &= ws_wait(&hd->fullB[sb], (cb / NB) & 1u, abort_flag);
-        ++cb;
+        const int s_next = ca.s;
+        ok &= ws_wait(&hd->fullA[s_next], ca.ph, abort_flag);
+        ca.next();
+        const int sb = cb.s;
+        ok &= ws_wait(&hd->fullB[sb], cb.ph, abort_flag);
+        cb.next();
         if (!ok) break;
         const double* Pc = ringA + s_cur * AD;
         const double* Pn = ringA + s_next * AD;

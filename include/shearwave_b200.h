@@ -255,6 +255,10 @@ typedef struct sw_fdtd_desc {
    * of sw_fdtd_steps replay one instantiated CUDA graph of 32 steps instead
    * of launching every step (NULL: direct launches only). */
   int32_t* clock;
+  /* Two device int32s, zero at the first call (the kernels leave them zero):
+   * the launch-wide tile queue of this solve's own step launches, which
+   * balances tiles over the SMs (NULL: tiles in a fixed stride). */
+  int32_t* queue;
 } sw_fdtd_desc;
 
 /* Material coefficients from rho, mu, eta.  Each of rho/mu/eta is a dense

@@ -75,6 +75,7 @@ class FdtdDesc(C.Structure):
         ("steps_per_pass", C.c_int32),
         ("kernel", C.c_int32),
         ("clock", C.c_void_p),
+        ("queue", C.c_void_p),
     ]
 
 

@@ -87,6 +87,7 @@ int make_step_args(const sw_fdtd_desc* d, StepArgs* a) {
   a->xchunk = d->xchunk;
   a->steps_per_pass = d->steps_per_pass;
   a->clock = d->clock;
+  a->queue = d->queue;
   const int nbuf = 3;
   for (int i = 0; i < nbuf; ++i)
     if (a->state[i] == nullptr) {

@@ -31,6 +31,7 @@ struct StepArgs {
   int xchunk;          // requested planes per tile (0 automatic)
   int steps_per_pass;  // mixed form: 2 two steps per launch, 0 / 1 one
   int* clock;          // device step counter for graph replays (or null)
+  int* queue;          // launch-wide tile queue of one-solve launches (or null)
 };
 
 // 7-point Laplacian of the mixed form from the three neighbour-pair sums

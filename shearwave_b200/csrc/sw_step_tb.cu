@@ -144,7 +144,7 @@ __global__ void __launch_bounds__(TmaF32TB::THREADS, 1)
                     int ninst, int ntiles, int it, const int* __restrict__ it_dev, int* queues) {
   if (it_dev != nullptr) it += *it_dev;  // step counter kept on the device (graph replays)
   // batched launches take tiles from a launch-wide queue (see step_f32_tma)
-  int* queue = (BATCH && queues != nullptr) ? queues : nullptr;
+  int* queue = queues;
   using T = TmaF32TB;
   constexpr int NA = T::NA, NB = T::NB, NL = T::NL, W = T::W, H = T::H, WB = T::WB, HB = T::HB;
   constexpr int LZ = T::LZ, LY = T::LY, NC = T::CONSUMER_WARPS * 32;

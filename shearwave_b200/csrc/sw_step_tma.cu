@@ -181,9 +181,9 @@ __global__ void __launch_bounds__(TmaF32::THREADS, TmaF32::MIN_CTAS)
   constexpr int TYH = TmaF32::TZ * TmaF32::TY / TZW;
   static_assert(TZW == 64 || TZW == 32, "tile widths 64 and 32");
   if (it_dev != nullptr) it += *it_dev;  // step counter kept on the device (graph replays)
-  // batched launches take tiles from a launch-wide queue, which the last CTA
-  // to finish resets for the next launch
-  int* queue = (BATCH && queues != nullptr) ? queues : nullptr;
+  // with a queue, CTAs take tiles from it (the last CTA to finish resets it
+  // for the next launch); without, tiles go in a fixed stride
+  int* queue = queues;
   constexpr int NA = F32Ring<KR>::NA, NB = F32Ring<KR>::NB;
   constexpr int HWB = TmaF32::box_cells(TZW);                   // halo-box cells per component
   constexpr uint32_t A_BYTES = (uint32_t)HWB * 6 * 4;          // one plane's u and d
@@ -398,7 +398,7 @@ __global__ void __launch_bounds__(TmaF64::THREADS, 2)
     step_f64_tma(const __grid_constant__ TmaF64 one, const TmaF64* __restrict__ tab, int ninst,
                  int ntiles, int it, const int* __restrict__ it_dev, int* queues) {
   if (it_dev != nullptr) it += *it_dev;  // step counter kept on the device (graph replays)
-  int* queue = (BATCH && queues != nullptr) ? queues : nullptr;  // see step_f32_tma
+  int* queue = queues;  // see step_f32_tma
   constexpr int NA = TmaF64::NA, NB = TmaF64::NB, W = TmaF64::W, H = TmaF64::H;
   constexpr int TZ = TmaF64::TZ, TY = TmaF64::TY;
   constexpr int AD = TmaF64::A_STAGE / 8, BD = TmaF64::B_STAGE / 8, HALF = TmaF64::HALF / 8;
@@ -687,6 +687,25 @@ int tma_xchunk(const Geom& g, int tz, int ty, long long slots) {
   return (int)((nxi + best_nc - 1) / best_nc);
 }
 
+// Planes per x chunk for a queue-fed launch over one grid: about
+// SW_TUNE_BATCH_TILES_PER_CTA tiles per CTA slot, at least 8 planes, the
+// interior split into equal chunks.
+static int queue_xchunk(const Geom& g, int tz, int ty, long long slots) {
+  const long long nxi = g.nx > 2 ? g.nx - 2 : 0;
+  if (nxi == 0) return 1;
+  const long long cols = (long long)((g.nz + tz - 1) / tz) * ((g.ny + ty - 1) / ty);
+  // when whole waves of equal chunks already fill >= 90 % of the slots, keep
+  // them (fewer chunks, fewer re-read halo planes)
+  const int xw = tma_xchunk(g, tz, ty, slots);
+  const long long tiles = cols * ((nxi + xw - 1) / xw);
+  const long long waves = (tiles + slots - 1) / slots;
+  if (10 * tiles >= 9 * waves * slots) return xw;
+  const long long want = (long long)tune_get(SW_TUNE_BATCH_TILES_PER_CTA) * slots;
+  const long long xc = std::max<long long>(8, (cols * nxi + want - 1) / want);
+  const long long nch = (nxi + xc - 1) / xc;
+  return (int)((nxi + nch - 1) / nch);
+}
+
 // Material coefficients must be one allocation: component 0 = mu term,
 // component 1 (optional) = eta term, ncell elements apart.
 static int coef_components(const StepArgs& a, size_t es, int* ncoef) {
@@ -723,7 +742,9 @@ int make_tma_f32(const StepArgs& a, int xchunk, TmaF32* t, int tzw) {
   t->tzw = tzw > 0 ? tzw : f32_tile_width(a.g);
   t->tyh = TmaF32::TZ * TmaF32::TY / t->tzw;
   const int xt = xchunk > 0 ? xchunk : tune_get(SW_TUNE_XCHUNK);
-  const int xc = xt > 0 ? xt : tma_xchunk(a.g, t->tzw, t->tyh, step_slots());
+  const int xc = xt > 0 ? xt
+                        : (a.queue ? queue_xchunk(a.g, t->tzw, t->tyh, step_slots())
+                                   : tma_xchunk(a.g, t->tzw, t->tyh, step_slots()));
   t->ts = make_tiles_t(a.g, xc, t->tzw, t->tyh);
   int rc = coef_components(a, 4, &t->ncoef);
   if (rc != SW_OK) return rc;
@@ -770,7 +791,9 @@ int make_tma_f64(const StepArgs& a, int xchunk, TmaF64* t) {
   *t = TmaF64{};
   t->g = a.g;
   const int xt = xchunk > 0 ? xchunk : tune_get(SW_TUNE_XCHUNK);
-  const int xc = xt > 0 ? xt : tma_xchunk(a.g, TmaF64::TZ, TmaF64::TY, step_slots(false));
+  const int xc = xt > 0 ? xt
+                        : (a.queue ? queue_xchunk(a.g, TmaF64::TZ, TmaF64::TY, step_slots(false))
+                                   : tma_xchunk(a.g, TmaF64::TZ, TmaF64::TY, step_slots(false)));
   t->ts = make_tiles_t(a.g, xc, TmaF64::TZ, TmaF64::TY);
   int rc = coef_components(a, 8, &t->ncoef);
   if (rc != SW_OK) return rc;
@@ -822,7 +845,7 @@ __global__ void clock_add(int* c, int by) { *c += by; }
 // explicitly, so the caller's stream may be the legacy default stream.
 template <typename Inst>
 int graph_loop(void* func, const Inst& t, int grid, int threads, size_t smem, int per_launch,
-               int seg, int* clock, int it0, int nsteps, cudaStream_t s, int* done) {
+               int seg, int* clock, int* queue, int it0, int nsteps, cudaStream_t s, int* done) {
   *done = 0;
   const int seg_steps = per_launch * seg;
   const int reps = nsteps / seg_steps;
@@ -834,7 +857,7 @@ int graph_loop(void* func, const Inst& t, int grid, int threads, size_t smem, in
   const Inst* tab = nullptr;
   int ninst = 1, ntiles = t.ts.count;
   const int* itd = clock;
-  int* queues = nullptr;
+  int* queues = queue;
   std::vector<int> offs(seg);
   for (int k = 0; k < seg && e == cudaSuccess; ++k) {
     offs[k] = k * per_launch;
@@ -888,11 +911,11 @@ int launch_steps_tma(const StepArgs& a, int xchunk, int it0, int nsteps, cudaStr
     const int grid = std::min(t.ts.count, step_slots(false));
     int done = 0;
     rc = graph_loop(reinterpret_cast<void*>(step_f64_tma<false>), t, grid, TmaF64::THREADS, smem,
-                    1, 32, a.clock, it0, nsteps, s, &done);
+                    1, 32, a.clock, a.queue, it0, nsteps, s, &done);
     if (rc != SW_OK) return rc;
     for (int it = it0 + done; it < it0 + nsteps; ++it)
       step_f64_tma<false><<<grid, TmaF64::THREADS, smem, s>>>(t, nullptr, 1, t.ts.count, it,
-                                                              nullptr, nullptr);
+                                                              nullptr, a.queue);
     count_launches((unsigned long long)(nsteps - done));
     SW_CHECK_LAUNCH("step (tma)");
     return SW_OK;
@@ -917,11 +940,11 @@ int launch_steps_tma(const StepArgs& a, int xchunk, int it0, int nsteps, cudaStr
     if (fuse && tb.ts.count > 0)
       rc = graph_loop(const_cast<void*>(step_f32_fused2_ptr()), tb,
                       std::min(tb.ts.count, kNumSMs), TmaF32TB::THREADS, tb_smem_bytes(), 2, 16,
-                      a.clock, it0, nsteps, s, &done);
+                      a.clock, a.queue, it0, nsteps, s, &done);
     else
       rc = graph_loop(const_cast<void*>(f32_kernel(false, t.tzw, t.kahan != 0)), t, grid,
-                      TmaF32::THREADS, f32_smem(t.kahan != 0), 1, 32, a.clock, it0, nsteps, s,
-                      &done);
+                      TmaF32::THREADS, f32_smem(t.kahan != 0), 1, 32, a.clock, a.queue, it0,
+                      nsteps, s, &done);
     if (rc != SW_OK) return rc;
     for (int it = it0 + done; it < it0 + nsteps;) {
       if (fuse && it + 1 < it0 + nsteps) {
@@ -929,7 +952,7 @@ int launch_steps_tma(const StepArgs& a, int xchunk, int it0, int nsteps, cudaStr
         it += 2;
       } else {
         launch_f32(f32_kernel(false, t.tzw, t.kahan != 0), grid, f32_smem(t.kahan != 0), s, t,
-                   nullptr, 1, t.ts.count, it, nullptr);
+                   nullptr, 1, t.ts.count, it, a.queue);
         it += 1;
       }
       ++n_launch;

@@ -421,6 +421,9 @@ class _Run:
         # device step counter: lets the library replay the loop as CUDA graphs
         self.clock = torch.zeros(1, dtype=torch.int32, device=dev)
         d.clock = self.clock.data_ptr()
+        # launch-wide tile queue of this solve's step launches
+        self.queue = torch.zeros(2, dtype=torch.int32, device=dev)
+        d.queue = self.queue.data_ptr()
         self.keep = []  # tensors referenced by the descriptor
 
     def p(self):

@@ -6,9 +6,10 @@ process-wide knobs of the CUDA library set the cut (enum ``sw_tune_knob``):
 
 * ``ctas_per_sm`` — resident step CTAs per SM (1 or 2): one CTA per SM
   leaves each CTA the whole SM's bandwidth share, two hide more latency;
-* ``batch_tiles_per_cta`` — batched launches cut x into chunks so that
-  about this many tiles fall to each CTA (more tiles balance better, each
-  chunk re-reads two halo planes);
+* ``batch_tiles_per_cta`` — launches fed by a tile queue (batches, and
+  one solve whose tiles would not fill the GPU in whole waves) cut x into
+  chunks so that about this many tiles fall to each CTA (more tiles balance
+  better, each chunk re-reads two halo planes);
 * ``xchunk`` — planes per x chunk for every launch (0 = automatic);
 * ``tile_shape`` — the mixed step kernel's (z, y) tile: 0 picks, per grid,
   whichever of 64 x 8 and 32 x 16 covers the plane with fewer cells; 1 and
@@ -120,11 +121,13 @@ def _time_steps(problems, precision) -> float:
 
 
 def _candidates(n_problems):
+    """Default sweep: tile shape x tiles per CTA (batches) or x chunk (one
+    solve), at two CTAs per SM (one CTA per SM measured slower everywhere)."""
     if n_problems > 1:
-        return [dict(ctas_per_sm=c, batch_tiles_per_cta=b, xchunk=0)
-                for c, b in itertools.product((1, 2), (2, 4, 8, 16))]
-    return [dict(ctas_per_sm=c, xchunk=x, batch_tiles_per_cta=8)
-            for c, x in itertools.product((1, 2), (0, 24, 48, 96))]
+        return [dict(ctas_per_sm=2, batch_tiles_per_cta=b, xchunk=0, tile_shape=t)
+                for t, b in itertools.product((0, 1, 2), (4, 8, 16))]
+    return [dict(ctas_per_sm=2, xchunk=x, batch_tiles_per_cta=8, tile_shape=t)
+            for t, x in itertools.product((0, 1, 2), (0, 32, 64))]
 
 
 def autotune(problems, *, precision="mixed", steps=64, repeats=2, candidates=None,

@@ -6,19 +6,21 @@
 //  * A CTA owns a TZ x TY tile of the (z, y) plane and marches along x over a
 //    chunk of planes.  For every plane it needs the halo'd fields (u and d in
 //    the mixed form, u_prev and u_curr in the plain form) at x-1, x, x+1.
-//  * One elected thread streams planes into a 4-stage shared-memory ring with
-//    4-D TMA tile loads (all halo'd components of a plane in one box, or two
+//  * One elected thread streams planes into a shared-memory ring with 4-D
+//    TMA tile loads (all halo'd components of a plane in one box, or two
 //    boxes for the two FP64 buffers), completion on one mbarrier per stage.
 //    The x neighbours at x-1 come from registers (each thread keeps the centre
 //    values of the plane it computed last), so a stage is freed as soon as
-//    its plane is computed: the ring holds planes x and x+1, and planes x+2
-//    and x+3 are in flight while plane x is computed.
+//    its plane is computed: the ring holds planes x and x+1 while the next
+//    planes are in flight.
 //  * The box starts 4 (FP32) / 2 (FP64) cells before the tile in z so the
 //    innermost coordinate stays 16-byte aligned; y starts one row before.
 //    Out-of-range rows/columns are zero-filled by TMA.
-//  * Point-wise inputs (Kahan compensation, material coefficients, forces)
-//    are read straight from global memory, coalesced along z; outputs are
-//    written with coalesced stores.
+//  * Point-wise inputs (material coefficients, Kahan compensation) come by
+//    TMA too: in the mixed kernel into the stage of their plane, in the FP64
+//    kernel into a second ring.  Force patterns (push steps only) are read
+//    straight from global memory, coalesced along z; outputs are written
+//    with coalesced stores.
 // Every mbarrier wait is bounded; a timeout sets bit 1 of the solve's flag
 // word and the CTA drains its outstanding copies (bounded) and returns.
 #include <math.h>
@@ -95,18 +97,20 @@ __device__ __forceinline__ void stg2(float* p, float a, float b) {
 // One plane of the mixed step for one thread's cell pair (z, z+1) of row y:
 // 8-byte shared-memory loads and global stores serve both cells.  `o` is the
 // pair's u component-0 index in the halo box, `ob` its index in the point
-// boxes, `i` its global cell index.  The arithmetic per cell is the same
-// expression as in the direct kernel (sw_step.cu), so the results agree bit
-// for bit.  Cells outside the interior (z = 0, z >= nz-1) get 0, which is
+// boxes, `Di` its cell in the output buffer.  The arithmetic per cell is the
+// same expression as in the direct kernel (sw_step.cu), so the results agree
+// bit for bit.  Cells outside the interior (z = 0, z >= nz-1) get 0, which is
 // what the shell and padding hold in every state buffer.  Non-finite values
-// are detected once, in the finish kernel.
-template <bool VISC, bool KAHAN, int HW>
+// are detected once, in the finish kernel.  The switches are template
+// arguments, fixed per tile: viscosity, compensated sum, damping, and whether
+// this step adds force terms.
+template <bool VISC, bool KAHAN, bool DAMP, bool PUSH, int HW>
 __device__ __forceinline__ void f32_pair_plane(
     const float* __restrict__ Pc, const float* __restrict__ Pn, const float* __restrict__ Bc,
     const float* __restrict__ Bm, int o, int ob, int W, float2 (&pu)[3], float2 (&pd)[3],
-    bool act_a, bool act_b, float hx, float hy, float hz, float hc, bool use_damp, float damp,
-    const TmaF32* __restrict__ in, int j0, int j1, long long nc, long long i,
-    float* __restrict__ D, float2 (&un)[3]) {
+    bool act_a, bool act_b, float hx, float hy, float hz, float hc, float damp,
+    const TmaF32* __restrict__ in, int j0, int j1, unsigned nc, long long i,
+    float* __restrict__ Di, float2 (&un)[3]) {
   // HW: halo-box cells per component; a point box holds PT cells per component
   constexpr int PT = TmaF32::PT;
   const float2 M = lds2(Bm + ob);
@@ -127,16 +131,18 @@ __device__ __forceinline__ void f32_pair_plane(
       const float ldb = lap7f(Xd.y + pd[c].y, Nd.y + Sd.y, Rd.x + Cd.x, Cd.y, hx, hy, hz, hc);
       inca += E.x * lda;
       incb += E.y * ldb;
+      pd[c] = Cd;
     }
     pu[c] = C;
-    pd[c] = Cd;
-    for (int j = j0; j < j1; ++j) {  // push steps only
-      const float2 P = ldg2(in->pat + ((long long)in->term_pat[j] * 3 + c) * nc + i);
-      const float sc = (float)in->term_scale[j];
-      inca += P.x * sc;
-      incb += P.y * sc;
+    if (PUSH) {
+      for (int j = j0; j < j1; ++j) {
+        const float2 P = ldg2(in->pat + ((long long)in->term_pat[j] * 3 + c) * nc + i);
+        const float sc = (float)in->term_scale[j];
+        inca += P.x * sc;
+        incb += P.y * sc;
+      }
     }
-    if (use_damp) {
+    if (DAMP) {
       inca *= damp;
       incb *= damp;
     }
@@ -146,31 +152,170 @@ __device__ __forceinline__ void f32_pair_plane(
       const float ya = inca - K.x, yb = incb - K.y;
       ua = C.x + ya;
       ub = C.y + yb;
-      stg2(D + (6 + c) * nc + i, act_a ? (ua - C.x) - ya : 0.f, act_b ? (ub - C.y) - yb : 0.f);
+      stg2(Di + (size_t)(6 + c) * nc, act_a ? (ua - C.x) - ya : 0.f,
+           act_b ? (ub - C.y) - yb : 0.f);
     } else {
       ua = C.x + inca;  // the compensation planes are neither read nor written
       ub = C.y + incb;
     }
     ua = act_a ? ua : 0.f;
     ub = act_b ? ub : 0.f;
-    stg2(D + c * nc + i, ua, ub);
-    stg2(D + (3 + c) * nc + i, act_a ? inca : 0.f, act_b ? incb : 0.f);
+    stg2(Di + (size_t)c * nc, ua, ub);
+    stg2(Di + (size_t)(3 + c) * nc, act_a ? inca : 0.f, act_b ? incb : 0.f);
     un[c] = make_float2(ua, ub);
   }
 }
 
-// Ring layout of the mixed step kernel.  With room for the compensation
-// planes (KR) a point stage holds c then the coefficients and the halo ring
-// has 4 stages; without, a point stage holds the coefficients only and the
-// space goes to a fifth halo stage (three planes in flight instead of two).
+// Rings of the mixed step kernel.  Ring A has NA stages of one plane's halo'd
+// u and d; ring B has NB stages of one plane's point-wise inputs (the
+// compensation planes when the ring has room for them (KR), then the
+// material coefficients).  Without the compensation planes ring A gets a
+// fifth stage (three planes in flight instead of two).  One ring with both
+// in each stage was measured slower (more DRAM traffic, 15 % longer steps).
 template <bool KR>
 struct F32Ring {
-  static constexpr int NA = TmaF32::MIN_CTAS == 2 ? (KR ? 4 : 5) : (KR ? 5 : 6), NB = 3;
-  static constexpr int C_OFF = KR ? round128(TmaF32::C_BYTES) : 0;  // coefficients, bytes
-  static constexpr int B_STAGE = C_OFF + round128(TmaF32::M_BYTES);
-  static constexpr size_t SMEM = 128 + 256 + (size_t)NA * TmaF32::A_STAGE + (size_t)NB * B_STAGE;
+  static_assert(TmaF32::MIN_CTAS == 2, "rings sized for two resident CTAs per SM");
+  static constexpr int NA = KR ? 4 : 5, NB = 3;
+  static constexpr int STAGE = round128(TmaF32::A_BYTES_MAX);                 // ring A stage
+  static constexpr int C_OFF = 0;                                             // in a B stage
+  static constexpr int M_OFF = C_OFF + (KR ? round128(TmaF32::C_BYTES) : 0);  // coefficients
+  static constexpr int B_STAGE = M_OFF + round128(TmaF32::M_BYTES);
+  static constexpr size_t SMEM = 128 + 256 + (size_t)NA * STAGE + (size_t)NB * B_STAGE;
 };
 static_assert(F32Ring<false>::SMEM <= F32Ring<true>::SMEM, "the compact ring must not be larger");
+static_assert(2 * (F32Ring<true>::SMEM + 1024) <= 233472, "two CTAs must fit one SM");
+
+// Consumer side of the rings: where they live and the next stage of each.
+template <bool KR>
+struct F32Consumer {
+  float* ring;  // ring A, then ring B
+  WsHeader* hd;
+  volatile int* abort_flag;
+  RingPos<F32Ring<KR>::NA> a;  // next plane
+  RingPos<F32Ring<KR>::NB> b;  // next point-wise plane
+  __device__ const float* stage_a(int s) const { return ring + s * (F32Ring<KR>::STAGE / 4); }
+  __device__ const float* stage_b(int s) const {
+    return ring + F32Ring<KR>::NA * (F32Ring<KR>::STAGE / 4) + s * (F32Ring<KR>::B_STAGE / 4);
+  }
+};
+
+// One tile of the consumer warps: plane x0-1 (centres only), then planes
+// x0..x1-1, each waited for, computed and released; the closing halo plane
+// x1 is released last.  On entry q.a is the stage of plane x0-1, whose full
+// barrier the caller has waited on.  Returns false when a wait gave up.
+template <int TZW, bool KR, bool VISC, bool KAHAN, bool DAMP, bool PUSH>
+__device__ __forceinline__ bool f32_tile(const TmaF32* __restrict__ in, int local, int lit,
+                                         F32Consumer<KR>& q, int warp, int lane) {
+  constexpr int TYH = TmaF32::TZ * TmaF32::TY / TZW;
+  constexpr int CF = F32Ring<KR>::C_OFF / 4, MF = F32Ring<KR>::M_OFF / 4;
+  constexpr int HWB = TmaF32::box_cells(TZW);  // halo-box cells per component
+  constexpr int Wb = TZW + 8;                  // halo box row length
+  const Geom& g = in->g;
+  const TileCoord tc = tile_coord_t(g, in->ts, local, TZW, TYH);
+  float* __restrict__ D = in->state[(lit + 1) % 3];
+  // this thread's cells: the pair z, z+1 of tile row `row`; a warp covers
+  // one row of 32 pairs (64 x 8 tiles) or two rows of 16 (32 x 16 tiles)
+  const int row = TZW == 64 ? warp : 2 * warp + (lane >> 4);
+  const int lz = TZW == 64 ? 2 * lane : 2 * (lane & 15);
+  const int y = tc.y0 + row;
+  const bool yin = (y >= 1 && y <= g.ny - 2);
+  const int z = tc.z0 + lz;
+  const bool inrow = yin && z < g.pz;  // pz is even: the whole pair is in the row
+  const bool act_a = yin && z >= 1 && z <= g.nz - 2;
+  const bool act_b = yin && z + 1 >= 1 && z + 1 <= g.nz - 2;
+  const int j0 = PUSH ? in->term_off[lit] : 0;
+  const int j1 = PUSH ? in->term_off[lit + 1] : 0;
+  const bool snap =
+      in->snap_stride > 0 && in->snaps != nullptr && ((lit + 1) % in->snap_stride) == 0;
+  const int slot = snap ? (lit + 1) / in->snap_stride - 1 : 0;
+  const unsigned nc = (unsigned)g.ncell;  // the host keeps ncell below 2^32
+  const float damp = in->damp;
+  const float hx = in->hx, hy = in->hy, hz = in->hz, hc = lap7_centre_coef(hx, hy, hz);
+  const int o = (row + 1) * Wb + lz + 4, ob = row * TZW + lz;
+  // Plane x-1 enters only through its centre values (x neighbours of the
+  // Laplacians), which each thread keeps in registers from the plane it
+  // computed last; so a plane's stage is released as soon as the plane is
+  // computed, and the ring holds planes x and x+1 with the rest in flight.
+  float2 pu[3], pd[3];  // u and d of plane x-1 at this thread's cells
+  {
+    const float* P0 = q.stage_a(q.a.s);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      pu[c] = lds2(P0 + o + c * HWB);
+      pd[c] = VISC ? lds2(P0 + o + (3 + c) * HWB) : make_float2(0.f, 0.f);
+    }
+  }
+  __syncwarp();
+  if (lane == 0) mbar_arrive(&q.hd->emptyA[q.a.s]);
+  q.a.next();
+  int s_cur = q.a.s;
+  if (!ws_wait(&q.hd->fullA[s_cur], q.a.ph, q.abort_flag)) return false;
+  q.a.next();
+  long long i = (long long)tc.x0 * g.sxy + (long long)y * g.pz + z;
+  for (int x = tc.x0; x < tc.x1; ++x, i += g.sxy) {
+    const int s_next = q.a.s, sb = q.b.s;
+    if (!ws_wait(&q.hd->fullA[s_next], q.a.ph, q.abort_flag)) return false;
+    q.a.next();
+    if (!ws_wait(&q.hd->fullB[sb], q.b.ph, q.abort_flag)) return false;
+    q.b.next();
+    if (inrow) {
+      const float* Bs = q.stage_b(sb);
+      float2 un[3];
+      f32_pair_plane<VISC, KAHAN, DAMP, PUSH, HWB>(q.stage_a(s_cur), q.stage_a(s_next), Bs + CF,
+                                                   Bs + MF, o, ob, Wb, pu, pd, act_a, act_b, hx,
+                                                   hy, hz, hc, damp, in, j0, j1, nc, i, D + i, un);
+      if (snap) {
+        float* sp = in->snaps + ((((long long)slot * g.nx + x) * g.ny + y) * g.nz + z) * 3;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          if (act_a) sp[c] = un[c].x;
+          if (act_b) sp[3 + c] = un[c].y;
+        }
+      }
+    }
+    __syncwarp();
+    if (lane == 0) {
+      mbar_arrive(&q.hd->emptyA[s_cur]);  // plane x is done
+      mbar_arrive(&q.hd->emptyB[sb]);
+    }
+    s_cur = s_next;
+  }
+  __syncwarp();
+  if (lane == 0) mbar_arrive(&q.hd->emptyA[s_cur]);  // the closing halo plane x1
+  return true;
+}
+
+// The tile's switches, resolved once per tile into a specialised plane loop
+// (runtime branches in the plane loop cost about 15 % of its instructions).
+template <int TZW, bool KR, bool VISC, bool DAMP, bool PUSH>
+__device__ __forceinline__ bool f32_tile_k(bool kahan, const TmaF32* __restrict__ in, int local,
+                                           int lit, F32Consumer<KR>& q, int warp, int lane) {
+  if constexpr (KR) {
+    if (kahan) return f32_tile<TZW, KR, VISC, true, DAMP, PUSH>(in, local, lit, q, warp, lane);
+  }
+  return f32_tile<TZW, KR, VISC, false, DAMP, PUSH>(in, local, lit, q, warp, lane);
+}
+
+template <int TZW, bool KR, bool VISC, bool DAMP>
+__device__ __forceinline__ bool f32_tile_p(bool push, bool kahan, const TmaF32* __restrict__ in,
+                                           int local, int lit, F32Consumer<KR>& q, int warp,
+                                           int lane) {
+  if (push) return f32_tile_k<TZW, KR, VISC, DAMP, true>(kahan, in, local, lit, q, warp, lane);
+  return f32_tile_k<TZW, KR, VISC, DAMP, false>(kahan, in, local, lit, q, warp, lane);
+}
+
+template <int TZW, bool KR>
+__device__ __forceinline__ bool f32_tile_any(const TmaF32* __restrict__ in, int local, int lit,
+                                             F32Consumer<KR>& q, int warp, int lane) {
+  const bool visc = in->ncoef > 1, damp = in->use_damp != 0, kahan = KR && in->kahan != 0;
+  const bool push = in->term_off != nullptr && in->term_off[lit + 1] > in->term_off[lit];
+  if (visc) {
+    if (damp) return f32_tile_p<TZW, KR, true, true>(push, kahan, in, local, lit, q, warp, lane);
+    return f32_tile_p<TZW, KR, true, false>(push, kahan, in, local, lit, q, warp, lane);
+  }
+  if (damp) return f32_tile_p<TZW, KR, false, true>(push, kahan, in, local, lit, q, warp, lane);
+  return f32_tile_p<TZW, KR, false, false>(push, kahan, in, local, lit, q, warp, lane);
+}
 
 template <bool BATCH, int TZW, bool KR>
 __global__ void __launch_bounds__(TmaF32::THREADS, TmaF32::MIN_CTAS)
@@ -185,19 +330,18 @@ __global__ void __launch_bounds__(TmaF32::THREADS, TmaF32::MIN_CTAS)
   // for the next launch); without, tiles go in a fixed stride
   int* queue = queues;
   constexpr int NA = F32Ring<KR>::NA, NB = F32Ring<KR>::NB;
-  constexpr int HWB = TmaF32::box_cells(TZW);                   // halo-box cells per component
-  constexpr uint32_t A_BYTES = (uint32_t)HWB * 6 * 4;          // one plane's u and d
+  constexpr int HWB = TmaF32::box_cells(TZW);           // halo-box cells per component
+  constexpr uint32_t A_BYTES = (uint32_t)HWB * 6 * 4;  // one plane's u and d
   constexpr int TZ = TmaF32::TZ, TY = TmaF32::TY;
-  constexpr int AF = TmaF32::A_STAGE / 4, BF = F32Ring<KR>::B_STAGE / 4;  // floats per stage
-  constexpr int CF = F32Ring<KR>::C_OFF / 4;  // offset of the coefficients in a point stage
+  constexpr int SF = F32Ring<KR>::STAGE / 4, SFB = F32Ring<KR>::B_STAGE / 4;  // floats
+  constexpr int CF = F32Ring<KR>::C_OFF / 4, MF = F32Ring<KR>::M_OFF / 4;
   extern __shared__ unsigned char smem_raw[];
   unsigned char* base = smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u);
   WsHeader* hd = reinterpret_cast<WsHeader*>(base);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(base + kAbortFlagOffset);
-  float* ringA = reinterpret_cast<float*>(base + kRingOffset);
-  float* ringB = ringA + NA * AF;
+  float* ring = reinterpret_cast<float*>(base + kRingOffset);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  if ((smem_addr(ringA) & 127u) != 0u) {  // never issue a TMA to a misaligned destination
+  if ((smem_addr(ring) & 127u) != 0u) {  // never issue a TMA to a misaligned destination
     int* fl = BATCH ? (ninst > 0 ? tab[0].flags : nullptr) : one.flags;
     if (threadIdx.x == 0 && fl) atomicOr(fl, 4);
     queue_cta_done(queue);
@@ -241,7 +385,7 @@ __global__ void __launch_bounds__(TmaF32::THREADS, TmaF32::MIN_CTAS)
         const CUtensorMap* tma = &in->tm[lit % 3];
         const CUtensorMap* tmc = &in->tmc[lit % 3];
         const bool kahan = KR && in->kahan;  // the compact ring never carries c
-        const uint32_t bbytes = (kahan ? TmaF32::C_BYTES : 0) + TZ * TY * 4 * in->ncoef;
+        const uint32_t pbytes = (kahan ? TmaF32::C_BYTES : 0) + TZ * TY * 4 * in->ncoef;
         for (int p = tc.x0 - 1; p <= tc.x1 && !*abort_flag; ++p) {
           const int sa = pa.s;
           if (!ws_wait(&hd->emptyA[sa], pa.ph ^ 1u, abort_flag)) break;
@@ -251,15 +395,16 @@ __global__ void __launch_bounds__(TmaF32::THREADS, TmaF32::MIN_CTAS)
           }
           fence_proxy_async_smem();
           mbar_arrive_expect_tx(&hd->fullA[sa], A_BYTES);
-          tma_load_4d(ringA + sa * AF, tma, &hd->fullA[sa], tc.z0 - 4, tc.y0 - 1, p, 0);
+          tma_load_4d(ring + sa * SF, tma, &hd->fullA[sa], tc.z0 - 4, tc.y0 - 1, p, 0);
           pa.next();
-          if (p >= tc.x0 && p < tc.x1) {
+          if (p >= tc.x0 && p < tc.x1) {  // planes x0..x1-1 also need their point-wise inputs
             const int sb = pb.s;
             if (!ws_wait(&hd->emptyB[sb], pb.ph ^ 1u, abort_flag)) break;
+            float* sbp = ring + NA * SF + sb * SFB;
             fence_proxy_async_smem();
-            mbar_arrive_expect_tx(&hd->fullB[sb], bbytes);
-            if (kahan) tma_load_4d(ringB + sb * BF, tmc, &hd->fullB[sb], tc.z0, tc.y0, p, 6);
-            tma_load_4d(ringB + sb * BF + CF, &in->tmm, &hd->fullB[sb], tc.z0, tc.y0, p, 0);
+            mbar_arrive_expect_tx(&hd->fullB[sb], pbytes);
+            if (kahan) tma_load_4d(sbp + CF, tmc, &hd->fullB[sb], tc.z0, tc.y0, p, 6);
+            tma_load_4d(sbp + MF, &in->tmm, &hd->fullB[sb], tc.z0, tc.y0, p, 0);
             pb.next();
           }
         }
@@ -267,115 +412,16 @@ __global__ void __launch_bounds__(TmaF32::THREADS, TmaF32::MIN_CTAS)
     }
   } else {
     // ------------------------------- consumers ----------------------------
-    const int ly = warp;
-    RingPos<NA> ca;  // next plane to consume from ring A / ring B
-    RingPos<NB> cb;
+    F32Consumer<KR> q{ring, hd, abort_flag};
     while (true) {
       // the tile's first plane (its halo plane x0-1)
-      if (!ws_wait(&hd->fullA[ca.s], ca.ph, abort_flag)) break;
-      const int t = tile_slots(base)[ca.s];
+      if (!ws_wait(&hd->fullA[q.a.s], q.a.ph, abort_flag)) break;
+      const int t = tile_slots(base)[q.a.s];
       if (t < 0) break;
-      const TmaF32* in = BATCH ? &tab[solve_slots(base)[ca.s]] : &one;
+      const TmaF32* in = BATCH ? &tab[solve_slots(base)[q.a.s]] : &one;
       const int local = BATCH ? t - in->tile_base : t;
       const int lit = it - in->it_begin;
-      // the per-cell switches in registers: the table lives in global memory and
-      // the stores below could otherwise force reloads of its fields (fields
-      // used only on push / snapshot steps are read where they are used)
-      const Geom& g = in->g;
-      constexpr int tzw = TZW;
-      const TileCoord tc = tile_coord_t(g, in->ts, local, TZW, TYH);
-      float* __restrict__ D = in->state[(lit + 1) % 3];
-      const bool kahan = KR && in->kahan != 0, use_damp = in->use_damp != 0;
-      const float damp = in->damp;
-      // this thread's cells: the pair z, z+1 of tile row `row`; a warp covers
-      // one row of 32 pairs (64 x 8 tiles) or two rows of 16 (32 x 16 tiles)
-      const int row = tzw == 64 ? ly : 2 * ly + (lane >> 4);
-      const int lz = tzw == 64 ? 2 * lane : 2 * (lane & 15);
-      constexpr int Wb = tzw + 8;  // halo box row length
-      const int y = tc.y0 + row;
-      const bool yin = (y >= 1 && y <= g.ny - 2);
-      const int z = tc.z0 + lz;
-      const bool inrow = yin && z < g.pz;  // pz is even: the whole pair is in the row
-      const bool act_a = yin && z >= 1 && z <= g.nz - 2;
-      const bool act_b = yin && z + 1 >= 1 && z + 1 <= g.nz - 2;
-      const int j0 = in->term_off ? in->term_off[lit] : 0;
-      const int j1 = in->term_off ? in->term_off[lit + 1] : 0;
-      const bool snap =
-          in->snap_stride > 0 && in->snaps != nullptr && ((lit + 1) % in->snap_stride) == 0;
-      const int slot = snap ? (lit + 1) / in->snap_stride - 1 : 0;
-      const long long nc = g.ncell;
-      const bool visc = in->ncoef > 1;
-      const float hx = in->hx, hy = in->hy, hz = in->hz, hc = lap7_centre_coef(hx, hy, hz);
-      const int o = (row + 1) * Wb + lz + 4, ob = row * tzw + lz;
-      // Plane x-1 enters only through its centre values (x neighbours of the
-      // Laplacians), which each thread keeps in registers from the plane it
-      // computed last; so a plane's stage is released as soon as the plane is
-      // computed, and the ring holds planes x and x+1 with two more in flight.
-      float2 pu[3], pd[3];  // u and d of plane x-1 at this thread's cells
-      bool ok = true;
-      {  // plane x0-1 (waited for above): centres only
-        const float* P0 = ringA + ca.s * AF;
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          pu[c] = lds2(P0 + o + c * HWB);
-          pd[c] = lds2(P0 + o + (3 + c) * HWB);
-        }
-      }
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&hd->emptyA[ca.s]);
-      ca.next();
-      int s_cur = ca.s;
-      ok &= ws_wait(&hd->fullA[s_cur], ca.ph, abort_flag);
-      ca.next();
-      long long i = (long long)tc.x0 * g.sxy + (long long)y * g.pz + z;
-      for (int x = tc.x0; x < tc.x1 && ok; ++x, i += g.sxy) {
-        const int s_next = ca.s;
-        ok &= ws_wait(&hd->fullA[s_next], ca.ph, abort_flag);
-        ca.next();
-        const int sb = cb.s;
-        ok &= ws_wait(&hd->fullB[sb], cb.ph, abort_flag);
-        cb.next();
-        if (!ok) break;
-        if (inrow) {
-          const float* Pc = ringA + s_cur * AF;
-          const float* Pn = ringA + s_next * AF;
-          const float* Bc = ringB + sb * BF;
-          const float* Bm = Bc + CF;
-          float2 un[3];
-          if (visc) {
-            if (kahan)
-              f32_pair_plane<true, true, HWB>(Pc, Pn, Bc, Bm, o, ob, Wb, pu, pd, act_a, act_b, hx, hy, hz,
-                                         hc, use_damp, damp, in, j0, j1, nc, i, D, un);
-            else
-              f32_pair_plane<true, false, HWB>(Pc, Pn, Bc, Bm, o, ob, Wb, pu, pd, act_a, act_b, hx, hy, hz,
-                                          hc, use_damp, damp, in, j0, j1, nc, i, D, un);
-          } else {
-            if (kahan)
-              f32_pair_plane<false, true, HWB>(Pc, Pn, Bc, Bm, o, ob, Wb, pu, pd, act_a, act_b, hx, hy,
-                                          hz, hc, use_damp, damp, in, j0, j1, nc, i, D, un);
-            else
-              f32_pair_plane<false, false, HWB>(Pc, Pn, Bc, Bm, o, ob, Wb, pu, pd, act_a, act_b, hx, hy,
-                                           hz, hc, use_damp, damp, in, j0, j1, nc, i, D, un);
-          }
-          if (snap) {
-            float* sp = in->snaps + ((((long long)slot * g.nx + x) * g.ny + y) * g.nz + z) * 3;
-#pragma unroll
-            for (int c = 0; c < 3; ++c) {
-              if (act_a) sp[c] = un[c].x;
-              if (act_b) sp[3 + c] = un[c].y;
-            }
-          }
-        }
-        __syncwarp();
-        if (lane == 0) {
-          mbar_arrive(&hd->emptyA[s_cur]);  // plane x is done
-          mbar_arrive(&hd->emptyB[sb]);
-        }
-        s_cur = s_next;
-      }
-      if (!ok) break;
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&hd->emptyA[s_cur]);  // the closing halo plane x1
+      if (!f32_tile_any<TZW, KR>(in, local, lit, q, warp, lane)) break;
     }
   }
   __syncthreads();
@@ -738,6 +784,10 @@ int f32_tile_width(const Geom& g) {
 
 int make_tma_f32(const StepArgs& a, int xchunk, TmaF32* t, int tzw) {
   *t = TmaF32{};
+  if (a.g.ncell >= (1LL << 32)) {  // the kernel offsets components by a 32-bit cell count
+    set_error("grid too large for the TMA step kernel (%lld cells)", a.g.ncell);
+    return SW_ERANGE;
+  }
   t->g = a.g;
   t->tzw = tzw > 0 ? tzw : f32_tile_width(a.g);
   t->tyh = TmaF32::TZ * TmaF32::TY / t->tzw;

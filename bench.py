@@ -336,14 +336,15 @@ def run_reference(a, rank, world):
 # ---------------------------------------------------------------------------
 # serving: config-4 request stream through the continuous-batching server
 # ---------------------------------------------------------------------------
-def serving_run(n_requests: int, rate_hz: float, seed: int = 0) -> dict:
+def serving_run(n_requests: int, rate_hz: float, seed: int = 0, probs=None) -> dict:
     """Poisson arrivals of config-4 requests (log-uniform 64^3..256^3 cubes,
     1 or 4 pushes, nT 500..4000, inclusion media, HBM budget 150 GB)."""
     from shearwave_b200 import workloads as W
     from shearwave_b200.serve import ShearServer, poisson_arrivals, run_stream
 
-    rng = np.random.default_rng(1234 + seed)
-    probs = [W.problem_c4(rng) for _ in range(n_requests)]
+    if probs is None:
+        rng = np.random.default_rng(1234 + seed)
+        probs = [W.problem_c4(rng) for _ in range(n_requests)]
     arrivals = poisson_arrivals(rate_hz, n_requests, seed=seed)
     with ShearServer(hbm_budget=150e9, chunk_steps=50) as srv:
         run_stream(srv, probs, arrivals)
@@ -354,6 +355,39 @@ def serving_run(n_requests: int, rate_hz: float, seed: int = 0) -> dict:
             "cell_steps": int(sum(W.cell_steps(p) for p in probs)),
             "workload": "config-4 requests (log-uniform 64^3..256^3, 1 or 4 pushes, "
                         "nT 500..4000), Poisson arrivals, budget 150 GB, mixed form"}
+
+
+def serving_sweep(rates, n_requests: int, n_fp64: int, seed: int = 0) -> dict:
+    """The config-4 stream at several arrival rates (the same seeded requests
+    at every rate), and the first ``n_fp64`` requests solved one at a time in
+    plain FP64 (device-resident inputs, CUDA events) as the comparison."""
+    import torch
+
+    from shearwave_b200 import workloads as W
+
+    rng = np.random.default_rng(1234 + seed)
+    probs = [W.problem_c4(rng) for _ in range(n_requests)]
+    runs = [serving_run(n_requests, r, seed, probs) for r in rates]
+    out = {"rates": [{k: r[k] for k in ("rate_hz", "latency_s", "queue_s", "gcell_steps_per_s")}
+                     for r in runs],
+           "requests": n_requests, "workload": runs[0]["workload"]}
+    if n_fp64 > 0:
+        dev = torch.device("cuda", torch.cuda.current_device())
+        sample = [_to_dev(p, dev) for p in probs[:n_fp64]]
+        _solve(sample[0], "fp64", True)  # warm
+        torch.cuda.synchronize()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        for p in sample:
+            _solve(p, "fp64", True)
+        e.record()
+        torch.cuda.synchronize()
+        cs = sum(W.cell_steps(p) for p in probs[:n_fp64])
+        out["fp64_one_at_a_time"] = {
+            "value": cs / (s.elapsed_time(e) / 1e3) / 1e9, "unit": UNIT,
+            "sample": f"the first {n_fp64} requests of the stream, plain FP64 shear_fdtd "
+                      "calls one after another, inputs in HBM"}
+    return out
 
 
 # ---------------------------------------------------------------------------
@@ -375,6 +409,10 @@ def main(argv=None) -> int:
                     help="requests of the config-4 serving stream run after the timing (0: skip)")
     ap.add_argument("--serve-rate", type=float, default=4.0,
                     help="mean Poisson arrival rate of the serving stream (requests/s)")
+    ap.add_argument("--serve-sweep", default=None,
+                    help="comma-separated arrival rates (requests/s): run the serving stream "
+                         "at each rate instead of --serve-rate, plus plain-FP64 one-at-a-time "
+                         "solves of its first requests")
     ap.add_argument("--steps-per-pass", type=int, default=0, choices=[0, 1, 2],
                     help="mixed form: time steps fused per pass over HBM (0 = library default)")
     a = ap.parse_args(argv)
@@ -526,7 +564,11 @@ def main(argv=None) -> int:
                                "one warm-up step"}
 
     if rank == 0 and world == 1 and a.serve_requests > 0:
-        line["serving"] = serving_run(a.serve_requests, a.serve_rate, seed=rank)
+        if a.serve_sweep:
+            rates = [float(r) for r in a.serve_sweep.split(",")]
+            line["serving_sweep"] = serving_sweep(rates, a.serve_requests, 6, seed=rank)
+        else:
+            line["serving"] = serving_run(a.serve_requests, a.serve_rate, seed=rank)
 
     if rank == 0 and world == 1 and not a.no_cpu:
         line["cpu_baseline"] = cpu_baseline(probs)

@@ -11,10 +11,17 @@ happen between launches, so a request never waits for a whole batch to
 drain, and a solve's result is the same alone and in any mix: every cell of
 a batched launch runs the same kernel code as a solve run alone.
 
+The loop never waits for the GPU while it has work to give it: results are
+copied out on a second stream and a future resolves once its copy has
+landed, and the loop runs at most two chunks ahead of the GPU (so a new
+request joins the launches within two chunks of its admission).
+
 The queue, admission and bookkeeping are plain Python over an engine with
-six methods (footprint, admit, advance, steps, finish, release); the GPU
-engine drives the CUDA library, and the test suite drives the same loop with
-a fake engine on the CPU.
+six methods (footprint, admit, advance, steps, finish, release), plus
+optional ones for asynchronous completion (finish_begin, finish_ready,
+finish_end) and run-ahead control (mark, wait_mark); the GPU engine drives
+the CUDA library, and the test suite drives the same loop with a fake
+engine on the CPU.
 """
 
 from __future__ import annotations
@@ -42,7 +49,7 @@ def latency_percentiles(lat_s) -> dict:
 
 class _Request:
     __slots__ = ("problem", "future", "t_arrive", "t_admit", "t_done", "footprint", "handle",
-                 "begin", "rid")
+                 "begin", "rid", "token")
 
     def __init__(self, problem, rid):
         self.problem = problem
@@ -54,6 +61,7 @@ class _Request:
         self.handle = None
         self.begin = 0
         self.rid = rid
+        self.token = None
 
 
 class GpuEngine:
@@ -71,6 +79,7 @@ class GpuEngine:
         self.precision = precision
         self.return_device = return_device
         self.stream = torch.cuda.Stream(device=self.dev)
+        self.copy_stream = torch.cuda.Stream(device=self.dev)
 
     # -- sizes -------------------------------------------------------------
     @staticmethod
@@ -151,6 +160,30 @@ class GpuEngine:
         with self.torch.cuda.stream(self.stream):
             return handle.finish(self.return_device)
 
+    def finish_begin(self, handle):
+        """Enqueue the output conversion and the copies to the host (on the
+        copy stream); returns the token finish_end turns into the result."""
+        with self.torch.cuda.stream(self.stream):
+            return handle.finish_enqueue(self.return_device, self.copy_stream)
+
+    @staticmethod
+    def finish_ready(token) -> bool:
+        return token["event"].query()
+
+    def finish_end(self, handle, token):
+        with self.torch.cuda.stream(self.stream):
+            return handle.finish_collect(token)
+
+    def mark(self):
+        """An event after the work enqueued so far."""
+        ev = self.torch.cuda.Event()
+        ev.record(self.stream)
+        return ev
+
+    @staticmethod
+    def wait_mark(ev):
+        ev.synchronize()
+
     @staticmethod
     def release(handle):
         del handle
@@ -173,6 +206,8 @@ class ShearServer:
         self.chunk_steps = int(chunk_steps)
         self._pending = collections.deque()
         self._active = []
+        self._finishing = []  # results being copied out
+        self._marks = collections.deque()  # one event per chunk in flight
         self._cv = threading.Condition()
         self._stop = False
         self._thread = None
@@ -247,25 +282,32 @@ class ShearServer:
                 self.engine.on_thread_start()
             while True:
                 with self._cv:
-                    while not self._stop and not self._pending and not self._active:
+                    while (not self._stop and not self._pending and not self._active
+                           and not self._finishing):
                         self._cv.wait(timeout=0.05)
-                    if self._stop and not self._pending and not self._active:
+                    if (self._stop and not self._pending and not self._active
+                            and not self._finishing):
                         return
                 self._admit()
                 if not self._active:
+                    self._collect(block=True)  # nothing left to overlap the copies with
+                    if self._pending and not self._finishing:
+                        time.sleep(0.001)  # waiting on memory held by no one: retry
                     continue
                 t0 = time.perf_counter()
                 self._advance()
                 self._complete()
+                self._collect(block=False)
                 self.busy_s += time.perf_counter() - t0
         except BaseException as e:  # surface engine failures to every waiter
             self._error = e
             with self._cv:
-                for r in list(self._pending) + self._active:
+                for r in list(self._pending) + self._active + self._finishing:
                     if not r.future.done():
                         r.future.set_exception(e)
                 self._pending.clear()
                 self._active = []
+                self._finishing = []
 
     def _admit(self):
         while True:
@@ -298,6 +340,10 @@ class ShearServer:
         self.engine.advance([r.handle for r in self._active], [r.begin for r in self._active],
                             self._clock, n)
         self._clock += n
+        if hasattr(self.engine, "mark"):  # stay at most two chunks ahead of the GPU
+            self._marks.append(self.engine.mark())
+            while len(self._marks) > 2:
+                self.engine.wait_mark(self._marks.popleft())
 
     def _complete(self):
         keep = []
@@ -305,15 +351,33 @@ class ShearServer:
             if self._clock - r.begin < self.engine.steps(r.handle):
                 keep.append(r)
                 continue
-            result = self.engine.finish(r.handle)
-            r.t_done = time.perf_counter()
-            cells = _cell_steps(r.problem)
-            self.completed.append((r.rid, r.t_done - r.t_arrive, r.t_admit - r.t_arrive, cells))
-            self.engine.release(r.handle)
-            r.handle = None
-            self._used -= r.footprint
-            r.future.set_result(result)
+            if hasattr(self.engine, "finish_begin"):
+                r.token = self.engine.finish_begin(r.handle)
+                self._finishing.append(r)
+            else:
+                self._resolve(r, self.engine.finish(r.handle))
         self._active = keep
+
+    def _collect(self, block: bool):
+        """Resolve the requests whose results have reached the host (all of
+        them when ``block``)."""
+        left = []
+        for r in self._finishing:
+            if block or self.engine.finish_ready(r.token):
+                self._resolve(r, self.engine.finish_end(r.handle, r.token))
+            else:
+                left.append(r)
+        self._finishing = left
+
+    def _resolve(self, r, result):
+        r.t_done = time.perf_counter()
+        cells = _cell_steps(r.problem)
+        self.completed.append((r.rid, r.t_done - r.t_arrive, r.t_admit - r.t_arrive, cells))
+        self.engine.release(r.handle)
+        r.handle = None
+        r.token = None
+        self._used -= r.footprint  # the request's memory returns to the budget
+        r.future.set_result(result)
 
 
 def _cell_steps(p) -> int:

@@ -674,7 +674,9 @@ class _Solve:
         flag = torch.empty(1, dtype=torch.int32, pin_memory=True)
         if return_device:
             flag.copy_(run.flags, non_blocking=True)
-            return {"outs": outs, "flag": flag, "event": None, "device": True}
+            ev = torch.cuda.Event()
+            ev.record()
+            return {"outs": outs, "flag": flag, "event": ev, "device": True}
         done = torch.cuda.Event()
         done.record()
         cs = copy_stream if copy_stream is not None else torch.cuda.current_stream()
@@ -693,10 +695,7 @@ class _Solve:
 
     def finish_collect(self, handle):
         """Wait for a finish_enqueue handle and return the solve's result."""
-        if handle["event"] is not None:
-            handle["event"].synchronize()
-        else:
-            torch.cuda.current_stream().synchronize()
+        handle["event"].synchronize()
         nonfinite = bool(int(handle["flag"][0]))
         if self.info is not None:
             tev = self.tev

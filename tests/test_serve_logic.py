@@ -62,6 +62,49 @@ class FakeEngine:
             del self.live[h["id"]]
 
 
+class AsyncFakeEngine(FakeEngine):
+    """Completion in the background, as on the GPU: a result becomes ready
+    `copy_time` after finish_begin, and `mark` events complete `mark_time`
+    after they are made; the engine records how far the loop runs ahead."""
+
+    def __init__(self, step_time=0.0, copy_time=0.01, mark_time=0.003):
+        super().__init__(step_time)
+        self.copy_time = copy_time
+        self.mark_time = mark_time
+        self.ended = []
+        self.outstanding = 0
+        self.max_outstanding = 0
+
+    def finish_begin(self, h):
+        assert h["done"] == h["n"]
+        return {"id": h["id"], "ready_at": time.perf_counter() + self.copy_time}
+
+    @staticmethod
+    def finish_ready(token):
+        return time.perf_counter() >= token["ready_at"]
+
+    def finish_end(self, h, token):
+        dt = token["ready_at"] - time.perf_counter()
+        if dt > 0:
+            time.sleep(dt)
+        self.ended.append(token["id"])
+        return ("result", h["id"])
+
+    def mark(self):
+        self.outstanding += 1
+        self.max_outstanding = max(self.max_outstanding, self.outstanding)
+        return time.perf_counter() + self.mark_time
+
+    def wait_mark(self, t):
+        dt = t - time.perf_counter()
+        if dt > 0:
+            time.sleep(dt)
+        self.outstanding -= 1
+
+
+ENGINES = [FakeEngine, AsyncFakeEngine]
+
+
 class _Arr:
     shape = (8, 8, 8)
 
@@ -70,8 +113,9 @@ def _req(i, n_steps=10, fp=1, **kw):
     return dict(bx=None, by=None, bz=_Arr(), n_steps=n_steps, id=i, fp=fp, **kw)
 
 
-def test_all_requests_complete_with_their_own_results():
-    eng = FakeEngine()
+@pytest.mark.parametrize("engine", ENGINES)
+def test_all_requests_complete_with_their_own_results(engine):
+    eng = engine()
     with ShearServer(eng, hbm_budget=100, chunk_steps=4) as srv:
         futs = [srv.submit(_req(i, n_steps=5 + 3 * i)) for i in range(6)]
         res = [f.result(timeout=10) for f in futs]
@@ -81,8 +125,9 @@ def test_all_requests_complete_with_their_own_results():
     assert st["latency_s"]["p99"] >= st["latency_s"]["p50"] >= 0
 
 
-def test_admission_respects_the_memory_budget():
-    eng = FakeEngine()
+@pytest.mark.parametrize("engine", ENGINES)
+def test_admission_respects_the_memory_budget(engine):
+    eng = engine()
     with ShearServer(eng, hbm_budget=10, chunk_steps=2) as srv:
         futs = [srv.submit(_req(i, n_steps=6, fp=4)) for i in range(5)]
         for f in futs:
@@ -104,8 +149,9 @@ def test_malformed_request_raises_before_queueing():
         srv.submit(dict(bx=None, by=None, bz=None, n_steps=3))
 
 
-def test_failures_stay_with_their_request():
-    eng = FakeEngine()
+@pytest.mark.parametrize("engine", ENGINES)
+def test_failures_stay_with_their_request(engine):
+    eng = engine()
     with ShearServer(eng, hbm_budget=100, chunk_steps=3) as srv:
         ok1 = srv.submit(_req(0))
         oom = srv.submit(_req(1, oom=True))
@@ -149,3 +195,17 @@ def test_latency_percentiles():
     p = latency_percentiles([0.1, 0.2, 0.3, 0.4])
     assert abs(p["p50"] - 0.25) < 1e-12 and p["n"] == 4
     assert latency_percentiles([])["p99"] is None
+
+
+def test_async_completion_resolves_each_request_once_and_bounds_run_ahead():
+    """Results are copied out while later chunks run; every request is
+    resolved exactly once, and the loop is never more than two chunks (plus
+    the one being enqueued) ahead of the device."""
+    eng = AsyncFakeEngine(step_time=0.0005, copy_time=0.02)
+    with ShearServer(eng, hbm_budget=100, chunk_steps=3) as srv:
+        futs = [srv.submit(_req(i, n_steps=4 + 5 * (i % 3))) for i in range(9)]
+        res = [f.result(timeout=10) for f in futs]
+    assert res == [("result", i) for i in range(9)]
+    assert sorted(eng.ended) == list(range(9))
+    assert eng.max_outstanding <= 3
+    assert srv.stats()["completed"] == 9

@@ -474,7 +474,7 @@ def main(argv=None) -> int:
     # launches one kernel per pair of time steps (one per single step at an
     # odd end); a batched run covers all running solves in each launch.
     # achieved = algorithmic bytes of the launches / their device time.
-    spl = 2 if a.steps_per_pass == 2 else 1
+    spl = 1 if a.steps_per_pass == 1 else 2  # the library fuses step pairs by default
     if len(probs) > 1:
         step_ms = max(i["t_steps_ms"] for i in infos)
         steps_total = max(p["n_steps"] for p in probs)
@@ -490,7 +490,7 @@ def main(argv=None) -> int:
     per_launch_ms = step_ms / launches_step
     achieved = alg_bytes / (step_ms / 1e3) / 1e9
     peak, peak_kind = measured_hbm()
-    bpcs = ncu_bytes_per_cell_step("step_f32_tma")
+    bpcs = ncu_bytes_per_cell_step("step_f32_fused2" if spl == 2 else "step_f32_tma")
     cells_per_launch = sum(math.prod(_shape(p)) * p["n_steps"] for p in probs) / launches_step
     traffic = None if bpcs is None else bpcs * cells_per_launch
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

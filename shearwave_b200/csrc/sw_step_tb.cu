@@ -88,16 +88,18 @@ __device__ __forceinline__ void tb_st2(float* p, float a, float b) {
 // before it in (pu, pd).  Writes the new u and the increment of each
 // component to `out + c * ocs` and `out + (3 + c) * ocs` (inactive cells:
 // 0) and, when `snap` is set, the new u of active cells to snap[3 c'] of the
-// AoS snapshot.  (pu, pd) become this plane's centres.
-template <bool VISC, int RS, int CS>
+// AoS snapshot.  (pu, pd) become this plane's centres.  The switches are
+// template arguments fixed per tile: viscosity, damping, whether the pair of
+// steps adds force terms, whether it writes a snapshot.
+template <bool VISC, bool DAMP, bool PUSH, bool SNAP, int RS, int CS>
 __device__ __forceinline__ void tb_pair_step(const float* __restrict__ P,
                                              const float* __restrict__ Pn, int o, float2 M,
                                              float2 E, float2 (&pu)[3], float2 (&pd)[3],
                                              bool act_a, bool act_b, float hx, float hy, float hz,
-                                             float hc, bool use_damp, float damp,
+                                             float hc, float damp,
                                              const TmaF32TB* __restrict__ in, int j0, int j1,
-                                             long long nc, long long i, float* __restrict__ out,
-                                             long long ocs, float* __restrict__ snap) {
+                                             unsigned nc, long long i, float* __restrict__ out,
+                                             unsigned ocs, float* __restrict__ snap) {
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
     const int oc = o + c * CS, od = oc + 3 * CS;
@@ -114,28 +116,230 @@ __device__ __forceinline__ void tb_pair_step(const float* __restrict__ P,
       const float ldb = lap7f(Xd.y + pd[c].y, Nd.y + Sd.y, Rd.x + Cd.x, Cd.y, hx, hy, hz, hc);
       inca += E.x * lda;
       incb += E.y * ldb;
+      pd[c] = Cd;
     }
     pu[c] = C;
-    pd[c] = Cd;
-    for (int j = j0; j < j1; ++j) {  // push steps only
-      const float2 Pt = __ldg(reinterpret_cast<const float2*>(
-          in->pat + ((long long)in->term_pat[j] * 3 + c) * nc + i));
-      const float sc = (float)in->term_scale[j];
-      inca += Pt.x * sc;
-      incb += Pt.y * sc;
+    if (PUSH) {
+      for (int j = j0; j < j1; ++j) {
+        const float2 Pt = __ldg(reinterpret_cast<const float2*>(
+            in->pat + ((long long)in->term_pat[j] * 3 + c) * nc + i));
+        const float sc = (float)in->term_scale[j];
+        inca += Pt.x * sc;
+        incb += Pt.y * sc;
+      }
     }
-    if (use_damp) {
+    if (DAMP) {
       inca *= damp;
       incb *= damp;
     }
     const float ua = C.x + inca, ub = C.y + incb;
-    tb_st2(out + c * ocs, act_a ? ua : 0.f, act_b ? ub : 0.f);
-    tb_st2(out + (3 + c) * ocs, act_a ? inca : 0.f, act_b ? incb : 0.f);
-    if (snap != nullptr) {
+    tb_st2(out + (size_t)c * ocs, act_a ? ua : 0.f, act_b ? ub : 0.f);
+    tb_st2(out + (size_t)(3 + c) * ocs, act_a ? inca : 0.f, act_b ? incb : 0.f);
+    if (SNAP && snap != nullptr) {
       if (act_a) snap[c] = ua;
       if (act_b) snap[3 + c] = ub;
     }
   }
+}
+
+// Where the two-step kernel's rings and barriers live.
+struct TbRings {
+  float* ringA;
+  float* ringB;
+  float* ringL;
+  WsHeader* hd;
+  uint64_t* Lfull;
+  uint64_t* Lempty;
+  volatile int* abort_flag;
+};
+
+// A consumer warp's next stage of each ring (level-0 planes, point-wise
+// planes, level-1 slots), and whether its waits have all succeeded.
+struct TbPos {
+  RingPos<TmaF32TB::NA> ca;
+  RingPos<TmaF32TB::NB> cb;
+  RingPos<TmaF32TB::NL> lw;
+  bool ok = true;
+};
+
+// One tile of a consumer warp (level-1 row w): the tile's first plane x0-2
+// (centres only; its full barrier waited on by the caller), then for every
+// plane q = x0-1 .. x1 level 1 at q and level 2 at q-1.  Returns the ring
+// positions after the tile, with ok = false when a wait gave up.
+template <bool VISC, bool DAMP, bool PUSH, bool SNAP>
+__device__ __forceinline__ TbPos tb_tile(const TmaF32TB* __restrict__ in, int local, int lit,
+                                         const TbRings& k, TbPos p, int w, int lane) {
+  using T = TmaF32TB;
+  constexpr int W = T::W, H = T::H, WB = T::WB, HB = T::HB, LZ = T::LZ;
+  constexpr int AF = T::A_STAGE / 4, BF = T::B_STAGE / 4, LF = T::L_STAGE / 4;
+  constexpr int LP = LZ * T::LY;  // level-1 cells per component
+  const Geom& g = in->g;
+  const TbCoord tc = tb_coord(g, in->ts, local);
+  float* __restrict__ D = in->state[(lit + 2) % 3];
+  const unsigned nc = (unsigned)g.ncell;  // the host keeps ncell below 2^32
+  const float damp = in->damp;
+  const float hx = in->hx, hy = in->hy, hz = in->hz, hc = lap7_centre_coef(hx, hy, hz);
+  // this thread: level-1 row w (y = y0-1+w), z pair zp, zp+1 (zp = z0-2+2 lane)
+  const int y = tc.y0 - 1 + w, zp = tc.z0 - 2 + 2 * lane;
+  const bool yin = y >= 1 && y <= g.ny - 2;
+  const bool zin_a = zp >= 1 && zp <= g.nz - 2, zin_b = zp + 1 >= 1 && zp + 1 <= g.nz - 2;
+  // level 2: rows 1..OY and pairs 1..30 are the output tile
+  const bool out_rc = w >= 1 && w <= T::OY && lane >= 1 && lane <= 30;
+  const bool store = out_rc && yin && zp < g.pz;  // pz is even: the pair is in the row
+  const int o = (w + 1) * W + 2 + 2 * lane, ob = w * WB + 2 + 2 * lane, ol = w * LZ + 2 * lane;
+  const int j10 = PUSH ? in->term_off[lit] : 0;
+  const int j11 = PUSH ? in->term_off[lit + 1] : 0;
+  const int j21 = PUSH ? in->term_off[lit + 2] : 0;
+  const bool snap1 = SNAP && ((lit + 1) % in->snap_stride) == 0;
+  const bool snap2 = SNAP && ((lit + 2) % in->snap_stride) == 0;
+  const int slot1 = snap1 ? (lit + 1) / in->snap_stride - 1 : 0;
+  const int slot2 = snap2 ? (lit + 2) / in->snap_stride - 1 : 0;
+  float2 pu[3], pd[3];  // level-0 centres of the plane before
+  float2 qu[3], qd[3];  // level-1 centres of the plane before
+  float2 Mp = make_float2(0.f, 0.f), Ep = Mp;  // coefficients of the previous plane
+  {
+    const float* P0 = k.ringA + p.ca.s * AF;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      pu[c] = tb_ld2(P0 + o + c * H * W);
+      pd[c] = VISC ? tb_ld2(P0 + o + (3 + c) * H * W) : make_float2(0.f, 0.f);
+      qu[c] = qd[c] = make_float2(0.f, 0.f);
+    }
+  }
+  __syncwarp();
+  if (lane == 0) mbar_arrive(&k.hd->emptyA[p.ca.s]);
+  p.ca.next();
+  RingPos<T::NA> cur = p.ca;  // plane q
+  if (!ws_wait(&k.hd->fullA[cur.s], cur.ph, k.abort_flag)) {
+      p.ok = false;
+      return p;
+    }
+  p.ca.next();
+  RingPos<T::NL> lprev = p.lw;  // slot of level-1 plane q-1 (meaningful from q = x0)
+  for (int q = tc.x0 - 1; q <= tc.x1; ++q) {
+    const RingPos<T::NA> nxt = p.ca;  // plane q+1
+    if (!ws_wait(&k.hd->fullA[nxt.s], nxt.ph, k.abort_flag)) {
+      p.ok = false;
+      return p;
+    }
+    p.ca.next();
+    const RingPos<T::NB> pt = p.cb;
+    if (!ws_wait(&k.hd->fullB[pt.s], pt.ph, k.abort_flag)) {
+      p.ok = false;
+      return p;
+    }
+    p.cb.next();
+    // the slot is free once every warp has read what it held before
+    if (!ws_wait(&k.Lempty[p.lw.s], p.lw.ph ^ 1u, k.abort_flag)) {
+      p.ok = false;
+      return p;
+    }
+    float* Lw = k.ringL + p.lw.s * LF;
+    // ---- level 1: step lit+1 at plane q on the level-1 region ----
+    const float* Bm = k.ringB + pt.s * BF;
+    const float2 Mc = tb_ld2(Bm + ob);
+    const float2 Ec = VISC ? tb_ld2(Bm + HB * WB + ob) : make_float2(0.f, 0.f);
+    {
+      const bool xin = q >= 1 && q <= g.nx - 2;
+      const bool aa = xin && yin && zin_a, ab = xin && yin && zin_b;
+      long long i = 0;  // the pair's cell, for the force patterns
+      int jl0 = 0, jl1 = 0;
+      if (PUSH) {
+        i = (long long)min(max(q, 0), g.nx - 1) * g.sxy +
+            (long long)min(max(y, 0), g.ny - 1) * g.pz + max(zp, 0);
+        jl0 = (aa || ab) ? j10 : 0;
+        jl1 = (aa || ab) ? j11 : 0;
+      }
+      float* sp = nullptr;
+      if (SNAP && snap1 && store && q >= tc.x0 && q < tc.x1)
+        sp = in->snaps + ((((long long)slot1 * g.nx + q) * g.ny + y) * g.nz + zp) * 3;
+      tb_pair_step<VISC, DAMP, PUSH, SNAP, W, H * W>(
+          k.ringA + cur.s * AF, k.ringA + nxt.s * AF, o, Mc, Ec, pu, pd, aa, ab, hx, hy, hz, hc,
+          damp, in, jl0, jl1, nc, i, Lw + ol, (unsigned)LP, sp);
+    }
+    __syncwarp();
+    if (lane == 0) {
+      mbar_arrive(&k.hd->emptyA[cur.s]);  // level-0 plane q is no longer needed
+      mbar_arrive(&k.hd->emptyB[pt.s]);
+      mbar_arrive(&k.Lfull[p.lw.s]);      // this warp's row of level-1 plane q is written
+    }
+    if (q >= tc.x0) {
+      const float* Lc = k.ringL + lprev.s * LF;  // level-1 plane q-1
+      if (q == tc.x0) {  // level-1 centres of plane x0-1 (own pair) for the first level 2
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          qu[c] = tb_ld2(Lc + ol + c * LP);
+          qd[c] = VISC ? tb_ld2(Lc + ol + (3 + c) * LP) : make_float2(0.f, 0.f);
+        }
+      } else {
+        // ---- level 2: step lit+2 at plane x = q-1 on the output tile ----
+        // (reads rows w-1..w+1 of plane q-1: wait until every warp wrote it)
+        if (!ws_wait(&k.Lfull[lprev.s], lprev.ph, k.abort_flag)) {
+      p.ok = false;
+      return p;
+    }
+        if (store) {
+          const int x = q - 1;
+          const long long i = (long long)x * g.sxy + (long long)y * g.pz + zp;
+          float* sp = nullptr;
+          if (SNAP && snap2)
+            sp = in->snaps + ((((long long)slot2 * g.nx + x) * g.ny + y) * g.nz + zp) * 3;
+          tb_pair_step<VISC, DAMP, PUSH, SNAP, LZ, LP>(Lc, Lw, ol, Mp, Ep, qu, qd, zin_a, zin_b,
+                                                       hx, hy, hz, hc, damp, in, j11, j21, nc, i,
+                                                       D + i, nc, sp);
+        }
+      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&k.Lempty[lprev.s]);  // this warp is done with plane q-1
+    }
+    Mp = Mc;
+    Ep = Ec;
+    lprev = p.lw;
+    p.lw.next();
+    cur = nxt;
+  }
+  __syncwarp();
+  if (lane == 0) {
+    mbar_arrive(&k.hd->emptyA[cur.s]);  // the closing halo plane x1+1
+    mbar_arrive(&k.Lempty[lprev.s]);    // the tile's last level-1 plane x1
+  }
+  return p;
+}
+
+// Tiles of push or snapshot steps (a few steps of a run) go through a
+// function of their own, so that their extra live values do not raise the
+// register pressure of the loop every other tile runs.
+template <bool VISC, bool DAMP, bool PUSH, bool SNAP>
+__device__ __noinline__ TbPos tb_tile_rare(const TmaF32TB* __restrict__ in, int local, int lit,
+                                           TbRings k, TbPos p, int w, int lane) {
+  return tb_tile<VISC, DAMP, PUSH, SNAP>(in, local, lit, k, p, w, lane);
+}
+
+// The tile's switches, resolved once per tile into a specialised loop.
+template <bool VISC, bool DAMP>
+__device__ __forceinline__ TbPos tb_tile_ps(bool push, bool snap, const TmaF32TB* __restrict__ in,
+                                            int local, int lit, const TbRings& k, TbPos p, int w,
+                                            int lane) {
+  if (push) {
+    if (snap) return tb_tile_rare<VISC, DAMP, true, true>(in, local, lit, k, p, w, lane);
+    return tb_tile_rare<VISC, DAMP, true, false>(in, local, lit, k, p, w, lane);
+  }
+  if (snap) return tb_tile_rare<VISC, DAMP, false, true>(in, local, lit, k, p, w, lane);
+  return tb_tile<VISC, DAMP, false, false>(in, local, lit, k, p, w, lane);
+}
+
+__device__ __forceinline__ TbPos tb_tile_any(const TmaF32TB* __restrict__ in, int local, int lit,
+                                             const TbRings& k, TbPos p, int w, int lane) {
+  const bool visc = in->ncoef > 1, damp = in->use_damp != 0;
+  const bool push = in->term_off != nullptr && in->term_off[lit + 2] > in->term_off[lit];
+  const bool snap = in->snap_stride > 0 && in->snaps != nullptr &&
+                    (((lit + 1) % in->snap_stride) == 0 || ((lit + 2) % in->snap_stride) == 0);
+  if (visc) {
+    if (damp) return tb_tile_ps<true, true>(push, snap, in, local, lit, k, p, w, lane);
+    return tb_tile_ps<true, false>(push, snap, in, local, lit, k, p, w, lane);
+  }
+  if (damp) return tb_tile_ps<false, true>(push, snap, in, local, lit, k, p, w, lane);
+  return tb_tile_ps<false, false>(push, snap, in, local, lit, k, p, w, lane);
 }
 
 template <bool BATCH>
@@ -146,10 +350,8 @@ __global__ void __launch_bounds__(TmaF32TB::THREADS, 1)
   // batched launches take tiles from a launch-wide queue (see step_f32_tma)
   int* queue = queues;
   using T = TmaF32TB;
-  constexpr int NA = T::NA, NB = T::NB, NL = T::NL, W = T::W, H = T::H, WB = T::WB, HB = T::HB;
-  constexpr int LZ = T::LZ, LY = T::LY, NC = T::CONSUMER_WARPS * 32;
+  constexpr int NA = T::NA, NB = T::NB, NL = T::NL, WB = T::WB, HB = T::HB;
   constexpr int AF = T::A_STAGE / 4, BF = T::B_STAGE / 4, LF = T::L_STAGE / 4;
-  constexpr int LP = LZ * LY;  // level-1 cells per component
   extern __shared__ unsigned char smem_raw[];
   unsigned char* base = smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u);
   WsHeader* hd = reinterpret_cast<WsHeader*>(base);
@@ -245,145 +447,18 @@ __global__ void __launch_bounds__(TmaF32TB::THREADS, 1)
     }
   } else {
     // ------------------------------- consumers ----------------------------
-    const int w = warp;
-    RingPos<NA> ca;  // next level-0 plane to consume
-    RingPos<NB> cb;  // next point plane
-    RingPos<NL> lw;  // slot of the next level-1 plane
+    const TbRings k{ringA, ringB, ringL, hd, Lfull, Lempty, abort_flag};
+    TbPos p;
     while (true) {
       // the tile's first plane, x0-2: centres only
-      if (!ws_wait(&hd->fullA[ca.s], ca.ph, abort_flag)) break;
-      const int t = tile_slots(base)[ca.s];
+      if (!ws_wait(&hd->fullA[p.ca.s], p.ca.ph, abort_flag)) break;
+      const int t = tile_slots(base)[p.ca.s];
       if (t < 0) break;
-      const T* in = BATCH ? &tab[solve_slots(base)[ca.s]] : &one;
+      const T* in = BATCH ? &tab[solve_slots(base)[p.ca.s]] : &one;
       const int local = BATCH ? t - in->tile_base : t;
       const int lit = it - in->it_begin;
-      const Geom& g = in->g;
-      const TbCoord tc = tb_coord(g, in->ts, local);
-      float* __restrict__ D = in->state[(lit + 2) % 3];
-      const long long nc = g.ncell;
-      const bool use_damp = in->use_damp != 0, visc = in->ncoef > 1;
-      const float damp = in->damp;
-      const float hx = in->hx, hy = in->hy, hz = in->hz, hc = lap7_centre_coef(hx, hy, hz);
-      // this thread: level-1 row w (y = y0-1+w), z pair zp, zp+1 (zp = z0-2+2 lane)
-      const int y = tc.y0 - 1 + w, zp = tc.z0 - 2 + 2 * lane;
-      const bool yin = y >= 1 && y <= g.ny - 2;
-      const bool zin_a = zp >= 1 && zp <= g.nz - 2, zin_b = zp + 1 >= 1 && zp + 1 <= g.nz - 2;
-      // level 2: rows 1..OY and pairs 1..30 are the output tile
-      const bool out_rc = w >= 1 && w <= T::OY && lane >= 1 && lane <= 30;
-      const bool store = out_rc && yin && zp < g.pz;  // pz is even: the pair is in the row
-      const int o = (w + 1) * W + 2 + 2 * lane, ob = w * WB + 2 + 2 * lane, ol = w * LZ + 2 * lane;
-      const int j10 = in->term_off ? in->term_off[lit] : 0;
-      const int j11 = in->term_off ? in->term_off[lit + 1] : 0;
-      const int j20 = j11;
-      const int j21 = in->term_off ? in->term_off[lit + 2] : 0;
-      const bool snap1 =
-          in->snap_stride > 0 && in->snaps != nullptr && ((lit + 1) % in->snap_stride) == 0;
-      const bool snap2 =
-          in->snap_stride > 0 && in->snaps != nullptr && ((lit + 2) % in->snap_stride) == 0;
-      const int slot1 = snap1 ? (lit + 1) / in->snap_stride - 1 : 0;
-      const int slot2 = snap2 ? (lit + 2) / in->snap_stride - 1 : 0;
-      float2 pu[3], pd[3];  // level-0 centres of the plane before
-      float2 qu[3], qd[3];  // level-1 centres of the plane before
-      float2 Mp = make_float2(0.f, 0.f), Ep = Mp;  // coefficients of the previous plane
-      {
-        const float* P0 = ringA + ca.s * AF;
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          pu[c] = tb_ld2(P0 + o + c * H * W);
-          pd[c] = tb_ld2(P0 + o + (3 + c) * H * W);
-          qu[c] = qd[c] = make_float2(0.f, 0.f);
-        }
-      }
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&hd->emptyA[ca.s]);
-      ca.next();
-      RingPos<NA> cur = ca;  // plane q
-      bool ok = ws_wait(&hd->fullA[cur.s], cur.ph, abort_flag);
-      ca.next();
-      RingPos<NL> lprev = lw;  // slot of level-1 plane q-1 (meaningful from q = x0)
-      for (int q = tc.x0 - 1; q <= tc.x1 && ok; ++q) {
-        const RingPos<NA> nxt = ca;  // plane q+1
-        ok = ok && ws_wait(&hd->fullA[nxt.s], nxt.ph, abort_flag);
-        ca.next();
-        const RingPos<NB> pt = cb;
-        ok = ok && ws_wait(&hd->fullB[pt.s], pt.ph, abort_flag);
-        cb.next();
-        // the slot is free once every warp has read what it held before
-        ok = ok && ws_wait(&Lempty[lw.s], lw.ph ^ 1u, abort_flag);
-        if (!ok) break;
-        float* Lw = ringL + lw.s * LF;
-        // ---- level 1: step lit+1 at plane q on the level-1 region ----
-        const float* Bm = ringB + pt.s * BF;
-        const float2 Mc = tb_ld2(Bm + ob);
-        const float2 Ec = visc ? tb_ld2(Bm + HB * WB + ob) : make_float2(0.f, 0.f);
-        {
-          const float* Pc = ringA + cur.s * AF;
-          const float* Pn = ringA + nxt.s * AF;
-          const bool xin = q >= 1 && q <= g.nx - 2;
-          const bool aa = xin && yin && zin_a, ab = xin && yin && zin_b;
-          const long long i = (long long)min(max(q, 0), g.nx - 1) * g.sxy +
-                              (long long)min(max(y, 0), g.ny - 1) * g.pz + max(zp, 0);
-          const int jl0 = (aa || ab) ? j10 : 0, jl1 = (aa || ab) ? j11 : 0;
-          float* sp = (snap1 && store && q >= tc.x0 && q < tc.x1)
-                          ? in->snaps + ((((long long)slot1 * g.nx + q) * g.ny + y) * g.nz + zp) * 3
-                          : nullptr;
-          if (visc)
-            tb_pair_step<true, W, H * W>(Pc, Pn, o, Mc, Ec, pu, pd, aa, ab, hx, hy, hz, hc,
-                                         use_damp, damp, in, jl0, jl1, nc, i, Lw + ol, LP, sp);
-          else
-            tb_pair_step<false, W, H * W>(Pc, Pn, o, Mc, Ec, pu, pd, aa, ab, hx, hy, hz, hc,
-                                          use_damp, damp, in, jl0, jl1, nc, i, Lw + ol, LP, sp);
-        }
-        __syncwarp();
-        if (lane == 0) {
-          mbar_arrive(&hd->emptyA[cur.s]);  // level-0 plane q is no longer needed
-          mbar_arrive(&hd->emptyB[pt.s]);
-          mbar_arrive(&Lfull[lw.s]);        // this warp's row of level-1 plane q is written
-        }
-        if (q >= tc.x0) {
-          const float* Lc = ringL + lprev.s * LF;  // level-1 plane q-1
-          if (q == tc.x0) {  // level-1 centres of plane x0-1 (own pair) for the first level 2
-#pragma unroll
-            for (int c = 0; c < 3; ++c) {
-              qu[c] = tb_ld2(Lc + ol + c * LP);
-              qd[c] = tb_ld2(Lc + ol + (3 + c) * LP);
-            }
-          } else {
-            // ---- level 2: step lit+2 at plane x = q-1 on the output tile ----
-            // (reads rows w-1..w+1 of plane q-1: wait until every warp wrote it)
-            ok = ws_wait(&Lfull[lprev.s], lprev.ph, abort_flag);
-            if (!ok) break;
-            if (store) {
-              const int x = q - 1;
-              const long long i = (long long)x * g.sxy + (long long)y * g.pz + zp;
-              float* sp =
-                  snap2 ? in->snaps + ((((long long)slot2 * g.nx + x) * g.ny + y) * g.nz + zp) * 3
-                        : nullptr;
-              if (visc)
-                tb_pair_step<true, LZ, LP>(Lc, Lw, ol, Mp, Ep, qu, qd, zin_a, zin_b, hx, hy, hz,
-                                           hc, use_damp, damp, in, j20, j21, nc, i, D + i, nc,
-                                           sp);
-              else
-                tb_pair_step<false, LZ, LP>(Lc, Lw, ol, Mp, Ep, qu, qd, zin_a, zin_b, hx, hy, hz,
-                                            hc, use_damp, damp, in, j20, j21, nc, i, D + i, nc,
-                                            sp);
-            }
-          }
-          __syncwarp();
-          if (lane == 0) mbar_arrive(&Lempty[lprev.s]);  // this warp is done with plane q-1
-        }
-        Mp = Mc;
-        Ep = Ec;
-        lprev = lw;
-        lw.next();
-        cur = nxt;
-      }
-      if (!ok) break;
-      __syncwarp();
-      if (lane == 0) {
-        mbar_arrive(&hd->emptyA[cur.s]);   // the closing halo plane x1+1
-        mbar_arrive(&Lempty[lprev.s]);     // the tile's last level-1 plane x1
-      }
+      p = tb_tile_any(in, local, lit, k, p, warp, lane);
+      if (!p.ok) break;
     }
   }
   __syncthreads();
@@ -445,6 +520,10 @@ static int tb_xchunk(const Geom& g) {
 
 int make_tma_f32_tb(const StepArgs& a, int xchunk, TmaF32TB* t) {
   *t = TmaF32TB{};
+  if (a.g.ncell >= (1LL << 32)) {  // the kernel offsets components by a 32-bit cell count
+    set_error("grid too large for the two-step kernel (%lld cells)", a.g.ncell);
+    return SW_ERANGE;
+  }
   t->g = a.g;
   t->ts = make_tiles_tb(a.g, xchunk > 0 ? xchunk : tb_xchunk(a.g));
   if (a.coef_e == nullptr) {

@@ -249,8 +249,9 @@ typedef struct sw_fdtd_desc {
   void* traces;           /* dense (n_traces, n_steps) of the field dtype */
   int32_t* flags;         /* device int, bit 0 set when a non-finite u appears (may be NULL) */
   int32_t xchunk;         /* planes per tile along x (0 = automatic) */
-  int32_t steps_per_pass; /* F32: 0 (automatic) / 2 = two steps per pass over HBM where two
-                           * remain and the compensated sum is off; 1 = one step per pass */
+  int32_t steps_per_pass; /* F32: 2 = two steps per pass over HBM where two remain and the
+                           * compensated sum is off; 1 = one step per pass; 0 (automatic) =
+                           * two in sw_fdtd_batch_steps, one in sw_fdtd_steps */
   int32_t kernel;         /* 0: TMA-staged step kernels (default), 1: direct-load kernels */
   /* Device int the step loop may use as its step counter: with it, long runs
    * of sw_fdtd_steps replay one instantiated CUDA graph of 32 steps instead

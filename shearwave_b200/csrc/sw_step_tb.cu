@@ -1,5 +1,6 @@
 // Mixed-form step kernel that advances two time steps per pass over HBM
-// (opts steps_per_pass=2; runs without the compensated sum).
+// (the default of batched launches, opts steps_per_pass=2 for a lone solve;
+// runs without the compensated sum).
 //
 // Same per-cell update as the one-step kernels (src/shearwave/solver.py:
 // 195-226 in increment form), applied twice in one pass:
@@ -30,9 +31,9 @@
 // two steps here equal two one-step launches bit for bit.  A pass reads
 // buffer t mod 3 and writes buffer (t+2) mod 3.
 //
-// Per output cell and pair of steps it moves about 35 bytes of DRAM traffic
-// per step (u, d in and out once per two steps, coefficients, halos),
-// against 66 for one-step launches.
+// It moves about 27 bytes of DRAM traffic per cell-step (u, d in and out
+// once per two steps, coefficients twice, halos), against 66 for one-step
+// launches, and executes about 1.6 times their instructions.
 #include <math.h>
 
 #include <algorithm>

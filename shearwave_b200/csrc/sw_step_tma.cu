@@ -970,10 +970,11 @@ int launch_steps_tma(const StepArgs& a, int xchunk, int it0, int nsteps, cudaStr
     SW_CHECK_LAUNCH("step (tma)");
     return SW_OK;
   } else {
-    // steps_per_pass 2 and 0 (automatic): two steps per launch where two
-    // remain (one step otherwise) unless the compensated sum is on; 1: one
-    // step per launch
-    const bool fuse = a.steps_per_pass != 1 && !a.kahan && nsteps >= 2;
+    // steps_per_pass 2: two steps per launch where two remain (one step
+    // otherwise) unless the compensated sum is on; 0 (automatic) and 1: one
+    // step per launch (a lone solve at full clock runs faster one step at a
+    // time: 102 against 90 Gcell-steps/s at 192^3)
+    const bool fuse = a.steps_per_pass == 2 && !a.kahan && nsteps >= 2;
     TmaF32 t;
     rc = make_tma_f32(a, xchunk, &t, 0);
     if (rc != SW_OK) return rc;
@@ -1146,7 +1147,12 @@ int build_batch(const sw_fdtd_desc* descs, const int32_t* begins, int n, int it,
 constexpr size_t kBatchHeader = 256;
 
 // Mixed form: two steps per launch whenever every running solve runs both
-// steps of the pair; one-step launches around starts and ends.  The table
+// steps of the pair (unless a solve asks for one step per launch or for the
+// compensated sum); one-step launches around starts and ends.  Two steps per
+// pass are the default here: a batch keeps the GPU under its power cap long
+// enough that the one-step kernel runs at about 1.55 GHz, while the two-step
+// kernel, with 2.7x less DRAM traffic, keeps the full clock (config 3: 99
+// against 91 Gcell-steps/s).  The table
 // holds the one-step instance array, then the fused-kernel array.
 int batch_steps_mixed(const sw_fdtd_desc* descs, const int32_t* begins, int n, int it0,
                       int nsteps, void* table, cudaStream_t s) {

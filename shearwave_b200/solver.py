@@ -799,9 +799,9 @@ def shear_fdtd(
     ("auto" default: the reference's CG for fp64, and for mixed the exact
     direct spectral Poisson solve when ``poisson_tol <= 1e-8``; or "cg" /
     "spectral" explicitly), ``kahan`` (False: compensated displacement sum), ``step_kernel`` ("tma" default, or "direct"), ``xchunk`` (planes
-    per tile along x, 0 = automatic), ``steps_per_pass`` (mixed form: 0
-    (default) or 2 fuse two time steps per pass over HBM, except with
-    ``kahan``; 1 one step per launch), ``cuda_graph`` (True: long step runs replay one instantiated CUDA
+    per tile along x, 0 = automatic), ``steps_per_pass`` (mixed form: 2
+    fuses two time steps per pass over HBM, except with ``kahan``; 1 one
+    step per launch; 0 (default) two in batches, one for a lone solve), ``cuda_graph`` (True: long step runs replay one instantiated CUDA
     graph of 32 steps), ``force_terms`` (extra separable terms:
     list of ``((bx, by, bz), env)``), ``snapshot_stride`` (alias of the
     keyword), ``info`` (dict filled with CG statistics, phase times and a

@@ -1151,8 +1151,8 @@ constexpr size_t kBatchHeader = 256;
 // compensated sum); one-step launches around starts and ends.  Two steps per
 // pass are the default here: a batch keeps the GPU under its power cap long
 // enough that the one-step kernel runs at about 1.55 GHz, while the two-step
-// kernel, with 2.7x less DRAM traffic, keeps the full clock (config 3: 99
-// against 91 Gcell-steps/s).  The table
+// kernel, with 2.5x less DRAM traffic, keeps the full clock (48 solves of
+// 64^3..160x160x224 cells: 99 against 91 Gcell-steps/s).  The table
 // holds the one-step instance array, then the fused-kernel array.
 int batch_steps_mixed(const sw_fdtd_desc* descs, const int32_t* begins, int n, int it0,
                       int nsteps, void* table, cudaStream_t s) {

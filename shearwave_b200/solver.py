@@ -842,7 +842,8 @@ def shear_fdtd_batch(problems, *, precision=None, return_device=False):
     ``snapshot_stride``); grids, materials, pushes and ``n_steps`` may all
     differ.  The force projections of all problems run as one batched CG
     (every launch advances every unfinished solve) and the time loops as one
-    launch per step over the tiles of every running solve.  ``precision``
+    launch per pair of steps (per step where a solve starts or ends, or with
+    ``steps_per_pass=1`` or ``kahan``) over the tiles of every running solve.  ``precision``
     overrides ``opts["precision"]`` for all problems.
 
     Problems that need the host between steps (callback-free here, but 4-D

@@ -89,7 +89,10 @@ enum sw_tune_knob {
   SW_TUNE_BATCH_TILES_PER_CTA = 1, /* batched launches: tiles per CTA, 1..64 (8)   */
   SW_TUNE_XCHUNK = 2,              /* planes per x chunk, 0 = automatic (0)          */
   SW_TUNE_TILE_SHAPE = 3,          /* mixed step tiles: 0 auto, 1 64-wide, 2 32-wide */
-  SW_TUNE_COUNT = 4
+  SW_TUNE_STEPS_PER_PASS = 4,      /* mixed solves whose steps_per_pass is 0: 0 auto (two
+                                    * per pass in batched launches, one for a lone solve),
+                                    * 1 or 2 steps per pass (0) */
+  SW_TUNE_COUNT = 5
 };
 /* SW_EINVAL for an unknown knob or a value out of range. */
 int sw_tune_set(int knob, int value);

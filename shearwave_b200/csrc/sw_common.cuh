@@ -185,6 +185,15 @@ __device__ inline bool interior(const Geom& g, int x, int y, int z) {
 void set_error(const char* fmt, ...);
 // Launch-shape knob (enum sw_tune_knob), process-wide.
 int tune_get(int knob);
+// Steps per pass of a mixed-form solve: its own setting (desc.steps_per_pass)
+// when non-zero, else the SW_TUNE_STEPS_PER_PASS knob when non-zero, else two
+// in batched launches and one for a lone solve.
+inline int steps_per_pass_of(int own, bool batched) {
+  if (own != 0) return own;
+  const int k = tune_get(SW_TUNE_STEPS_PER_PASS);
+  if (k != 0) return k;
+  return batched ? 2 : 1;
+}
 constexpr int kNumSMs = 148;  // B200
 // CTA slots a step launch is sized for (SMs x CTAs per SM): the mixed
 // kernel follows the SW_TUNE_STEP_CTAS_PER_SM knob, the plain FP64 kernel

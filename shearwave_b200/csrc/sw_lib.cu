@@ -21,7 +21,7 @@ static std::atomic<unsigned long long> g_launches{0};
 
 void count_launches(unsigned long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
-static std::atomic<int> g_tune[SW_TUNE_COUNT] = {{2}, {8}, {0}, {0}};
+static std::atomic<int> g_tune[SW_TUNE_COUNT] = {{2}, {8}, {0}, {0}, {0}};
 
 int tune_get(int knob) { return (knob >= 0 && knob < SW_TUNE_COUNT) ? g_tune[knob].load() : -1; }
 
@@ -49,7 +49,8 @@ extern "C" size_t sw_fdtd_desc_size(void) { return sizeof(sw_fdtd_desc); }
 extern "C" uint64_t sw_launch_count(void) { return sw::g_launches.load(); }
 
 extern "C" int sw_tune_set(int knob, int value) {
-  static const int lo[SW_TUNE_COUNT] = {1, 1, 0, 0}, hi[SW_TUNE_COUNT] = {2, 64, 1 << 20, 2};
+  static const int lo[SW_TUNE_COUNT] = {1, 1, 0, 0, 0};
+  static const int hi[SW_TUNE_COUNT] = {2, 64, 1 << 20, 2, 2};
   if (knob < 0 || knob >= SW_TUNE_COUNT || value < lo[knob] || value > hi[knob]) {
     sw::set_error("sw_tune_set: knob %d does not take the value %d", knob, value);
     return SW_EINVAL;

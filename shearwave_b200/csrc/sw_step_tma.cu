@@ -970,11 +970,11 @@ int launch_steps_tma(const StepArgs& a, int xchunk, int it0, int nsteps, cudaStr
     SW_CHECK_LAUNCH("step (tma)");
     return SW_OK;
   } else {
-    // steps_per_pass 2: two steps per launch where two remain (one step
-    // otherwise) unless the compensated sum is on; 0 (automatic) and 1: one
-    // step per launch (a lone solve at full clock runs faster one step at a
-    // time: 102 against 90 Gcell-steps/s at 192^3)
-    const bool fuse = a.steps_per_pass == 2 && !a.kahan && nsteps >= 2;
+    // two steps per pass: two steps per launch where two remain (one step
+    // otherwise) unless the compensated sum is on.  A lone solve defaults to
+    // one step per launch: at full clock it runs faster that way (102
+    // against 90 Gcell-steps/s at 192^3).
+    const bool fuse = steps_per_pass_of(a.steps_per_pass, false) == 2 && !a.kahan && nsteps >= 2;
     TmaF32 t;
     rc = make_tma_f32(a, xchunk, &t, 0);
     if (rc != SW_OK) return rc;
@@ -1162,7 +1162,8 @@ int batch_steps_mixed(const sw_fdtd_desc* descs, const int32_t* begins, int n, i
   cudaError_t e0 = cudaMemsetAsync(queues, 0, 2 * sizeof(int), s);
   if (e0 != cudaSuccess) return cuda_status(e0, "batch queue reset");
   bool fuse_ok = true;
-  for (int i = 0; i < n; ++i) fuse_ok &= (descs[i].steps_per_pass != 1 && !descs[i].kahan);
+  for (int i = 0; i < n; ++i)
+    fuse_ok &= (steps_per_pass_of(descs[i].steps_per_pass, true) == 2 && !descs[i].kahan);
   auto active = [&](int i, int it) {
     const int lit = it - (begins ? begins[i] : 0);
     return lit >= 0 && lit < descs[i].n_steps;

@@ -1,8 +1,9 @@
 """Autotuner for the launch shape of the step kernels.
 
 The step kernels' results do not depend on how the grid is cut into tiles
-(every cell runs the same arithmetic), only their speed does.  Four
-process-wide knobs of the CUDA library set the cut (enum ``sw_tune_knob``):
+or how many time steps a launch fuses (every cell runs the same
+arithmetic), only their speed does.  Five process-wide knobs of the CUDA
+library set the cut (enum ``sw_tune_knob``):
 
 * ``ctas_per_sm`` — resident step CTAs per SM (1 or 2): one CTA per SM
   leaves each CTA the whole SM's bandwidth share, two hide more latency;
@@ -13,7 +14,12 @@ process-wide knobs of the CUDA library set the cut (enum ``sw_tune_knob``):
 * ``xchunk`` — planes per x chunk for every launch (0 = automatic);
 * ``tile_shape`` — the mixed step kernel's (z, y) tile: 0 picks, per grid,
   whichever of 64 x 8 and 32 x 16 covers the plane with fewer cells; 1 and
-  2 force one.
+  2 force one;
+* ``steps_per_pass`` — time steps per launch of mixed solves that leave
+  ``opts["steps_per_pass"]`` at 0: 0 keeps the library's choice (two in
+  batched launches, one for a lone solve), 1 or 2 force it.  Which is
+  faster depends on whether the GPU runs at its power cap: the two-step
+  kernel moves 2.5 x fewer DRAM bytes but issues 1.6 x the instructions.
 
 :func:`autotune` times a shortened copy of a workload (one problem through
 ``shear_fdtd``, or a batch through ``shear_fdtd_batch``) under each
@@ -33,7 +39,8 @@ from pathlib import Path
 
 from . import _native
 
-KNOBS = {"ctas_per_sm": 0, "batch_tiles_per_cta": 1, "xchunk": 2, "tile_shape": 3}
+KNOBS = {"ctas_per_sm": 0, "batch_tiles_per_cta": 1, "xchunk": 2, "tile_shape": 3,
+         "steps_per_pass": 4}
 
 __all__ = ["KNOBS", "get_knobs", "set_knobs", "knobs", "workload_key", "autotune",
            "apply_cached", "default_cache_path"]
@@ -121,13 +128,18 @@ def _time_steps(problems, precision) -> float:
 
 
 def _candidates(n_problems):
-    """Default sweep: tile shape x tiles per CTA (batches) or x chunk (one
+    """Default sweep: two steps per pass (whose tiles are fixed), then one step
+    per pass under each tile shape x tiles per CTA (batches) or x chunk (one
     solve), at two CTAs per SM (one CTA per SM measured slower everywhere)."""
+    fused = [dict(ctas_per_sm=2, batch_tiles_per_cta=8, xchunk=0, tile_shape=0,
+                  steps_per_pass=2)]
     if n_problems > 1:
-        return [dict(ctas_per_sm=2, batch_tiles_per_cta=b, xchunk=0, tile_shape=t)
-                for t, b in itertools.product((0, 1, 2), (4, 8, 16))]
-    return [dict(ctas_per_sm=2, xchunk=x, batch_tiles_per_cta=8, tile_shape=t)
-            for t, x in itertools.product((0, 1, 2), (0, 32, 64))]
+        return fused + [dict(ctas_per_sm=2, batch_tiles_per_cta=b, xchunk=0, tile_shape=t,
+                             steps_per_pass=1)
+                        for t, b in itertools.product((0, 1, 2), (4, 8, 16))]
+    return fused + [dict(ctas_per_sm=2, xchunk=x, batch_tiles_per_cta=8, tile_shape=t,
+                         steps_per_pass=1)
+                    for t, x in itertools.product((0, 1, 2), (0, 32, 64))]
 
 
 def autotune(problems, *, precision="mixed", steps=64, repeats=2, candidates=None,

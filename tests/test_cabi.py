@@ -96,14 +96,18 @@ def test_tune_knobs_roundtrip():
     from shearwave_b200 import tune
 
     old = tune.get_knobs()
-    assert set(old) == {"ctas_per_sm", "batch_tiles_per_cta", "xchunk", "tile_shape"}
+    assert set(old) == {"ctas_per_sm", "batch_tiles_per_cta", "xchunk", "tile_shape",
+                        "steps_per_pass"}
+    assert old["steps_per_pass"] == 0  # automatic unless a caller sets it
     try:
-        with tune.knobs(ctas_per_sm=1, xchunk=32):
+        with tune.knobs(ctas_per_sm=1, xchunk=32, steps_per_pass=2):
             assert tune.get_knobs()["ctas_per_sm"] == 1
             assert tune.get_knobs()["xchunk"] == 32
+            assert tune.get_knobs()["steps_per_pass"] == 2
         assert tune.get_knobs() == old
         for bad in ({"ctas_per_sm": 3}, {"ctas_per_sm": 0}, {"batch_tiles_per_cta": 0},
-                    {"xchunk": -1}, {"tile_shape": 3}, {"nope": 1}):
+                    {"xchunk": -1}, {"tile_shape": 3}, {"steps_per_pass": 3},
+                    {"steps_per_pass": -1}, {"nope": 1}):
             with pytest.raises(ValueError):
                 tune.set_knobs(**bad)
         assert tune.get_knobs() == old

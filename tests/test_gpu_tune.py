@@ -1,5 +1,6 @@
 """Launch-shape knobs change only the speed of the step kernels, never the
-numbers: every cell runs the same arithmetic however the grid is tiled."""
+numbers: every cell runs the same arithmetic however the grid is tiled and
+however many time steps a launch fuses."""
 
 from __future__ import annotations
 
@@ -11,7 +12,9 @@ SETTINGS = [dict(ctas_per_sm=1, batch_tiles_per_cta=1, xchunk=0, tile_shape=0),
             dict(ctas_per_sm=2, batch_tiles_per_cta=16, xchunk=0, tile_shape=1),
             dict(ctas_per_sm=1, batch_tiles_per_cta=8, xchunk=5, tile_shape=2),
             dict(ctas_per_sm=2, batch_tiles_per_cta=8, xchunk=64, tile_shape=2),
-            dict(ctas_per_sm=2, batch_tiles_per_cta=4, xchunk=0, tile_shape=1)]
+            dict(ctas_per_sm=2, batch_tiles_per_cta=4, xchunk=0, tile_shape=1),
+            dict(ctas_per_sm=2, batch_tiles_per_cta=8, xchunk=0, tile_shape=0, steps_per_pass=1),
+            dict(ctas_per_sm=2, batch_tiles_per_cta=8, xchunk=0, tile_shape=0, steps_per_pass=2)]
 
 
 def _problems():

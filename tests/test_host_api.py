@@ -142,3 +142,21 @@ def test_arrival_analysis_recovers_a_known_speed():
     r = arrival_analysis(traces, dT, dist, c)
     assert abs(r["c_fit"] - c) / c < 0.02
     assert np.all(np.abs(r["speeds"] - c) / c < 0.05)
+
+
+def test_bench_traffic_table_covers_both_step_kernels():
+    """bench.py's roofline reads the ncu bytes per cell-step of whichever step
+    kernel the run used from profiles/traffic.txt: both must be there, and
+    the two-step kernel must move fewer bytes than the one-step kernel."""
+    import importlib.util
+    from pathlib import Path
+
+    root = Path(__file__).resolve().parents[1]
+    spec = importlib.util.spec_from_file_location("bench_for_test", root / "bench.py")
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    one = bench.ncu_bytes_per_cell_step("step_f32_tma")
+    two = bench.ncu_bytes_per_cell_step("step_f32_fused2")
+    assert one is not None and two is not None
+    assert 0 < two < one
+    assert bench.ncu_bytes_per_cell_step("no_such_kernel") is None

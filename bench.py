@@ -145,7 +145,7 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # workloads
 # ---------------------------------------------------------------------------
-def make_workload(name: str, rank: int, grid=None, nsteps=None):
+def make_workload(name: str, rank: int, grid=None, nsteps=None, shrink=1.0, instances=48):
     from shearwave_b200 import workloads as W
 
     if name == "c1":
@@ -154,11 +154,11 @@ def make_workload(name: str, rank: int, grid=None, nsteps=None):
     if name == "c0":
         return [W.problem_c0()]
     if name == "c3":
-        return W.batch_c3(seed=rank)
+        return W.batch_c3(seed=rank, n=instances, shrink=shrink)
     raise SystemExit(f"unknown workload {name}")
 
 
-def describe(name: str, probs) -> dict:
+def describe(name: str, probs, shrink: float = 1.0) -> dict:
     cs = sum(_cell_steps(p) for p in probs)
     if name == "c1" and (_shape(probs[0]) != (192, 192, 192) or probs[0]["n_steps"] != 2000):
         name = "c1"  # overridden size: grid / n_steps below say which
@@ -171,6 +171,7 @@ def describe(name: str, probs) -> dict:
             "grid": list(_shape(probs[0])) if len(probs) == 1 else "varied",
             "n_steps": probs[0]["n_steps"] if len(probs) == 1 else "varied",
             "dX_m": probs[0]["dX"], "precision": "mixed (FP32 u and increment, FP64 projection)",
+            "full_size": bool(name != "c3" or (len(probs) == 48 and shrink == 1.0)),
             "l2_flush": "none needed: per-solve state is larger than the 126 MB L2",
             "data": "seeded synthetic inputs with the config shapes"}
     return desc
@@ -300,7 +301,7 @@ def run_reference(a, rank, world):
     """Reference arm: the CPU port of the reference on the host's cores."""
     if rank != 0:
         return 0
-    probs = make_workload(a.workload, 0, a.grid, a.nsteps)
+    probs = make_workload(a.workload, 0, a.grid, a.nsteps, a.shrink, a.instances)
     ncpu = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
     procs = ncpu if len(probs) > 1 else 1
     budget = 2.0
@@ -323,7 +324,7 @@ def run_reference(a, rank, world):
         "steps": a.steps, "warmup": a.warmup,
         "ms_per_step": 1e3 * statistics.median(s[1] for s in samples),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic", "config": describe(a.workload, probs),
+        "data": "synthetic", "config": describe(a.workload, probs, a.shrink),
         "cpu_baseline": {"value": val, "unit": UNIT, "cores": procs, "kind": "port",
                          "sample": f"{procs} process(es) x ~{budget:.0f} s of the FP32 CPU port "
                                    "of the reference time loop on this workload's grids"},
@@ -336,7 +337,8 @@ def run_reference(a, rank, world):
 # ---------------------------------------------------------------------------
 # serving: config-4 request stream through the continuous-batching server
 # ---------------------------------------------------------------------------
-def serving_run(n_requests: int, rate_hz: float, seed: int = 0, probs=None) -> dict:
+def serving_run(n_requests: int, rate_hz: float, seed: int = 0, probs=None,
+                n_fp64: int = 2) -> dict:
     """Poisson arrivals of config-4 requests (log-uniform 64^3..256^3 cubes,
     1 or 4 pushes, nT 500..4000, inclusion media, HBM budget 150 GB)."""
     from shearwave_b200 import workloads as W
@@ -349,12 +351,15 @@ def serving_run(n_requests: int, rate_hz: float, seed: int = 0, probs=None) -> d
     with ShearServer(hbm_budget=150e9, chunk_steps=50) as srv:
         run_stream(srv, probs, arrivals)
     st = srv.stats()
-    return {"requests": n_requests, "rate_hz": rate_hz,
-            "latency_s": st["latency_s"], "queue_s": st["queue_s"],
-            "gcell_steps_per_s": st["gcell_steps_per_s"],
-            "cell_steps": int(sum(W.cell_steps(p) for p in probs)),
-            "workload": "config-4 requests (log-uniform 64^3..256^3, 1 or 4 pushes, "
-                        "nT 500..4000), Poisson arrivals, budget 150 GB, mixed form"}
+    out = {"requests": n_requests, "rate_hz": rate_hz,
+           "latency_s": st["latency_s"], "queue_s": st["queue_s"],
+           "gcell_steps_per_s": st["gcell_steps_per_s"], "failed": st.get("failed", 0),
+           "cell_steps": int(sum(W.cell_steps(p) for p in probs)),
+           "workload": "config-4 requests (log-uniform 64^3..256^3, 1 or 4 pushes, "
+                       "nT 500..4000), Poisson arrivals, budget 150 GB, mixed form"}
+    if n_fp64 > 0:
+        out["fp64_one_at_a_time"] = _fp64_one_at_a_time(probs[:n_fp64])
+    return out
 
 
 def serving_sweep(rates, n_requests: int, n_fp64: int, seed: int = 0) -> dict:
@@ -367,27 +372,125 @@ def serving_sweep(rates, n_requests: int, n_fp64: int, seed: int = 0) -> dict:
 
     rng = np.random.default_rng(1234 + seed)
     probs = [W.problem_c4(rng) for _ in range(n_requests)]
-    runs = [serving_run(n_requests, r, seed, probs) for r in rates]
+    runs = [serving_run(n_requests, r, seed, probs, n_fp64=0) for r in rates]
     out = {"rates": [{k: r[k] for k in ("rate_hz", "latency_s", "queue_s", "gcell_steps_per_s")}
                      for r in runs],
            "requests": n_requests, "workload": runs[0]["workload"]}
     if n_fp64 > 0:
-        dev = torch.device("cuda", torch.cuda.current_device())
-        sample = [_to_dev(p, dev) for p in probs[:n_fp64]]
-        _solve(sample[0], "fp64", True)  # warm
-        torch.cuda.synchronize()
-        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        s.record()
-        for p in sample:
-            _solve(p, "fp64", True)
-        e.record()
-        torch.cuda.synchronize()
-        cs = sum(W.cell_steps(p) for p in probs[:n_fp64])
-        out["fp64_one_at_a_time"] = {
-            "value": cs / (s.elapsed_time(e) / 1e3) / 1e9, "unit": UNIT,
-            "sample": f"the first {n_fp64} requests of the stream, plain FP64 shear_fdtd "
-                      "calls one after another, inputs in HBM"}
+        out["fp64_one_at_a_time"] = _fp64_one_at_a_time(probs[:n_fp64])
     return out
+
+
+def _fp64_one_at_a_time(sample) -> dict:
+    """Plain-FP64 shear_fdtd calls one after another on requests of the
+    stream (inputs in HBM, CUDA events): the serving comparison."""
+    import torch
+
+    from shearwave_b200 import workloads as W
+
+    dev = torch.device("cuda", torch.cuda.current_device())
+    dsample = [_to_dev(p, dev) for p in sample]
+    _solve(dsample[0], "fp64", True)  # warm
+    torch.cuda.synchronize()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record()
+    for p in dsample:
+        _solve(p, "fp64", True)
+    e.record()
+    torch.cuda.synchronize()
+    cs = sum(W.cell_steps(p) for p in sample)
+    return {"value": cs / (s.elapsed_time(e) / 1e3) / 1e9, "unit": UNIT,
+            "sample": f"{len(sample)} requests of the stream, plain FP64 shear_fdtd calls one "
+                      "after another, inputs in HBM"}
+
+
+# ---------------------------------------------------------------------------
+# accuracy and phase-time extras of the bench line
+# ---------------------------------------------------------------------------
+def _knobs():
+    from shearwave_b200 import tune
+
+    return tune.get_knobs()
+
+
+def _split(infos, batched: bool) -> dict:
+    """Device time of the phases of one bench step (CUDA events in the solver):
+    setup + force projection, the time loop, the output conversion.  A batch
+    runs each phase for all solves together (max over solves); sequential
+    solves add up."""
+    agg = max if batched else sum
+    out = {k: agg(i[f"t_{k}_ms"] for i in infos) for k in ("setup", "steps", "finish")}
+    out["projection_method"] = sorted({c.get("method", "cg") for i in infos for c in i["cg"]})
+    out["cg_iterations"] = int(sum(c["iters"] for i in infos for c in i["cg"]))
+    out["note"] = ("setup = materials, initial state and the force projection; steps = the "
+                   "time loop; finish = output conversion")
+    return out
+
+
+def _strain_rel(outs, o64, probs) -> dict:
+    """Max over solves of the relative L2 of each strain invariant of the mixed
+    result against the plain FP64 result (fused strain post-pass on both)."""
+    import shearwave_b200 as sw
+
+    worst = {}
+    for (u32, *_), (u64, *_), p in zip(outs, o64, probs):
+        _e, i32 = sw.compute_strain_fields(u32, p["dX"], p["dY"], p["dZ"], return_tensor=False,
+                                           return_device=True)
+        _e, i64 = sw.compute_strain_fields(u64, p["dX"], p["dY"], p["dZ"], return_tensor=False,
+                                           return_device=True)
+        for k in i64:
+            a, b = i32[k].double(), i64[k].double()
+            r = float((a - b).norm() / b.norm().clamp_min(1e-300))
+            worst[k] = max(worst.get(k, 0.0), r)
+    return worst
+
+
+def _divergence_residual(dprobs) -> dict:
+    """Divergence residual max|div_c f_S| / max|div_c f| of each solve's
+    projected force: the mixed form's projection (spectral solve) and the
+    plain FP64 form's CG at the solve's tolerance, and the relative L2 of the
+    mixed projected force against the FP64 one."""
+    import torch
+
+    import shearwave_b200 as sw
+
+    rows = []
+    for p in dprobs:
+        z = torch.zeros_like(p["bz"], dtype=torch.float64)
+        bz = p["bz"].double()
+        h = (p["dX"], p["dY"], p["dZ"])
+        tol, it = p["opts"]["poisson_tol"], p["opts"]["poisson_max_iters"]
+        din = sw.divergence_center(z, z, bz, *h).abs().max()
+        fs = sw.project_vector_field(z, z, bz, *h, tol, it, method="spectral")
+        fc = sw.project_vector_field(z, z, bz, *h, tol, it, method="cg")
+        rs = float(sw.divergence_center(*fs, *h).abs().max() / din)
+        rc = float(sw.divergence_center(*fc, *h).abs().max() / din)
+        num = sum(float((a - b).norm() ** 2) for a, b in zip(fs, fc)) ** 0.5
+        den = sum(float(b.norm() ** 2) for b in fc) ** 0.5
+        rows.append((rs, rc, num / den))
+    return {"mixed_spectral": max(r[0] for r in rows), "fp64_cg": max(r[1] for r in rows),
+            "rel_l2_mixed_vs_fp64_force": max(r[2] for r in rows),
+            "solves": len(rows),
+            "note": "max over the first solves of the workload, each at its own poisson_tol"}
+
+
+def _kahan_run(dprobs, cs_rank, o64, max_over_ranks, sum_over_ranks) -> dict:
+    """One bench step with the compensated displacement sum (kahan=True: one
+    step per launch, 12 more bytes per cell-step), device-timed."""
+    import torch
+
+    kprobs = [dict(p, opts=dict(p["opts"], kahan=True)) for p in dprobs]
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record()
+    outs = _solve_all(kprobs, "mixed", True)
+    e.record()
+    torch.cuda.synchronize()
+    t = max_over_ranks(s.elapsed_time(e) / 1e3)
+    ru = max(float((o[0].double() - r[0]).norm() / r[0].norm()) for o, r in zip(outs, o64))
+    rv = max(float((o[1].double() - r[1]).norm() / r[1].norm()) for o, r in zip(outs, o64))
+    return {"value": sum_over_ranks(cs_rank) / t / 1e9, "unit": UNIT, "rel_l2_u": ru,
+            "rel_l2_v": rv, "how": "the same batch with opts kahan=True (one step per "
+                                   "launch), one device-timed bench step"}
 
 
 # ---------------------------------------------------------------------------
@@ -405,6 +508,9 @@ def main(argv=None) -> int:
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--grid", type=int, default=None, help="c1 only: cubic grid override")
     ap.add_argument("--nsteps", type=int, default=None, help="c1 only: nT override")
+    ap.add_argument("--shrink", type=float, default=1.0,
+                    help="c3 only: scale grids and nT down (small cases for profiling)")
+    ap.add_argument("--instances", type=int, default=48, help="c3 only: solves in the batch")
     ap.add_argument("--serve-requests", type=int, default=16,
                     help="requests of the config-4 serving stream run after the timing (0: skip)")
     ap.add_argument("--serve-rate", type=float, default=4.0,
@@ -415,6 +521,13 @@ def main(argv=None) -> int:
                          "solves of its first requests")
     ap.add_argument("--steps-per-pass", type=int, default=0, choices=[0, 1, 2],
                     help="mixed form: time steps fused per pass over HBM (0 = library default)")
+    ap.add_argument("--no-tune", action="store_true",
+                    help="skip the autotuner (library default launch shapes)")
+    ap.add_argument("--tune-steps", type=int, default=128,
+                    help="time steps of the shortened workload each autotuner candidate runs")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the compensated-sum run, the pageable e2e run and the "
+                         "divergence / strain-invariant accuracy checks")
     a = ap.parse_args(argv)
     rank, world, local = rank_info()
     if a.impl == "reference":
@@ -442,12 +555,26 @@ def main(argv=None) -> int:
     def sum_over_ranks(x: float) -> float:
         return reduce_scalar(x, "sum", dev, world)
 
-    probs = make_workload(a.workload, rank, a.grid, a.nsteps)
+    probs = make_workload(a.workload, rank, a.grid, a.nsteps, a.shrink, a.instances)
     if a.steps_per_pass:
         for p in probs:
             p["opts"] = dict(p["opts"], steps_per_pass=a.steps_per_pass)
     dprobs = [_to_dev(p, dev) for p in probs]
     cs_rank = sum(_cell_steps(p) for p in probs)
+
+    # ---- launch shapes chosen by the autotuner (shearwave_b200/tune.py) ----
+    tune_info = None
+    default_knobs = _knobs()
+    if not a.no_tune and not a.steps_per_pass:
+        from shearwave_b200 import tune
+
+        t0 = time.perf_counter()
+        cands = tune.fused_batch_candidates() if len(dprobs) > 1 else None
+        res = tune.autotune(dprobs, steps=a.tune_steps, repeats=1, candidates=cands)
+        tune_info = {"knobs": res["best"], "candidates": len(res["results"]),
+                     "tune_steps": a.tune_steps, "seconds": time.perf_counter() - t0,
+                     "scores_gcell_steps_s": [round(r["gcell_steps_per_s"], 2)
+                                              for r in res["results"]]}
 
     # ---- device-resident timing -------------------------------------------
     for _ in range(a.warmup):
@@ -456,7 +583,7 @@ def main(argv=None) -> int:
     barrier()
     torch.cuda.synchronize()
     infos = []
-    n0 = native.launch_count()
+    n0, h0 = native.launch_count(), native.host_enqueue_count()
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
         start.record()
@@ -467,6 +594,7 @@ def main(argv=None) -> int:
         torch.cuda.synchronize()
     barrier()
     launches = native.launch_count() - n0
+    host_enqueues = native.host_enqueue_count() - h0
     t_dev = max_over_ranks(start.elapsed_time(end) / 1e3)
     value = sum_over_ranks(cs_rank) * a.steps / t_dev / 1e9
 
@@ -496,6 +624,7 @@ def main(argv=None) -> int:
     traffic = None if bpcs is None else bpcs * cells_per_launch
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
+            "frac_of_nominal_8000_gbs": achieved / 8000.0,
             "traffic_note": ("DRAM bytes per launch: ncu's read+write bytes per cell-step "
                              "(profiles/traffic.txt) x the cells a launch updates"),
             "traffic_bytes_per_cell_step": bpcs,
@@ -510,9 +639,12 @@ def main(argv=None) -> int:
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": 1e3 * t_dev / a.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": describe(a.workload, probs), "roofline": roof,
+        "config": dict(describe(a.workload, probs, a.shrink), autotune=tune_info,
+                       knobs=_knobs()), "roofline": roof,
         "clocks": clk.summary(), "gpu_launches": int(launches),
+        "host_enqueues": int(host_enqueues),
         "cg_iters": [c["iters"] for i in infos for c in i["cg"]],
+        "time_split_ms": {"mixed": _split(infos, batched=len(probs) > 1)},
     }
 
     # ---- plain FP64 GPU drop-in on the same workload: one solve at a time ----
@@ -521,12 +653,17 @@ def main(argv=None) -> int:
         torch.cuda.synchronize()
         barrier()
         s2, e2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        s2.record()
-        o64 = [_solve(p, "fp64", True) for p in dprobs]
-        e2.record()
-        torch.cuda.synchronize()
+        infos64 = [{} for _ in dprobs]
+        from shearwave_b200 import tune
+
+        with tune.knobs(**default_knobs):  # the plain drop-in runs the library defaults
+            s2.record()
+            o64 = [_solve(p, "fp64", True, i) for p, i in zip(dprobs, infos64)]
+            e2.record()
+            torch.cuda.synchronize()
         t64 = max_over_ranks(s2.elapsed_time(e2) / 1e3)
         v64 = sum_over_ranks(cs_rank) / t64 / 1e9
+        line["time_split_ms"]["fp64"] = _split(infos64, batched=False)
         rl = []
         for (u32, v32, *_), (u64, v64_, *_) in zip(outs, o64):
             du = torch.linalg.vector_norm(u32.double() - u64) / torch.linalg.vector_norm(u64)
@@ -537,6 +674,11 @@ def main(argv=None) -> int:
                                         "shear_fdtd calls, device-resident, CUDA events",
                                  "rel_l2_u": max(r[0] for r in rl),
                                  "rel_l2_v": max(r[1] for r in rl)}
+        if not a.no_extras:
+            line["vs_plain_fp64"]["rel_l2_strain_invariants"] = _strain_rel(outs, o64, probs)
+            line["divergence_residual"] = _divergence_residual(dprobs[:4])
+            line["kahan"] = _kahan_run(dprobs, cs_rank, o64, max_over_ranks, sum_over_ranks)
+        del o64
 
     # ---- end to end through the public API with host arrays ---------------
     # inputs in page-locked host memory, outputs returned as numpy arrays;
@@ -563,6 +705,20 @@ def main(argv=None) -> int:
                        "note": "page-locked host inputs in, numpy outputs back, through "
                                "shear_fdtd_batch (projection included), wall clock after "
                                "one warm-up step"}
+        if not a.no_extras:
+            # the same with the plain (pageable) numpy arrays a drop-in caller passes
+            t0 = time.perf_counter()
+            for _ in range(e2e_steps):
+                outs = _solve_all(probs, "mixed", False)
+                del outs
+            torch.cuda.synchronize()
+            tp = max_over_ranks(time.perf_counter() - t0)
+            line["e2e_pageable"] = {
+                "value": sum_over_ranks(cs_rank) * e2e_steps / tp / 1e9, "unit": UNIT,
+                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                "steps": e2e_steps,
+                "note": "pageable numpy inputs in (as a drop-in caller passes them), numpy "
+                        "outputs back, otherwise as e2e"}
 
     if rank == 0 and world == 1 and a.serve_requests > 0:
         if a.serve_sweep:

@@ -50,7 +50,9 @@ enum sw_status {
   SW_ECUDA = 2,       /* a CUDA runtime call or launch failed */
   SW_ENONFINITE = 3,  /* non-finite values detected in the state */
   SW_ERANGE = 4,      /* size above a compiled-in maximum */
-  SW_EWORKSPACE = 5   /* workspace smaller than the *_workspace_bytes query */
+  SW_EWORKSPACE = 5,  /* workspace smaller than the *_workspace_bytes query */
+  SW_ETIMEOUT = 6     /* a bounded device-side wait ran out, or a step launch refused to
+                       * run: the solve's state is incomplete (sw_fdtd_status) */
 };
 
 /* Why a CG solve stopped (solver.py:1033-1048 plus the early exit of 672-676). */
@@ -79,6 +81,9 @@ int sw_pitch(int nz);
 size_t sw_fdtd_desc_size(void);
 /* Number of kernels this library has launched in the process so far. */
 uint64_t sw_launch_count(void);
+/* Number of host-side enqueue calls behind those kernels (a CUDA-graph
+ * replay of a segment of the time loop launches many kernels with one). */
+uint64_t sw_host_enqueue_count(void);
 
 /* Launch-shape knobs of the step kernels (no counterpart in the reference:
  * the autotuner in shearwave_b200/tune.py sweeps them per workload).  They
@@ -92,7 +97,11 @@ enum sw_tune_knob {
   SW_TUNE_STEPS_PER_PASS = 4,      /* mixed solves whose steps_per_pass is 0: 0 auto (two
                                     * per pass in batched launches, one for a lone solve),
                                     * 1 or 2 steps per pass (0) */
-  SW_TUNE_COUNT = 5
+  SW_TUNE_WAIT_BUDGET = 5,         /* step kernels: how long a CTA waits on its pipeline
+                                    * (after the first failed test) before it abandons its
+                                    * tiles and flags their solves, in units of 1024 cycles,
+                                    * 1..4000000 (3906250, about 4e9 cycles) */
+  SW_TUNE_COUNT = 6
 };
 /* SW_EINVAL for an unknown knob or a value out of range. */
 int sw_tune_set(int knob, int value);
@@ -250,7 +259,10 @@ typedef struct sw_fdtd_desc {
   int32_t n_traces;       /* > 0: record u_z at trace cells every step */
   const int32_t* trace_cells; /* n_traces x (ix, iy, iz) */
   void* traces;           /* dense (n_traces, n_steps) of the field dtype */
-  int32_t* flags;         /* device int, bit 0 set when a non-finite u appears (may be NULL) */
+  int32_t* flags;         /* device int: bit 0 a non-finite u (set by sw_fdtd_finish), bit 1 a
+                           * step kernel's bounded wait ran out, bit 2 a step launch refused
+                           * to run; a solve with bit 1 or 2 set is skipped by later step
+                           * launches (may be NULL) */
   int32_t xchunk;         /* planes per tile along x (0 = automatic) */
   int32_t steps_per_pass; /* F32: 2 = two steps per pass over HBM where two remain and the
                            * compensated sum is off; 1 = one step per pass; 0 (automatic) =
@@ -264,6 +276,12 @@ typedef struct sw_fdtd_desc {
    * the launch-wide tile queue of this solve's own step launches, which
    * balances tiles over the SMs (NULL: tiles in a fixed stride). */
   int32_t* queue;
+  /* Testing switch (0 in normal use): non-zero makes the TMA step kernels
+   * leave the first ring stage of each of this solve's tiles unarmed, so
+   * that the consumers' bounded waits run out (nothing faults or hangs: the
+   * CTA drains its copies, flags the solve and returns).  Lets a test drive
+   * the timeout path of sw_fdtd_status. */
+  int32_t stall_test;
 } sw_fdtd_desc;
 
 /* Material coefficients from rho, mu, eta.  Each of rho/mu/eta is a dense
@@ -284,6 +302,15 @@ int sw_fdtd_steps(const sw_fdtd_desc* d, int32_t it0, int32_t nsteps, void* stre
  * (nx,ny,nz,3) arrays of the field dtype (either may be NULL). */
 int sw_fdtd_finish(const sw_fdtd_desc* d, int32_t steps_done, void* u_out, void* v_out,
                    void* stream);
+
+/* Status of a solve after its steps: synchronises `stream`, copies the
+ * solve's device flag word into *host_flags (may be NULL) and returns
+ * SW_ETIMEOUT when a step kernel abandoned any of the solve's tiles (a
+ * bounded wait ran out, or a launch refused a misaligned TMA destination),
+ * SW_ENONFINITE when sw_fdtd_finish found a non-finite u, else SW_OK.
+ * Flag bits: 1 non-finite, 2 wait timeout, 4 refused launch.  The
+ * reference's time loop has no such check (solver.py:194-239). */
+int sw_fdtd_status(const sw_fdtd_desc* d, int32_t* host_flags, void* stream);
 
 /* Device bytes of the instance table sw_fdtd_batch_steps needs for n solves. */
 size_t sw_fdtd_batch_table_bytes(int n);

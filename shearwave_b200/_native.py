@@ -15,7 +15,11 @@ LIB_PATH = Path(__file__).resolve().parent / "_lib" / "libshearwave_b200.so"
 
 SW_F32, SW_F64 = 0, 1
 SW_PLAIN_F64, SW_MIXED_F32 = 0, 1
-SW_OK, SW_EINVAL, SW_ECUDA, SW_ENONFINITE, SW_ERANGE, SW_EWORKSPACE = range(6)
+SW_OK, SW_EINVAL, SW_ECUDA, SW_ENONFINITE, SW_ERANGE, SW_EWORKSPACE, SW_ETIMEOUT = range(7)
+# solve flag bits (sw_fdtd_desc.flags)
+FLAG_NONFINITE, FLAG_TIMEOUT, FLAG_REFUSED = 1, 2, 4
+# sw_tune_knob values that are not launch-shape knobs
+SW_TUNE_WAIT_BUDGET = 5
 SW_CG_CONVERGED = 1
 CG_REASONS = {0: "running", 1: "converged", 2: "breakdown", 3: "nonfinite", 4: "max_iters",
               5: "early_exit"}
@@ -76,6 +80,7 @@ class FdtdDesc(C.Structure):
         ("kernel", C.c_int32),
         ("clock", C.c_void_p),
         ("queue", C.c_void_p),
+        ("stall_test", C.c_int32),
     ]
 
 
@@ -86,6 +91,7 @@ _SIGNATURES = {
     "sw_pitch": ([C.c_int], C.c_int),
     "sw_fdtd_desc_size": ([], _sz),
     "sw_launch_count": ([], C.c_uint64),
+    "sw_host_enqueue_count": ([], C.c_uint64),
     "sw_arf_workspace_bytes": ([C.c_int64, C.c_int32], _sz),
     "sw_arf_envelope": ([C.c_int, _vp, C.c_int64, C.c_int32, _vp, _vp, _sz, _vp], C.c_int),
     "sw_arf_force": ([C.c_int, C.c_int, _vp, _vp, _vp, _vp, C.c_int64, C.c_int32, _vp, C.c_int32,
@@ -127,6 +133,7 @@ _SIGNATURES = {
     "sw_fdtd_init": ([C.POINTER(FdtdDesc), _vp, _vp, _vp], C.c_int),
     "sw_fdtd_steps": ([C.POINTER(FdtdDesc), _i32, _i32, _vp], C.c_int),
     "sw_fdtd_finish": ([C.POINTER(FdtdDesc), _i32, _vp, _vp, _vp], C.c_int),
+    "sw_fdtd_status": ([C.POINTER(FdtdDesc), C.POINTER(C.c_int32), _vp], C.c_int),
     "sw_fdtd_reproject": ([C.POINTER(FdtdDesc), _i32, _f64, C.c_int, _vp, _vp, _sz,
                            C.POINTER(CGStats), _vp], C.c_int),
     "sw_strain": ([C.c_int, _vp, _vp, _vp, _i64, _i64, _i64, C.c_int, C.c_int, C.c_int, _f64,
@@ -188,3 +195,8 @@ def call(name: str, *args) -> None:
 def launch_count() -> int:
     """Kernels launched by the library in this process so far."""
     return int(load().sw_launch_count())
+
+
+def host_enqueue_count() -> int:
+    """Host-side enqueue calls (kernel or graph launches) behind those kernels."""
+    return int(load().sw_host_enqueue_count())

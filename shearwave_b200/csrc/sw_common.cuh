@@ -39,6 +39,11 @@ __host__ __device__ inline Geom make_geom(int nx, int ny, int nz, int pz) {
 
 __host__ __device__ inline int pad_pitch(int nz) { return (nz + 7) & ~7; }
 
+// Solve flag bits (sw_fdtd_desc.flags): bit 0 a non-finite value, bit 1 a
+// step kernel's bounded wait ran out and the CTA abandoned its tiles, bit 2
+// a step launch refused to issue a TMA to a misaligned destination.
+constexpr int kFlagNonFinite = 1, kFlagTimeout = 2, kFlagRefused = 4;
+
 // Thread-block tile of the marching kernels: 32 cells along z (one warp, one
 // coalesced 128 B / 256 B row segment) x TILE_Y rows along y; each thread
 // marches along x over a chunk of planes.
@@ -202,8 +207,11 @@ inline int step_slots(bool mixed = true) {
   return kNumSMs * (mixed ? tune_get(SW_TUNE_STEP_CTAS_PER_SM) : 2);
 }
 int cuda_status(cudaError_t e, const char* what);
-// Count kernel launches issued by this library (exported as sw_launch_count).
-void count_launches(unsigned long long n);
+// Count kernels launched by this library (exported as sw_launch_count) and
+// the host-side enqueue calls that launched them (sw_host_enqueue_count):
+// `host` defaults to `n` (one call per kernel); a graph launch enqueues many
+// kernels with one call.
+void count_launches(unsigned long long n, unsigned long long host = ~0ull);
 
 #define SW_CHECK_LAUNCH(what)                                   \
   do {                                                          \

@@ -17,11 +17,14 @@ void set_error(const char* fmt, ...) {
   va_end(ap);
 }
 
-static std::atomic<unsigned long long> g_launches{0};
+static std::atomic<unsigned long long> g_launches{0}, g_enqueues{0};
 
-void count_launches(unsigned long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+void count_launches(unsigned long long n, unsigned long long host) {
+  g_launches.fetch_add(n, std::memory_order_relaxed);
+  g_enqueues.fetch_add(host == ~0ull ? n : host, std::memory_order_relaxed);
+}
 
-static std::atomic<int> g_tune[SW_TUNE_COUNT] = {{2}, {8}, {0}, {0}, {0}};
+static std::atomic<int> g_tune[SW_TUNE_COUNT] = {{2}, {8}, {0}, {0}, {0}, {3906250}};
 
 int tune_get(int knob) { return (knob >= 0 && knob < SW_TUNE_COUNT) ? g_tune[knob].load() : -1; }
 
@@ -48,9 +51,11 @@ extern "C" size_t sw_fdtd_desc_size(void) { return sizeof(sw_fdtd_desc); }
 
 extern "C" uint64_t sw_launch_count(void) { return sw::g_launches.load(); }
 
+extern "C" uint64_t sw_host_enqueue_count(void) { return sw::g_enqueues.load(); }
+
 extern "C" int sw_tune_set(int knob, int value) {
-  static const int lo[SW_TUNE_COUNT] = {1, 1, 0, 0, 0};
-  static const int hi[SW_TUNE_COUNT] = {2, 64, 1 << 20, 2, 2};
+  static const int lo[SW_TUNE_COUNT] = {1, 1, 0, 0, 0, 1};
+  static const int hi[SW_TUNE_COUNT] = {2, 64, 1 << 20, 2, 2, 4000000};
   if (knob < 0 || knob >= SW_TUNE_COUNT || value < lo[knob] || value > hi[knob]) {
     sw::set_error("sw_tune_set: knob %d does not take the value %d", knob, value);
     return SW_EINVAL;

@@ -152,139 +152,229 @@ __global__ void __launch_bounds__(TILE_THREADS) cg_prep(const CgInst* __restrict
 // ---------------------------------------------------------------------------
 // apply: p_k (fused update), Ap = A p_k, partial p_k.Ap
 // ---------------------------------------------------------------------------
+// Loads of data that other blocks of the same launch may have written: the
+// persistent kernel (COH) reads them from L2 (ld.global.cg), since a block's
+// L1 can hold lines from an earlier iteration; separate launches may use L1.
+template <bool COH, typename T>
+__device__ __forceinline__ T ldv(const T* p) {
+  if (COH) return __ldcg(p);
+  return *p;
+}
+
+template <bool COH>
 struct PView {
   const double* r;
   const double* pold;
   double beta;
   bool first;
   __device__ inline double operator()(long long i) const {
-    return first ? pold[i] : fma(beta, pold[i], r[i]);
+    return first ? ldv<COH>(pold + i) : fma(beta, ldv<COH>(pold + i), ldv<COH>(r + i));
   }
 };
+
+// One tile of the apply phase (every thread of the block; uniform control).
+template <bool COH>
+__device__ __forceinline__ void apply_tile(const CgInst* __restrict__ tab, int ninst, int t,
+                                           double* red, unsigned int* lastflag) {
+  const int ii = find_inst(tab, ninst, t);
+  const CgInst& in = tab[ii];
+  const CgState* st = in.st;
+  if (ldv<COH>(&st->reason) != SW_CG_RUNNING) return;  // uniform across the block
+  const Geom& g = in.g;
+  const int k = ldv<COH>(&st->k);
+  PView<COH> pv;
+  pv.first = (k == 0);
+  pv.r = in.r;
+  pv.beta = ldv<COH>(&st->beta);
+  pv.pold = pv.first ? in.p0 : ((k - 1) & 1 ? in.p1 : in.p0);
+  double* pnew = (k & 1) ? in.p1 : in.p0;
+  const int local = t - in.tile_base;
+  const TileCoord tc = tile_coord(g, in.ts, local);
+  const int z = tc.z0 + threadIdx.x, y = tc.y0 + threadIdx.y;
+  double acc = 0.0;
+  for (int x = tc.x0; x < tc.x1; ++x) {
+    if (!interior(g, x, y, z)) continue;
+    const long long i = (long long)x * g.sxy + (long long)y * g.pz + z;
+    const double pc = pv(i);
+    if (in.op == 1) {  // -mu L7(p), laplacian_center's operation order
+      const double lap = ((pv(i + g.sxy) - 2.0 * pc) + pv(i - g.sxy)) * in.ihx2 +
+                         ((pv(i + g.pz) - 2.0 * pc) + pv(i - g.pz)) * in.ihy2 +
+                         ((pv(i + 1) - 2.0 * pc) + pv(i - 1)) * in.ihz2;
+      const double ap = -in.muf[i] * lap;
+      in.ap[i] = ap;
+      if (!pv.first) pnew[i] = pc;
+      acc += pc * ap;
+      continue;
+    }
+    double gp, gm, tx, ty, tz;
+    gp = (x + 1 <= g.nx - 2) ? (pv(i + 2 * g.sxy) - pc) * in.c2x : 0.0;
+    gm = (x - 1 >= 1) ? (pc - pv(i - 2 * g.sxy)) * in.c2x : 0.0;
+    tx = (gp - gm) * in.c2x;
+    gp = (y + 1 <= g.ny - 2) ? (pv(i + 2 * g.pz) - pc) * in.c2y : 0.0;
+    gm = (y - 1 >= 1) ? (pc - pv(i - 2 * g.pz)) * in.c2y : 0.0;
+    ty = (gp - gm) * in.c2y;
+    gp = (z + 1 <= g.nz - 2) ? (pv(i + 2) - pc) * in.c2z : 0.0;
+    gm = (z - 1 >= 1) ? (pc - pv(i - 2)) * in.c2z : 0.0;
+    tz = (gp - gm) * in.c2z;
+    const double ap = -((tx + ty) + tz);
+    in.ap[i] = ap;
+    if (!pv.first) pnew[i] = pc;
+    acc += pc * ap;
+  }
+  double bs = block_sum(acc, red);
+  if (flat_tid() == 0) in.partials[local] = make_double2(bs, 0.0);
+  if (last_block(in, lastflag)) {
+    double2 tot = reduce_partials(in, red);
+    if (flat_tid() == 0) {
+      CgState* w = in.st;
+      w->ticket = 0u;
+      const double denom = tot.x;
+      const bool stop = (in.op == 1) ? (denom <= 0.0) : (!isfinite(denom) || denom <= 0.0);
+      if (stop) w->reason = SW_CG_BREAKDOWN;
+      else w->alpha = w->rs / denom;
+      __threadfence();
+    }
+  }
+  __syncthreads();
+}
 
 __global__ void __launch_bounds__(TILE_THREADS) cg_apply(const CgInst* __restrict__ tab, int ninst,
                                                          int ntiles) {
   __shared__ double red[32];
   __shared__ unsigned int lastflag;
-  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-    const int ii = find_inst(tab, ninst, t);
-    const CgInst& in = tab[ii];
-    const CgState* st = in.st;
-    if (st->reason != SW_CG_RUNNING) continue;  // uniform across the block
-    const Geom& g = in.g;
-    const int k = st->k;
-    PView pv;
-    pv.first = (k == 0);
-    pv.r = in.r;
-    pv.beta = st->beta;
-    pv.pold = pv.first ? in.p0 : ((k - 1) & 1 ? in.p1 : in.p0);
-    double* pnew = (k & 1) ? in.p1 : in.p0;
-    const int local = t - in.tile_base;
-    const TileCoord tc = tile_coord(g, in.ts, local);
-    const int z = tc.z0 + threadIdx.x, y = tc.y0 + threadIdx.y;
-    double acc = 0.0;
-    for (int x = tc.x0; x < tc.x1; ++x) {
-      if (!interior(g, x, y, z)) continue;
-      const long long i = (long long)x * g.sxy + (long long)y * g.pz + z;
-      const double pc = pv(i);
-      if (in.op == 1) {  // -mu L7(p), laplacian_center's operation order
-        const double lap = ((pv(i + g.sxy) - 2.0 * pc) + pv(i - g.sxy)) * in.ihx2 +
-                           ((pv(i + g.pz) - 2.0 * pc) + pv(i - g.pz)) * in.ihy2 +
-                           ((pv(i + 1) - 2.0 * pc) + pv(i - 1)) * in.ihz2;
-        const double ap = -in.muf[i] * lap;
-        in.ap[i] = ap;
-        if (!pv.first) pnew[i] = pc;
-        acc += pc * ap;
-        continue;
-      }
-      double gp, gm, tx, ty, tz;
-      gp = (x + 1 <= g.nx - 2) ? (pv(i + 2 * g.sxy) - pc) * in.c2x : 0.0;
-      gm = (x - 1 >= 1) ? (pc - pv(i - 2 * g.sxy)) * in.c2x : 0.0;
-      tx = (gp - gm) * in.c2x;
-      gp = (y + 1 <= g.ny - 2) ? (pv(i + 2 * g.pz) - pc) * in.c2y : 0.0;
-      gm = (y - 1 >= 1) ? (pc - pv(i - 2 * g.pz)) * in.c2y : 0.0;
-      ty = (gp - gm) * in.c2y;
-      gp = (z + 1 <= g.nz - 2) ? (pv(i + 2) - pc) * in.c2z : 0.0;
-      gm = (z - 1 >= 1) ? (pc - pv(i - 2)) * in.c2z : 0.0;
-      tz = (gp - gm) * in.c2z;
-      const double ap = -((tx + ty) + tz);
-      in.ap[i] = ap;
-      if (!pv.first) pnew[i] = pc;
-      acc += pc * ap;
-    }
-    double bs = block_sum(acc, red);
-    if (flat_tid() == 0) in.partials[local] = make_double2(bs, 0.0);
-    if (last_block(in, &lastflag)) {
-      double2 tot = reduce_partials(in, red);
-      if (flat_tid() == 0) {
-        CgState* w = in.st;
-        w->ticket = 0u;
-        const double denom = tot.x;
-        const bool stop = (in.op == 1) ? (denom <= 0.0) : (!isfinite(denom) || denom <= 0.0);
-        if (stop) w->reason = SW_CG_BREAKDOWN;
-        else w->alpha = w->rs / denom;
-        __threadfence();
-      }
-    }
-    __syncthreads();
-  }
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x)
+    apply_tile<false>(tab, ninst, t, red, &lastflag);
 }
 
 // ---------------------------------------------------------------------------
 // update: x += alpha p_k, r -= alpha Ap, partial r.r, stopping rule
 // ---------------------------------------------------------------------------
+// Every vector read here was written by this same thread (x, r, Ap, p_k at
+// its own cells), so plain loads are coherent even in the persistent kernel;
+// the scalar state comes from L2 there.
+template <bool COH>
+__device__ __forceinline__ void update_tile(const CgInst* __restrict__ tab, int ninst, int t,
+                                            double* red, unsigned int* lastflag) {
+  const int ii = find_inst(tab, ninst, t);
+  const CgInst& in = tab[ii];
+  const CgState* st = in.st;
+  if (ldv<COH>(&st->reason) != SW_CG_RUNNING) return;
+  const Geom& g = in.g;
+  const int k = ldv<COH>(&st->k);
+  const double alpha = ldv<COH>(&st->alpha);
+  const double* pk = (k & 1) ? in.p1 : in.p0;
+  const int local = t - in.tile_base;
+  const TileCoord tc = tile_coord(g, in.ts, local);
+  const int z = tc.z0 + threadIdx.x, y = tc.y0 + threadIdx.y;
+  double acc = 0.0;
+  for (int x = tc.x0; x < tc.x1; ++x) {
+    if (!interior(g, x, y, z)) continue;
+    const long long i = (long long)x * g.sxy + (long long)y * g.pz + z;
+    in.x[i] = fma(alpha, pk[i], in.x[i]);
+    const double rn = fma(-alpha, in.ap[i], in.r[i]);
+    in.r[i] = rn;
+    acc += rn * rn;
+  }
+  double bs = block_sum(acc, red);
+  if (flat_tid() == 0) in.partials[local] = make_double2(bs, 0.0);
+  if (last_block(in, lastflag)) {
+    double2 tot = reduce_partials(in, red);
+    if (flat_tid() == 0) {
+      CgState* w = in.st;
+      w->ticket = 0u;
+      const double rs_new = tot.x;
+      w->iters += 1;
+      if (in.op == 0 && !isfinite(rs_new)) {
+        w->reason = SW_CG_NONFINITE;
+      } else {
+        const double rel = sqrt(rs_new / w->rs0);
+        w->rel = rel;
+        if (rel < w->tol) {
+          w->reason = SW_CG_CONVERGED;
+        } else {
+          w->beta = rs_new / fmax(w->rs, 2.220446049250313e-16);
+          w->rs = rs_new;
+          w->k += 1;
+          if (w->iters >= w->max_iters) w->reason = SW_CG_MAXITERS;
+        }
+      }
+      __threadfence();
+    }
+  }
+  __syncthreads();
+}
+
 __global__ void __launch_bounds__(TILE_THREADS) cg_update(const CgInst* __restrict__ tab, int ninst,
                                                           int ntiles) {
   __shared__ double red[32];
   __shared__ unsigned int lastflag;
-  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-    const int ii = find_inst(tab, ninst, t);
-    const CgInst& in = tab[ii];
-    const CgState* st = in.st;
-    if (st->reason != SW_CG_RUNNING) continue;
-    const Geom& g = in.g;
-    const int k = st->k;
-    const double alpha = st->alpha;
-    const double* pk = (k & 1) ? in.p1 : in.p0;
-    const int local = t - in.tile_base;
-    const TileCoord tc = tile_coord(g, in.ts, local);
-    const int z = tc.z0 + threadIdx.x, y = tc.y0 + threadIdx.y;
-    double acc = 0.0;
-    for (int x = tc.x0; x < tc.x1; ++x) {
-      if (!interior(g, x, y, z)) continue;
-      const long long i = (long long)x * g.sxy + (long long)y * g.pz + z;
-      in.x[i] = fma(alpha, pk[i], in.x[i]);
-      const double rn = fma(-alpha, in.ap[i], in.r[i]);
-      in.r[i] = rn;
-      acc += rn * rn;
-    }
-    double bs = block_sum(acc, red);
-    if (flat_tid() == 0) in.partials[local] = make_double2(bs, 0.0);
-    if (last_block(in, &lastflag)) {
-      double2 tot = reduce_partials(in, red);
-      if (flat_tid() == 0) {
-        CgState* w = in.st;
-        w->ticket = 0u;
-        const double rs_new = tot.x;
-        w->iters += 1;
-        if (in.op == 0 && !isfinite(rs_new)) {
-          w->reason = SW_CG_NONFINITE;
-        } else {
-          const double rel = sqrt(rs_new / w->rs0);
-          w->rel = rel;
-          if (rel < w->tol) {
-            w->reason = SW_CG_CONVERGED;
-          } else {
-            w->beta = rs_new / fmax(w->rs, 2.220446049250313e-16);
-            w->rs = rs_new;
-            w->k += 1;
-            if (w->iters >= w->max_iters) w->reason = SW_CG_MAXITERS;
-          }
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x)
+    update_tile<false>(tab, ninst, t, red, &lastflag);
+}
+
+// ---------------------------------------------------------------------------
+// persistent CG: every iteration of every instance in one cooperative launch
+// ---------------------------------------------------------------------------
+// The two phases of an iteration are separated by a grid-wide barrier; the
+// per-instance scalars still advance in the "last block" of each phase, so
+// the arithmetic (and the order of every sum) is the two-launch version's.
+// The barrier's waits are bounded: one that runs out sets the error word and
+// every block leaves the loop (the host reports it); nothing spins forever.
+constexpr uint32_t kCgBarrierBudget = 1u << 20;  // units of 1024 cycles (~0.5 s)
+
+__device__ bool cg_grid_sync(CgGrid* b) {
+  __shared__ int ok_s;
+  __syncthreads();
+  if (flat_tid() == 0) {
+    int ok = 1;
+    volatile unsigned int* gen = &b->gen;
+    const unsigned int g0 = *gen;
+    __threadfence();
+    if (atomicAdd(&b->count, 1u) + 1u == gridDim.x) {
+      atomicExch(&b->count, 0u);
+      __threadfence();
+      atomicAdd(&b->gen, 1u);
+    } else {
+      const uint32_t t0 = (uint32_t)clock();
+      while (*gen == g0) {
+        if (*(volatile int*)&b->error) {
+          ok = 0;
+          break;
         }
-        __threadfence();
+        if ((((uint32_t)clock() - t0) >> 10) > kCgBarrierBudget) {
+          atomicExch(&b->error, 1);
+          ok = 0;
+          break;
+        }
+        __nanosleep(64);
       }
     }
+    __threadfence();
+    ok_s = ok;
+  }
+  __syncthreads();
+  return ok_s != 0;
+}
+
+__global__ void __launch_bounds__(TILE_THREADS) cg_persist(const CgInst* __restrict__ tab,
+                                                           int ninst, int ntiles, CgGrid* bar) {
+  __shared__ double red[32];
+  __shared__ unsigned int lastflag;
+  __shared__ int any_s;
+  for (;;) {
+    if (flat_tid() == 0) {
+      int any = 0;
+      for (int i = 0; i < ninst && !any; ++i) any = __ldcg(&tab[i].st->reason) == SW_CG_RUNNING;
+      any_s = any;
+    }
     __syncthreads();
+    if (!any_s) break;  // the same answer in every block: the states changed before a barrier
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x)
+      apply_tile<true>(tab, ninst, t, red, &lastflag);
+    if (!cg_grid_sync(bar)) break;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x)
+      update_tile<true>(tab, ninst, t, red, &lastflag);
+    if (!cg_grid_sync(bar)) break;
   }
 }
 
@@ -327,7 +417,7 @@ size_t cg_workspace_bytes(const Geom& g, const TileSpace& ts) {
   size_t vec = align_up((size_t)g.ncell * sizeof(double), 256);
   size_t b = 6 * vec;                                            // x r p0 p1 ap muf
   b += align_up((size_t)ts.count * sizeof(double2), 256);        // partials
-  b += align_up(sizeof(CgState), 256);                           // state
+  b += align_up(sizeof(CgState), 256);                           // state + grid barrier
   b += align_up(sizeof(CgInst), 256);                            // instance table
   b += align_up(3 * sizeof(void*) + sizeof(InStride) + sizeof(double*), 256);
   return b;
@@ -368,11 +458,45 @@ int cg_layout(const Geom& g, char* ws, size_t ws_bytes, CgInst* in, CgState** st
   return SW_OK;
 }
 
+// Blocks of a cooperative cg_persist launch on the current device (all
+// resident at once), or 0 when the device cannot launch one.
+static int cg_coop_blocks() {
+  int dev = 0, coop = 0, sms = 0, per = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+  if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess || !coop)
+    return 0;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, cg_persist, TILE_THREADS, 0) !=
+      cudaSuccess)
+    return 0;
+  return per * sms;
+}
+
 int cg_run(const CgInst* d_tab, int ninst, int ntiles, CgState* d_states, int nst,
-           cudaStream_t s) {
-  // Launch CG iterations in growing batches; after each batch read every
-  // instance's exit reason (one small D2H copy of the contiguous state
-  // array) and stop when all are done.
+           CgGrid* d_grid, cudaStream_t s) {
+  // One cooperative launch runs every iteration (grid barriers between the
+  // phases); without cooperative launch support, iterations are launched in
+  // growing batches and the host polls the exit reasons between batches.
+  const int coop = d_grid != nullptr ? cg_coop_blocks() : 0;
+  if (coop > 0) {
+    const int grid = std::max(1, std::min(ntiles, coop));
+    cudaError_t e = cudaMemsetAsync(d_grid, 0, sizeof(CgGrid), s);
+    void* args[] = {(void*)&d_tab, (void*)&ninst, (void*)&ntiles, (void*)&d_grid};
+    if (e == cudaSuccess)
+      e = cudaLaunchCooperativeKernel((const void*)cg_persist, dim3(grid),
+                                      dim3(TILE_Z, TILE_Y), args, 0, s);
+    if (e != cudaSuccess) return cuda_status(e, "cg_persist launch");
+    count_launches(1);
+    CgGrid hg{};
+    e = cudaMemcpyAsync(&hg, d_grid, sizeof(hg), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_status(e, "cg_persist readback");
+    if (hg.error) {
+      set_error("CG: a grid barrier of the persistent kernel timed out");
+      return SW_ETIMEOUT;
+    }
+    return SW_OK;
+  }
   const int grid = std::max(1, std::min(ntiles, 148 * 8));
   CgState local[4];  // a single solve polls without touching the heap
   std::vector<CgState> heap(nst > 4 ? nst : 0);
@@ -447,7 +571,7 @@ int project_one(const void* fx, const void* fy, const void* fz, InStride fs, con
     cg_prep<T><<<grid, dim3(TILE_Z, TILE_Y), 0, s>>>(d_tab, 1, ntiles, d_fin, d_fs);
     count_launches(1);
     SW_CHECK_LAUNCH("cg_prep");
-    rc = cg_run(d_tab, 1, ntiles, st, 1, s);
+    rc = cg_run(d_tab, 1, ntiles, st, 1, cg_grid_of(st), s);
     if (rc != SW_OK) return rc;
     cg_finish<T><<<grid, dim3(TILE_Z, TILE_Y), 0, s>>>(d_tab, 1, ntiles, d_fin, d_fs, d_out);
     count_launches(1);
@@ -510,7 +634,7 @@ int static_one(const void* b, const void* mu, double mu_s, InStride fs, const Ge
     cg_prep<T><<<grid, dim3(TILE_Z, TILE_Y), 0, s>>>(d_tab, 1, ntiles, d_fin, d_fs);
     count_launches(1);
     SW_CHECK_LAUNCH("static cg_prep");
-    rc = cg_run(d_tab, 1, ntiles, st, 1, s);
+    rc = cg_run(d_tab, 1, ntiles, st, 1, cg_grid_of(st), s);
     if (rc != SW_OK) return rc;
   }
   e = cudaMemcpyAsync(out, in.x, (size_t)g.ncell * sizeof(double), cudaMemcpyDeviceToDevice, s);
@@ -574,7 +698,7 @@ extern "C" int sw_project(int in_dtype, const void* fx, const void* fy, const vo
 // ---------------------------------------------------------------------------
 namespace {
 struct BatchTableLayout {
-  size_t inst, state, fin, strides, outs, total;
+  size_t inst, state, fin, strides, outs, grid, total;
 };
 BatchTableLayout batch_layout(int n) {
   BatchTableLayout L;
@@ -589,6 +713,8 @@ BatchTableLayout batch_layout(int n) {
   off += align_up((size_t)n * sizeof(InStride), 256);
   L.outs = off;
   off += align_up((size_t)n * sizeof(double*), 256);
+  L.grid = off;
+  off += align_up(sizeof(CgGrid), 256);
   L.total = off;
   return L;
 }
@@ -652,7 +778,7 @@ int project_batch_t(const sw_project_job* jobs, int n, char* table, sw_cg_stats*
                                                      (const InStride*)(table + L.strides));
     count_launches(1);
     SW_CHECK_LAUNCH("cg_prep (batch)");
-    int rc = cg_run(d_tab, n, ntiles, d_states, n, s);
+    int rc = cg_run(d_tab, n, ntiles, d_states, n, (CgGrid*)(table + L.grid), s);
     if (rc != SW_OK) return rc;
     cg_finish<T><<<grid, dim3(TILE_Z, TILE_Y), 0, s>>>(d_tab, n, ntiles,
                                                        (const T* const*)(table + L.fin),

@@ -26,6 +26,19 @@ struct CgState {
   unsigned int ticket;
 };
 
+static_assert(sizeof(CgState) <= 128, "the grid barrier shares the state's 256-byte slot");
+
+// Grid-wide barrier of the persistent CG kernel (zeroed before each launch):
+// arrivals, generation, and an error word set when a wait runs out.
+struct CgGrid {
+  unsigned int count;
+  unsigned int gen;
+  int error;
+  int pad;
+};
+// The barrier of a single solve lives 128 bytes after its state.
+inline CgGrid* cg_grid_of(CgState* st) { return (CgGrid*)((char*)st + 128); }
+
 // One solve in a launch's instance table.
 //   op 0: the projection's Poisson operator A = -div_c(grad_c .)
 //         (src/shearwave/solver.py:1024-1026), rhs = -div_c(mask f);

@@ -88,6 +88,7 @@ int make_step_args(const sw_fdtd_desc* d, StepArgs* a) {
   a->steps_per_pass = d->steps_per_pass;
   a->clock = d->clock;
   a->queue = d->queue;
+  a->stall_test = d->stall_test;
   const int nbuf = 3;
   for (int i = 0; i < nbuf; ++i)
     if (a->state[i] == nullptr) {
@@ -500,6 +501,37 @@ extern "C" int sw_fdtd_finish(const sw_fdtd_desc* d, int32_t steps_done, void* u
                                                                                   u_out, v_out);
   count_launches(1);
   SW_CHECK_LAUNCH("finish");
+  return SW_OK;
+}
+
+extern "C" int sw_fdtd_status(const sw_fdtd_desc* d, int32_t* host_flags, void* stream) {
+  if (d == nullptr) {
+    set_error("sw_fdtd_status: null descriptor");
+    return SW_EINVAL;
+  }
+  int32_t f = 0;
+  if (d->flags != nullptr) {
+    cudaError_t e = cudaMemcpyAsync(&f, d->flags, sizeof f, cudaMemcpyDeviceToHost,
+                                    (cudaStream_t)stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize((cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_status(e, "sw_fdtd_status");
+  } else {
+    cudaError_t e = cudaStreamSynchronize((cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_status(e, "sw_fdtd_status");
+  }
+  if (host_flags != nullptr) *host_flags = f;
+  if (f & kFlagTimeout) {
+    set_error("a step kernel's bounded wait ran out: tiles of this solve were abandoned");
+    return SW_ETIMEOUT;
+  }
+  if (f & kFlagRefused) {
+    set_error("a step launch refused to issue a TMA to a misaligned shared-memory destination");
+    return SW_ETIMEOUT;
+  }
+  if (f & kFlagNonFinite) {
+    set_error("non-finite displacement in the state");
+    return SW_ENONFINITE;
+  }
   return SW_OK;
 }
 

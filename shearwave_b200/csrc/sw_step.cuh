@@ -32,6 +32,7 @@ struct StepArgs {
   int steps_per_pass;  // mixed form: 2 two steps per launch, 0 / 1 one
   int* clock;          // device step counter for graph replays (or null)
   int* queue;          // launch-wide tile queue of one-solve launches (or null)
+  int stall_test;      // testing: leave one ring stage of every tile unarmed
 };
 
 // 7-point Laplacian of the mixed form from the three neighbour-pair sums

@@ -363,12 +363,15 @@ __global__ void __launch_bounds__(TmaF32TB::THREADS, 1)
   uint64_t* Lfull = reinterpret_cast<uint64_t*>(ringL + NL * LF);  // after the rings
   uint64_t* Lempty = Lfull + NL;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  auto flags_of = [&](int k) -> int* { return BATCH ? tab[k].flags : one.flags; };
   if ((smem_addr(ringA) & 127u) != 0u) {
-    int* fl = BATCH ? (ninst > 0 ? tab[0].flags : nullptr) : one.flags;
-    if (threadIdx.x == 0 && fl) atomicOr(fl, 4);
+    if (threadIdx.x == 0)
+      for (int k = 0; k < (BATCH ? ninst : 1); ++k)
+        if (int* fl = flags_of(k)) atomicOr(fl, kFlagRefused);
     queue_cta_done(queue);
     return;
   }
+  AbortLog* lg = abort_log(base);
   if (threadIdx.x == 0) {
     for (int s = 0; s < NA; ++s) {
       mbar_init(&hd->fullA[s], 1);
@@ -383,6 +386,10 @@ __global__ void __launch_bounds__(TmaF32TB::THREADS, 1)
       mbar_init(&Lempty[s], T::CONSUMER_WARPS);
     }
     *abort_flag = 0;
+    abort_flag[1] = BATCH ? (ninst > 0 ? tab[0].wait_k : 1) : one.wait_k;
+    lg->n_taken = 0;
+    lg->armedA = lg->parA = lg->armedB = lg->parB = 0;
+    for (int w = 0; w < 16; ++w) lg->done[w] = 0;
     mbar_fence_init();
   }
   __syncthreads();
@@ -407,7 +414,9 @@ __global__ void __launch_bounds__(TmaF32TB::THREADS, 1)
         const T* in = BATCH ? &tab[k] : &one;
         const int local = BATCH ? t - in->tile_base : t;
         const int lit = it - in->it_begin;
-        if (lit < 0 || lit + 1 >= in->n_steps) continue;
+        if (lit < 0 || lit + 1 >= in->n_steps || solve_abandoned(in->flags)) continue;
+        lg->solve[lg->n_taken & 7] = k;
+        ++lg->n_taken;
         const Geom& g = in->g;
         const TbCoord tc = tb_coord(g, in->ts, local);
         const CUtensorMap* tma = &in->tm[lit % 3];
@@ -418,14 +427,19 @@ __global__ void __launch_bounds__(TmaF32TB::THREADS, 1)
           ok = ok && ws_wait(&hd->emptyA[sa], pa.ph ^ 1u, abort_flag);
           if (!ok) return;
           if (first) {
+            first = false;
+            if (in->stall_test) {  // the testing switch leaves the tile's first stage unarmed
+              pa.next();
+              return;
+            }
             tile_slots(base)[sa] = t;
             solve_slots(base)[sa] = k;
-            first = false;
           }
           const int pl = min(max(p, 0), g.nx - 1);  // planes outside the grid feed only the shell
           fence_proxy_async_smem();
           mbar_arrive_expect_tx(&hd->fullA[sa], T::A_BYTES);
           tma_load_4d(ringA + sa * AF, tma, &hd->fullA[sa], tc.z0 - 4, tc.y0 - 2, pl, 0);
+          arm_record(lg->armedA, lg->parA, sa, pa.ph);
           pa.next();
         };
         auto issueB = [&](int q) {
@@ -436,6 +450,7 @@ __global__ void __launch_bounds__(TmaF32TB::THREADS, 1)
           fence_proxy_async_smem();
           mbar_arrive_expect_tx(&hd->fullB[sb], bbytes);
           tma_load_4d(ringB + sb * BF, &in->tmm, &hd->fullB[sb], tc.z0 - 4, tc.y0 - 1, ql, 0);
+          arm_record(lg->armedB, lg->parB, sb, pb.ph);
           pb.next();
         };
         issueA(tc.x0 - 2);
@@ -460,15 +475,15 @@ __global__ void __launch_bounds__(TmaF32TB::THREADS, 1)
       const int lit = it - in->it_begin;
       p = tb_tile_any(in, local, lit, k, p, warp, lane);
       if (!p.ok) break;
+      if (lane == 0) ++lg->done[warp];
     }
   }
   __syncthreads();
-  if (*abort_flag && threadIdx.x == 0) {
-    int* fl = BATCH ? (ninst > 0 ? tab[0].flags : nullptr) : one.flags;
-    if (fl) atomicOr(fl, 2);
-    const long long t0 = clock64();
-    while (clock64() - t0 < 200000000LL) {
-    }
+  if (*abort_flag && warp == T::CONSUMER_WARPS && lane == 0) {
+    // let every copy still in flight land, then flag the abandoned tiles' solves
+    drain_ring(hd->fullA, lg->armedA, lg->parA, NA);
+    drain_ring(hd->fullB, lg->armedB, lg->parB, NB);
+    flag_unfinished(lg, T::CONSUMER_WARPS, BATCH ? ninst : 1, kFlagTimeout, flags_of);
   }
   queue_cta_done(queue);
 }
@@ -480,7 +495,7 @@ __global__ void __launch_bounds__(TmaF32TB::THREADS, 1)
 // ---------------------------------------------------------------------------
 // alignment slack + header + rings + the level-1 ring's full / empty barriers
 size_t tb_smem_bytes() {
-  return 128 + 256 + (size_t)TmaF32TB::NA * TmaF32TB::A_STAGE +
+  return 128 + kRingOffset + (size_t)TmaF32TB::NA * TmaF32TB::A_STAGE +
          (size_t)TmaF32TB::NB * TmaF32TB::B_STAGE + (size_t)TmaF32TB::NL * TmaF32TB::L_STAGE +
          2 * TmaF32TB::NL * sizeof(uint64_t);
 }
@@ -570,12 +585,18 @@ int make_tma_f32_tb(const StepArgs& a, int xchunk, TmaF32TB* t) {
   t->flags = a.flags;
   t->it_begin = 0;
   t->tile_base = 0;
+  t->wait_k = tune_get(SW_TUNE_WAIT_BUDGET);
+  t->stall_test = a.stall_test;
   return SW_OK;
 }
 
 int launch_fused2_prepare() { return tb_set_attr(); }
 
 const void* step_f32_fused2_ptr() { return reinterpret_cast<const void*>(step_f32_fused2<false>); }
+
+const void* step_f32_fused2_batch_ptr() {
+  return reinterpret_cast<const void*>(step_f32_fused2<true>);
+}
 
 void launch_fused2_raw(const TmaF32TB& t, int it, cudaStream_t s) {
   if (t.ts.count == 0) return;

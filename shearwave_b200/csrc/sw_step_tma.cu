@@ -180,7 +180,7 @@ struct F32Ring {
   static constexpr int C_OFF = 0;                                             // in a B stage
   static constexpr int M_OFF = C_OFF + (KR ? round128(TmaF32::C_BYTES) : 0);  // coefficients
   static constexpr int B_STAGE = M_OFF + round128(TmaF32::M_BYTES);
-  static constexpr size_t SMEM = 128 + 256 + (size_t)NA * STAGE + (size_t)NB * B_STAGE;
+  static constexpr size_t SMEM = 128 + kRingOffset + (size_t)NA * STAGE + (size_t)NB * B_STAGE;
 };
 static_assert(F32Ring<false>::SMEM <= F32Ring<true>::SMEM, "the compact ring must not be larger");
 static_assert(2 * (F32Ring<true>::SMEM + 1024) <= 233472, "two CTAs must fit one SM");
@@ -341,12 +341,15 @@ __global__ void __launch_bounds__(TmaF32::THREADS, TmaF32::MIN_CTAS)
   volatile int* abort_flag = reinterpret_cast<volatile int*>(base + kAbortFlagOffset);
   float* ring = reinterpret_cast<float*>(base + kRingOffset);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  auto flags_of = [&](int k) -> int* { return BATCH ? tab[k].flags : one.flags; };
   if ((smem_addr(ring) & 127u) != 0u) {  // never issue a TMA to a misaligned destination
-    int* fl = BATCH ? (ninst > 0 ? tab[0].flags : nullptr) : one.flags;
-    if (threadIdx.x == 0 && fl) atomicOr(fl, 4);
+    if (threadIdx.x == 0)
+      for (int k = 0; k < (BATCH ? ninst : 1); ++k)
+        if (int* fl = flags_of(k)) atomicOr(fl, kFlagRefused);
     queue_cta_done(queue);
     return;
   }
+  AbortLog* lg = abort_log(base);
   if (threadIdx.x == 0) {
     for (int s = 0; s < NA; ++s) {
       mbar_init(&hd->fullA[s], 1);
@@ -357,6 +360,10 @@ __global__ void __launch_bounds__(TmaF32::THREADS, TmaF32::MIN_CTAS)
       mbar_init(&hd->emptyB[s], TmaF32::CONSUMER_WARPS);
     }
     *abort_flag = 0;
+    abort_flag[1] = BATCH ? (ninst > 0 ? tab[0].wait_k : 1) : one.wait_k;
+    lg->n_taken = 0;
+    lg->armedA = lg->parA = lg->armedB = lg->parB = 0;
+    for (int w = 0; w < 16; ++w) lg->done[w] = 0;
     mbar_fence_init();
   }
   __syncthreads();
@@ -380,7 +387,9 @@ __global__ void __launch_bounds__(TmaF32::THREADS, TmaF32::MIN_CTAS)
         const TmaF32* in = BATCH ? &tab[k] : &one;
         const int local = BATCH ? t - in->tile_base : t;
         const int lit = it - in->it_begin;
-        if (lit < 0 || lit >= in->n_steps) continue;
+        if (lit < 0 || lit >= in->n_steps || solve_abandoned(in->flags)) continue;
+        lg->solve[lg->n_taken & 7] = k;
+        ++lg->n_taken;
         const TileCoord tc = tile_coord_t(in->g, in->ts, local, TZW, TYH);
         const CUtensorMap* tma = &in->tm[lit % 3];
         const CUtensorMap* tmc = &in->tmc[lit % 3];
@@ -389,13 +398,17 @@ __global__ void __launch_bounds__(TmaF32::THREADS, TmaF32::MIN_CTAS)
         for (int p = tc.x0 - 1; p <= tc.x1 && !*abort_flag; ++p) {
           const int sa = pa.s;
           if (!ws_wait(&hd->emptyA[sa], pa.ph ^ 1u, abort_flag)) break;
-          if (p == tc.x0 - 1) {
-            tile_slots(base)[sa] = t;
-            solve_slots(base)[sa] = k;
+          // the testing switch leaves the tile's first stage unarmed
+          if (!(p == tc.x0 - 1 && in->stall_test)) {
+            if (p == tc.x0 - 1) {
+              tile_slots(base)[sa] = t;
+              solve_slots(base)[sa] = k;
+            }
+            fence_proxy_async_smem();
+            mbar_arrive_expect_tx(&hd->fullA[sa], A_BYTES);
+            tma_load_4d(ring + sa * SF, tma, &hd->fullA[sa], tc.z0 - 4, tc.y0 - 1, p, 0);
+            arm_record(lg->armedA, lg->parA, sa, pa.ph);
           }
-          fence_proxy_async_smem();
-          mbar_arrive_expect_tx(&hd->fullA[sa], A_BYTES);
-          tma_load_4d(ring + sa * SF, tma, &hd->fullA[sa], tc.z0 - 4, tc.y0 - 1, p, 0);
           pa.next();
           if (p >= tc.x0 && p < tc.x1) {  // planes x0..x1-1 also need their point-wise inputs
             const int sb = pb.s;
@@ -405,6 +418,7 @@ __global__ void __launch_bounds__(TmaF32::THREADS, TmaF32::MIN_CTAS)
             mbar_arrive_expect_tx(&hd->fullB[sb], pbytes);
             if (kahan) tma_load_4d(sbp + CF, tmc, &hd->fullB[sb], tc.z0, tc.y0, p, 6);
             tma_load_4d(sbp + MF, &in->tmm, &hd->fullB[sb], tc.z0, tc.y0, p, 0);
+            arm_record(lg->armedB, lg->parB, sb, pb.ph);
             pb.next();
           }
         }
@@ -422,16 +436,15 @@ __global__ void __launch_bounds__(TmaF32::THREADS, TmaF32::MIN_CTAS)
       const int local = BATCH ? t - in->tile_base : t;
       const int lit = it - in->it_begin;
       if (!f32_tile_any<TZW, KR>(in, local, lit, q, warp, lane)) break;
+      if (lane == 0) ++lg->done[warp];
     }
   }
   __syncthreads();
-  if (*abort_flag && threadIdx.x == 0) {
-    int* fl = BATCH ? (ninst > 0 ? tab[0].flags : nullptr) : one.flags;
-    if (fl) atomicOr(fl, 2);
-    // bounded drain: let any copy still in flight land before the CTA exits
-    const long long t0 = clock64();
-    while (clock64() - t0 < 200000000LL) {
-    }
+  if (*abort_flag && warp == TmaF32::CONSUMER_WARPS && lane == 0) {
+    // let every copy still in flight land, then flag the abandoned tiles' solves
+    drain_ring(hd->fullA, lg->armedA, lg->parA, NA);
+    drain_ring(hd->fullB, lg->armedB, lg->parB, NB);
+    flag_unfinished(lg, TmaF32::CONSUMER_WARPS, BATCH ? ninst : 1, kFlagTimeout, flags_of);
   }
   queue_cta_done(queue);
 }
@@ -455,12 +468,15 @@ __global__ void __launch_bounds__(TmaF64::THREADS, 2)
   double* ringA = reinterpret_cast<double*>(base + kRingOffset);
   double* ringB = ringA + NA * AD;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  auto flags_of = [&](int k) -> int* { return BATCH ? tab[k].flags : one.flags; };
   if ((smem_addr(ringA) & 127u) != 0u) {
-    int* fl = BATCH ? (ninst > 0 ? tab[0].flags : nullptr) : one.flags;
-    if (threadIdx.x == 0 && fl) atomicOr(fl, 4);
+    if (threadIdx.x == 0)
+      for (int k = 0; k < (BATCH ? ninst : 1); ++k)
+        if (int* fl = flags_of(k)) atomicOr(fl, kFlagRefused);
     queue_cta_done(queue);
     return;
   }
+  AbortLog* lg = abort_log(base);
   if (threadIdx.x == 0) {
     for (int s = 0; s < NA; ++s) {
       mbar_init(&hd->fullA[s], 1);
@@ -471,6 +487,10 @@ __global__ void __launch_bounds__(TmaF64::THREADS, 2)
       mbar_init(&hd->emptyB[s], TmaF64::CONSUMER_WARPS);
     }
     *abort_flag = 0;
+    abort_flag[1] = BATCH ? (ninst > 0 ? tab[0].wait_k : 1) : one.wait_k;
+    lg->n_taken = 0;
+    lg->armedA = lg->parA = lg->armedB = lg->parB = 0;
+    for (int w = 0; w < 16; ++w) lg->done[w] = 0;
     mbar_fence_init();
   }
   __syncthreads();
@@ -493,7 +513,9 @@ __global__ void __launch_bounds__(TmaF64::THREADS, 2)
         const TmaF64* in = BATCH ? &tab[k] : &one;
         const int local = BATCH ? t - in->tile_base : t;
         const int lit = it - in->it_begin;
-        if (lit < 0 || lit >= in->n_steps) continue;
+        if (lit < 0 || lit >= in->n_steps || solve_abandoned(in->flags)) continue;
+        lg->solve[lg->n_taken & 7] = k;
+        ++lg->n_taken;
         const TileCoord tc = tile_coord_t(in->g, in->ts, local, TZ, TY);
         const CUtensorMap* tmp = &in->tm[lit % 3];
         const CUtensorMap* tmc = &in->tm[(lit + 1) % 3];
@@ -501,14 +523,19 @@ __global__ void __launch_bounds__(TmaF64::THREADS, 2)
         for (int p = tc.x0 - 1; p <= tc.x1 && !*abort_flag; ++p) {
           const int sa = pa.s;
           if (!ws_wait(&hd->emptyA[sa], pa.ph ^ 1u, abort_flag)) break;
-          if (p == tc.x0 - 1) {
-            tile_slots(base)[sa] = t;
-            solve_slots(base)[sa] = k;
+          // the testing switch leaves the tile's first stage unarmed
+          if (!(p == tc.x0 - 1 && in->stall_test)) {
+            if (p == tc.x0 - 1) {
+              tile_slots(base)[sa] = t;
+              solve_slots(base)[sa] = k;
+            }
+            fence_proxy_async_smem();
+            mbar_arrive_expect_tx(&hd->fullA[sa], 2 * TmaF64::BOX_BYTES);
+            tma_load_4d(ringA + sa * AD, tmp, &hd->fullA[sa], tc.z0 - 2, tc.y0 - 1, p, 0);
+            tma_load_4d(ringA + sa * AD + HALF, tmc, &hd->fullA[sa], tc.z0 - 2, tc.y0 - 1, p,
+                        0);
+            arm_record(lg->armedA, lg->parA, sa, pa.ph);
           }
-          fence_proxy_async_smem();
-          mbar_arrive_expect_tx(&hd->fullA[sa], 2 * TmaF64::BOX_BYTES);
-          tma_load_4d(ringA + sa * AD, tmp, &hd->fullA[sa], tc.z0 - 2, tc.y0 - 1, p, 0);
-          tma_load_4d(ringA + sa * AD + HALF, tmc, &hd->fullA[sa], tc.z0 - 2, tc.y0 - 1, p, 0);
           pa.next();
           if (p >= tc.x0 && p < tc.x1) {
             const int sb = pb.s;
@@ -516,6 +543,7 @@ __global__ void __launch_bounds__(TmaF64::THREADS, 2)
             fence_proxy_async_smem();
             mbar_arrive_expect_tx(&hd->fullB[sb], bbytes);
             tma_load_4d(ringB + sb * BD, &in->tmm, &hd->fullB[sb], tc.z0, tc.y0, p, 0);
+            arm_record(lg->armedB, lg->parB, sb, pb.ph);
             pb.next();
           }
         }
@@ -641,15 +669,15 @@ __global__ void __launch_bounds__(TmaF64::THREADS, 2)
       if (!ok) break;
       __syncwarp();
       if (lane == 0) mbar_arrive(&hd->emptyA[s_cur]);  // the closing halo plane x1
+      if (lane == 0) ++lg->done[warp];
     }
   }
   __syncthreads();
-  if (*abort_flag && threadIdx.x == 0) {
-    int* fl = BATCH ? (ninst > 0 ? tab[0].flags : nullptr) : one.flags;
-    if (fl) atomicOr(fl, 2);
-    const long long t0 = clock64();
-    while (clock64() - t0 < 200000000LL) {
-    }
+  if (*abort_flag && warp == TmaF64::CONSUMER_WARPS && lane == 0) {
+    // let every copy still in flight land, then flag the abandoned tiles' solves
+    drain_ring(hd->fullA, lg->armedA, lg->parA, NA);
+    drain_ring(hd->fullB, lg->armedB, lg->parB, NB);
+    flag_unfinished(lg, TmaF64::CONSUMER_WARPS, BATCH ? ninst : 1, kFlagTimeout, flags_of);
   }
   queue_cta_done(queue);
 }
@@ -660,7 +688,7 @@ __global__ void __launch_bounds__(TmaF64::THREADS, 2)
 // dynamic shared memory: alignment slack + header + ring A + ring B
 size_t tma_smem_bytes(int precision) {
   if (precision == SW_PLAIN_F64)
-    return 128 + 256 + (size_t)TmaF64::NA * TmaF64::A_STAGE + (size_t)TmaF64::NB * TmaF64::B_STAGE;
+    return 128 + kRingOffset + (size_t)TmaF64::NA * TmaF64::A_STAGE + (size_t)TmaF64::NB * TmaF64::B_STAGE;
   return F32Ring<true>::SMEM;  // the larger of the two mixed layouts
 }
 
@@ -834,6 +862,8 @@ int make_tma_f32(const StepArgs& a, int xchunk, TmaF32* t, int tzw) {
   t->flags = a.flags;
   t->it_begin = 0;
   t->tile_base = 0;
+  t->wait_k = tune_get(SW_TUNE_WAIT_BUDGET);
+  t->stall_test = a.stall_test;
   return SW_OK;
 }
 
@@ -881,6 +911,8 @@ int make_tma_f64(const StepArgs& a, int xchunk, TmaF64* t) {
   t->flags = a.flags;
   t->it_begin = 0;
   t->tile_base = 0;
+  t->wait_k = tune_get(SW_TUNE_WAIT_BUDGET);
+  t->stall_test = a.stall_test;
   return SW_OK;
 }
 
@@ -892,10 +924,13 @@ __global__ void clock_add(int* c, int by) { *c += by; }
 // 0, per_launch, ...) reading the step counter `clock`, then a node that
 // advances the counter.  Returns the number of steps enqueued this way (0
 // when the run is too short to be worth a graph).  Kernel nodes are built
-// explicitly, so the caller's stream may be the legacy default stream.
+// explicitly, so the caller's stream may be the legacy default stream.  A
+// batched launch passes its device table (`tab`, `ninst` solves, `ntiles`
+// tiles; `t` unused); a lone solve passes `t` and tab = nullptr.
 template <typename Inst>
 int graph_loop(void* func, const Inst& t, int grid, int threads, size_t smem, int per_launch,
-               int seg, int* clock, int* queue, int it0, int nsteps, cudaStream_t s, int* done) {
+               int seg, int* clock, int* queue, int it0, int nsteps, cudaStream_t s, int* done,
+               const Inst* tab = nullptr, int ninst = 1, int ntiles = -1) {
   *done = 0;
   const int seg_steps = per_launch * seg;
   const int reps = nsteps / seg_steps;
@@ -904,8 +939,7 @@ int graph_loop(void* func, const Inst& t, int grid, int threads, size_t smem, in
   cudaGraphExec_t ex = nullptr;
   cudaError_t e = cudaGraphCreate(&g, 0);
   cudaGraphNode_t prev = nullptr;
-  const Inst* tab = nullptr;
-  int ninst = 1, ntiles = t.ts.count;
+  if (ntiles < 0) ntiles = t.ts.count;
   const int* itd = clock;
   int* queues = queue;
   std::vector<int> offs(seg);
@@ -944,7 +978,7 @@ int graph_loop(void* func, const Inst& t, int grid, int threads, size_t smem, in
   if (ex) cudaGraphExecDestroy(ex);  // freed once the enqueued replays complete
   if (g) cudaGraphDestroy(g);
   if (e != cudaSuccess) return cuda_status(e, "step-loop graph");
-  count_launches((unsigned long long)reps * (seg + 1) + 1);
+  count_launches((unsigned long long)reps * (seg + 1) + 1, (unsigned long long)reps + 1);
   *done = reps * seg_steps;
   return SW_OK;
 }
@@ -1143,7 +1177,8 @@ int build_batch(const sw_fdtd_desc* descs, const int32_t* begins, int n, int it,
 }
 
 // A batch table starts with the two launch-wide tile queues (zeroed at the
-// start of every call); the solve arrays follow at kBatchHeader.
+// start of every call) and the step counter of graph replays; the solve
+// arrays follow at kBatchHeader.
 constexpr size_t kBatchHeader = 256;
 
 // Mixed form: two steps per launch whenever every running solve runs both
@@ -1206,7 +1241,10 @@ int batch_steps_mixed(const sw_fdtd_desc* descs, const int32_t* begins, int n, i
           int rc = make_step_args(&descs[i], &a);
           if (rc != SW_OK) return rc;
           TmaF32TB t;
-          rc = make_tma_f32_tb(a, descs[i].xchunk > 0 ? descs[i].xchunk : 32, &t);
+          // planes per x chunk: the solve's own, else the SW_TUNE_XCHUNK knob,
+          // else 32 (each chunk re-reads four halo planes of level 0)
+          const int kx = tune_get(SW_TUNE_XCHUNK);
+          rc = make_tma_f32_tb(a, descs[i].xchunk > 0 ? descs[i].xchunk : (kx > 0 ? kx : 32), &t);
           if (rc != SW_OK) return rc;
           t.it_begin = begins ? begins[i] : 0;
           t.tile_base = ntiles;
@@ -1228,6 +1266,30 @@ int batch_steps_mixed(const sw_fdtd_desc* descs, const int32_t* begins, int n, i
     }
     int rc;
     if (kind == 1) {
+      // the steps from `it` on that keep this set of running solves (in
+      // pairs): long runs replay one CUDA graph of 16 fused launches that
+      // reads the step counter in the table header
+      int stop = it;
+      while (stop + 1 < end) {
+        bool same = true;
+        for (int i = 0; i < n && same; ++i)
+          same = active(i, stop) == (cur[i] != 0) && active(i, stop + 1) == (cur[i] != 0);
+        if (!same) break;
+        stop += 2;
+      }
+      if (stop - it >= 64) {
+        int done = 0;
+        TmaF32TB dummy{};
+        rc = graph_loop<TmaF32TB>(const_cast<void*>(step_f32_fused2_batch_ptr()), dummy,
+                                  std::min(ntiles, kNumSMs), TmaF32TB::THREADS, tb_smem_bytes(),
+                                  2, 16, queues + 2, queues, it, stop - it, s, &done,
+                                  (const TmaF32TB*)tab_fused, (int)tfused.size(), ntiles);
+        if (rc != SW_OK) return rc;
+        if (done > 0) {
+          it += done;
+          continue;
+        }
+      }
       rc = launch_fused2_batch(tab_fused, (int)tfused.size(), ntiles, it, queues, s);
       it += 2;
     } else {
@@ -1276,6 +1338,36 @@ int batch_steps(int precision, const sw_fdtd_desc* descs, const int32_t* begins,
       have = true;
     }
     if (tab.empty()) continue;
+    if (std::is_same<Inst, TmaF64>::value) {
+      // the steps from `it` on that keep this set of running solves replay
+      // one CUDA graph of 32 launches reading the counter in the table header
+      int stop = it;
+      while (stop < it0 + nsteps) {
+        bool same = true;
+        for (int i = 0; i < n && same; ++i) {
+          const int lit = stop - (begins ? begins[i] : 0);
+          same = ((lit >= 0 && lit < descs[i].n_steps) ? 1 : 0) == active[i];
+        }
+        if (!same) break;
+        ++stop;
+      }
+      if (stop - it >= 64) {
+        int rc = set_smem_attr(precision);
+        if (rc != SW_OK) return rc;
+        int done = 0;
+        TmaF64 dummy{};
+        rc = graph_loop<TmaF64>(reinterpret_cast<void*>(step_f64_tma<true>), dummy,
+                                std::min(ntiles, step_slots(false)), TmaF64::THREADS,
+                                tma_smem_bytes(precision), 1, 32, queues + 2, queues, it,
+                                stop - it, s, &done, (const TmaF64*)table, (int)tab.size(),
+                                ntiles);
+        if (rc != SW_OK) return rc;
+        if (done > 0) {
+          it += done - 1;  // the loop's ++it advances the last one
+          continue;
+        }
+      }
+    }
     int rc = launch_steps_tma_batch(precision, table, (int)tab.size(), ntiles, it, queues, 0,
                                     false, s);
     if (rc != SW_OK) return rc;

@@ -53,6 +53,8 @@ struct TmaF32 {
   int* flags;
   int it_begin;   // launch step index of this solve's step 0
   int tile_base;  // first global tile of this solve in a batched launch
+  int wait_k;     // wait budget, units of 1024 cycles (SW_TUNE_WAIT_BUDGET)
+  int stall_test; // testing switch: sw_fdtd_desc.stall_test
 };
 
 // Kernel-side view of one plain-FP64 solve.
@@ -87,6 +89,8 @@ struct TmaF64 {
   int* flags;
   int it_begin;
   int tile_base;
+  int wait_k;
+  int stall_test;
 };
 
 // Kernel-side view of one mixed-form solve for the two-steps-per-pass kernel
@@ -133,6 +137,8 @@ struct TmaF32TB {
   int* flags;
   int it_begin;
   int tile_base;
+  int wait_k;
+  int stall_test;
 };
 
 size_t tma_smem_bytes(int precision);
@@ -142,6 +148,7 @@ int launch_fused2(const StepArgs& a, int xchunk, int it, cudaStream_t s);
 int launch_fused2_prepare();                                   // kernel attributes, once
 void launch_fused2_raw(const TmaF32TB& t, int it, cudaStream_t s);  // enqueue one launch
 const void* step_f32_fused2_ptr();  // the single-solve fused kernel (for graph nodes)
+const void* step_f32_fused2_batch_ptr();  // the batched fused kernel (for graph nodes)
 int launch_fused2_batch(const void* d_tab, int ninst, int ntiles, int it, int* queues,
                         cudaStream_t s);
 int tma_xchunk(const Geom& g, int tz, int ty, long long want_tiles);

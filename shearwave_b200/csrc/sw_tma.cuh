@@ -86,16 +86,51 @@ __device__ inline void mbar_arrive(uint64_t* bar) {
 }
 
 // Shared-memory header of the warp-specialised kernels: the mbarriers at
-// offset 0, the abort flag at offset 192, the tile hand-off slots at 200, the
-// rings from offset 256.
+// offset 0, the control words (abort flag, wait budget) at offset 192, the
+// tile hand-off slots at 200, the abort log at 256, the rings from offset 384.
 struct WsHeader {
   uint64_t fullA[6], emptyA[6], fullB[4], emptyB[4];  // 160 bytes
 };
 static_assert(sizeof(WsHeader) <= 192, "header overlaps the abort flag");
 constexpr int kAbortFlagOffset = 192;
 constexpr int kTileSlotOffset = 200;  // int tile[6], then int solve[6]
-constexpr int kRingOffset = 256;
-static_assert(kTileSlotOffset + 48 <= kRingOffset, "tile slots overlap the rings");
+constexpr int kLogOffset = 256;
+constexpr int kRingOffset = 384;
+static_assert(kTileSlotOffset + 48 <= kLogOffset, "tile slots overlap the abort log");
+
+// What a CTA needs to know, after an abort, about the tiles it had taken:
+// the producer records the solve (table index) of every tile it takes and
+// will load, in take order; each consumer warp counts the tiles it has
+// finished.  Tiles from the smallest finished count to the taken count are
+// incomplete, and so are their solves.  A ring holds at most a few tiles, so
+// eight entries cover the window between the slowest warp and the producer.
+struct AbortLog {
+  int solve[8];  // solve of taken tile n at n & 7
+  int n_taken;
+  int done[16];  // tiles finished by consumer warp w
+  // the stages of rings A and B that the producer armed with a copy, and the
+  // phase parity of each stage's latest copy (one bit per stage)
+  uint32_t armedA, parA, armedB, parB;
+};
+static_assert(kLogOffset + (int)sizeof(AbortLog) <= kRingOffset, "abort log overlaps the rings");
+__device__ inline AbortLog* abort_log(unsigned char* base) {
+  return reinterpret_cast<AbortLog*>(base + kLogOffset);
+}
+
+// Record that the producer armed stage s of a ring with a copy whose phase
+// has parity ph.  After an abort the producer waits (bounded) for the latest
+// phase of every armed stage, so that no copy is still landing in shared
+// memory when the CTA exits.  The record lives in shared memory, so it holds
+// no register in the consumers' loops.
+__device__ inline void arm_record(uint32_t& armed, uint32_t& par, int s, uint32_t ph) {
+  armed |= 1u << s;
+  par = (par & ~(1u << s)) | (ph << s);
+}
+constexpr long long kDrainBudget = 1LL << 28;
+__device__ inline void drain_ring(uint64_t* full, uint32_t armed, uint32_t par, int n) {
+  for (int s = 0; s < n; ++s)
+    if ((armed >> s) & 1u) (void)mbar_wait_bounded(&full[s], (par >> s) & 1u, kDrainBudget);
+}
 
 // Tile hand-off: the producer picks the CTA's tiles (a fixed stride over the
 // tile range, or the next tile of a launch-wide queue) and writes the tile
@@ -160,17 +195,47 @@ __device__ inline int find_solve(const Inst* __restrict__ tab, int ninst, int t)
 }
 
 // A bounded wait that also gives up as soon as another thread has aborted.
+// `abort_flag` points at the CTA's two control words in shared memory: the
+// abort flag, then the wait budget in units of 1024 cycles (read only once a
+// test has failed, so the budget costs the fast path no register).
 __device__ inline bool ws_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag) {
   if (mbar_try_wait(bar, parity)) return true;
-  const long long t0 = clock64();
+  // 32-bit cycle counter: differences are exact below 2^32 cycles, and the
+  // budget stays below that (at most 4e6 units of 1024 cycles, under the
+  // 2^22 - 1 units a 32-bit difference can reach, so every wait can end)
+  const uint32_t t0 = (uint32_t)clock();
   while (!mbar_try_wait(bar, parity)) {
     if (*abort_flag) return false;
-    if (clock64() - t0 > 4000000000LL) {
+    if ((((uint32_t)clock() - t0) >> 10) > (uint32_t)abort_flag[1]) {
       *abort_flag = 1;
       return false;
     }
   }
   return true;
+}
+
+// After an abort: set `bit` in the flags of every solve with a tile this CTA
+// took and did not finish (all solves when the log cannot tell).  `flags_of(k)`
+// gives solve k's flag word (or null).
+template <typename FlagsOf>
+__device__ inline void flag_unfinished(const AbortLog* lg, int nwarps, int ninst, int bit,
+                                       FlagsOf flags_of) {
+  int lo = lg->n_taken;
+  for (int w = 0; w < nwarps; ++w) lo = min(lo, lg->done[w]);
+  if (lg->n_taken - lo > 8 || lo < 0) {
+    for (int k = 0; k < ninst; ++k)
+      if (int* fl = flags_of(k)) atomicOr(fl, bit);
+    return;
+  }
+  for (int n = lo; n < lg->n_taken; ++n)
+    if (int* fl = flags_of(lg->solve[n & 7])) atomicOr(fl, bit);
+}
+
+// Whether a solve has already been abandoned in an earlier launch (its
+// state is incomplete, so its remaining steps are skipped).
+__device__ inline bool solve_abandoned(const int* flags) {
+  return flags != nullptr && ((*reinterpret_cast<const volatile int*>(flags)) &
+                              (kFlagTimeout | kFlagRefused)) != 0;
 }
 
 // Resolve the tile's instance and local step; false if the tile is idle.

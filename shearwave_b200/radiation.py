@@ -15,8 +15,8 @@ from __future__ import annotations
 import numpy as np
 import torch
 
-from . import _native
-from ._device import dtype_code, is_tensor, require_cuda, stream_handle, to_device
+from . import ops
+from ._device import is_tensor, require_cuda, to_device
 
 __all__ = ["compute_radiation_force", "compute_radiation_force_velocity", "auto_gate"]
 
@@ -60,13 +60,7 @@ def auto_gate(p) -> np.ndarray:
     dt = _dtype_of(p) or torch.float32
     t = _record(p, dt, dev)
     nx, ny, nz, nt = t.shape
-    ncell = nx * ny * nz
-    ws = torch.empty(max(1, int(_native.load().sw_arf_workspace_bytes(ncell, nt))),
-                     dtype=torch.uint8, device=dev)
-    env = torch.empty(nt, dtype=torch.float64, device=dev)
-    _native.call("sw_arf_envelope", dtype_code(dt), t.data_ptr(), ncell, nt, env.data_ptr(),
-                 ws.data_ptr(), ws.numel(), stream_handle())
-    e = env.cpu().numpy()
+    e = ops.arf_envelope(t, nx * ny * nz, nt).cpu().numpy()
     mask = e >= 0.1 * e.max()
     return np.nonzero(mask)[0] if mask.any() else np.arange(nt)
 
@@ -101,14 +95,10 @@ def _force(records, c_map, rho_map, alpha_coeff_map, f0, gate):
     if len(strides) > 1:  # mix of scalars and fields: broadcast the scalars
         maps = [(m.expand(ncell).contiguous() if s == 0 else m, 1) for m, s in maps]
     stride = maps[0][1]
-    nf = 1 if len(recs) == 1 else 3  # pressure alone, or pressure and 3 velocity components
-    outs = [torch.empty((nx, ny, nz), dtype=dt_out, device=dev) for _ in range(nf)]
-    q = [r.data_ptr() for r in recs[1:]] if nf == 3 else [None, None, None]
-    o = [x.data_ptr() for x in outs] + [None] * (3 - nf)
-    _native.call("sw_arf_force", dtype_code(dt_in), nf, recs[0].data_ptr(), *q, ncell, nt,
-                 g.data_ptr(), int(g.numel()), maps[0][0].data_ptr(), maps[1][0].data_ptr(),
-                 maps[2][0].data_ptr(), stride, float(f0), dtype_code(dt_out), *o,
-                 stream_handle())
+    # pressure alone, or pressure and 3 velocity components
+    vel = recs[1:] if len(recs) == 4 else [None, None, None]
+    outs = ops.arf_force(recs[0], *vel, [nx, ny, nz], nt, g, maps[0][0], maps[1][0], maps[2][0],
+                         stride, float(f0), dt_out)
     if is_tensor(records[0]):
         return outs
     return [x.cpu().numpy() for x in outs]

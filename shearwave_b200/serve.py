@@ -111,7 +111,7 @@ class GpuEngine:
         self.native.call("sw_set_device", self.dev.index)
 
     def admit(self, p):
-        from .solver import _Solve, _Workspace, _project_raw, dtype_code
+        from .solver import _project_raw, _Solve
 
         with self.torch.cuda.stream(self.stream):
             opts = dict(p.get("opts") or {})
@@ -122,13 +122,10 @@ class GpuEngine:
             if sv.needs_per_step_host(None):
                 raise ValueError("the server runs batchable requests only (no 4-D forces, "
                                  "reproject_every, verbose, traces or direct kernels)")
-            nx, ny, nz = sv.shape
-            ws = _Workspace(nx, ny, nz, sv.dev)
             for k, comps in sv.separable_inputs():
-                st = _project_raw(ws, dtype_code(sv.dt), comps, (ny * nz, nz, 1), sv.shape,
-                                  *sv.spacing, sv.tol, sv.max_iters, sv.method)
+                fs, st = _project_raw(comps, sv.spacing, sv.tol, sv.max_iters, sv.method)
                 sv.cg_log.append(st)
-                sv.store_pattern(k, ws.out)
+                sv.store_pattern(k, fs)
             sv.build_terms()
             sv.mark_steps_begin()
             return sv
@@ -138,23 +135,14 @@ class GpuEngine:
         return handle.n_steps
 
     def advance(self, handles, begins, clock, nsteps):
-        torch, native = self.torch, self.native
-        lib = native.load()
-        import ctypes as C
+        from .solver import _batch_steps
 
-        with torch.cuda.stream(self.stream):
+        with self.torch.cuda.stream(self.stream):
             groups = {}
             for h, b in zip(handles, begins):
                 groups.setdefault(h.prec, []).append((h, b))
             for items in groups.values():
-                n = len(items)
-                descs = (native.FdtdDesc * n)(*[h.run.desc for h, _ in items])
-                beg = (C.c_int32 * n)(*[b for _, b in items])
-                tb = int(lib.sw_fdtd_batch_table_bytes(n))
-                table = torch.empty(tb + 64, dtype=torch.uint8, device=self.dev)
-                base = (table.data_ptr() + 63) // 64 * 64
-                native.call("sw_fdtd_batch_steps", descs, beg, n, int(clock), int(nsteps), base,
-                            tb, self.stream.cuda_stream)
+                _batch_steps([h.run for h, _ in items], [b for _, b in items], clock, nsteps)
 
     def finish(self, handle):
         with self.torch.cuda.stream(self.stream):
@@ -355,7 +343,12 @@ class ShearServer:
                 r.token = self.engine.finish_begin(r.handle)
                 self._finishing.append(r)
             else:
-                self._resolve(r, self.engine.finish(r.handle))
+                try:
+                    result = self.engine.finish(r.handle)
+                except RuntimeError as e:  # this request's solve was abandoned on the device
+                    self._fail(r, e)
+                    continue
+                self._resolve(r, result)
         self._active = keep
 
     def _collect(self, block: bool):
@@ -364,10 +357,25 @@ class ShearServer:
         left = []
         for r in self._finishing:
             if block or self.engine.finish_ready(r.token):
-                self._resolve(r, self.engine.finish_end(r.handle, r.token))
+                try:
+                    result = self.engine.finish_end(r.handle, r.token)
+                except RuntimeError as e:  # this request's solve was abandoned on the device
+                    self._fail(r, e)
+                    continue
+                self._resolve(r, result)
             else:
                 left.append(r)
         self._finishing = left
+
+    def _fail(self, r, exc):
+        """Fail one request whose device work reported an error (the other
+        requests of the mix keep running): its memory returns to the budget."""
+        self.failed += 1
+        self.engine.release(r.handle)
+        r.handle = None
+        r.token = None
+        self._used -= r.footprint
+        r.future.set_exception(exc)
 
     def _resolve(self, r, result):
         r.t_done = time.perf_counter()

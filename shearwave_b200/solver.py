@@ -29,7 +29,7 @@ import warnings
 import numpy as np
 import torch
 
-from . import _native
+from . import _native, ops
 from ._device import (
     dtype_code,
     is_tensor,
@@ -93,12 +93,8 @@ def _op_dtype(a) -> torch.dtype:
 def laplacian_center(field, dX, dY, dZ):
     """Compact 7-point Laplacian at cell centres, zero on the shell (solver.py:686-695)."""
     dev = require_cuda()
-    dt = _op_dtype(field)
-    f = to_device(field, dt, dev)
-    nx, ny, nz = _shape(f)
-    out = torch.empty_like(f)
-    _native.call("sw_laplacian", dtype_code(dt), ptr(f), ptr(out), nx, ny, nz, dX, dY, dZ,
-                 stream_handle())
+    f = to_device(field, _op_dtype(field), dev)
+    out = ops.laplacian(f, [dX, dY, dZ])
     return out if is_tensor(field) else out.cpu().numpy()
 
 
@@ -107,41 +103,21 @@ def divergence_center(fx, fy, fz, dX, dY, dZ):
     dev = require_cuda()
     dt = torch.promote_types(torch.promote_types(_op_dtype(fx), _op_dtype(fy)), _op_dtype(fz))
     a, b, c = (to_device(v, dt, dev) for v in (fx, fy, fz))
-    nx, ny, nz = _shape(a)
-    out = torch.empty_like(a)
-    _native.call("sw_divergence", dtype_code(dt), ptr(a), ptr(b), ptr(c), ptr(out), nx, ny, nz,
-                 dX, dY, dZ, stream_handle())
+    out = ops.divergence(a, b, c, [dX, dY, dZ])
     return out if is_tensor(fx) else out.cpu().numpy()
 
 
 def gradient_center(phi, dX, dY, dZ):
     """2h central gradient at cell centres, zero on the shell (solver.py:720-729)."""
     dev = require_cuda()
-    dt = _op_dtype(phi)
-    p = to_device(phi, dt, dev)
-    nx, ny, nz = _shape(p)
-    g = [torch.empty_like(p) for _ in range(3)]
-    _native.call("sw_gradient", dtype_code(dt), ptr(p), ptr(g[0]), ptr(g[1]), ptr(g[2]), nx, ny,
-                 nz, dX, dY, dZ, stream_handle())
+    p = to_device(phi, _op_dtype(phi), dev)
+    g = ops.gradient(p, [dX, dY, dZ])
     return tuple(g) if is_tensor(phi) else tuple(t.cpu().numpy() for t in g)
 
 
 # ---------------------------------------------------------------------------
 # Projection (solver.py:644-683, 1010-1050)
 # ---------------------------------------------------------------------------
-class _Workspace:
-    """Device scratch of one grid for the projection (owned by torch)."""
-
-    def __init__(self, nx, ny, nz, dev):
-        lib = _native.load()
-        self.bytes = max(int(lib.sw_project_workspace_bytes(nx, ny, nz)),
-                         int(lib.sw_project_spectral_workspace_bytes(nx, ny, nz)))
-        self.pz = int(lib.sw_pitch(nz))
-        self.ncell = nx * ny * self.pz
-        self.ws = torch.empty(self.bytes, dtype=torch.uint8, device=dev)
-        self.out = torch.empty((3, self.ncell), dtype=torch.float64, device=dev)
-
-
 _METHODS = ("cg", "spectral")
 
 
@@ -163,31 +139,29 @@ def _projection_method(choice: str, prec: int, tol: float) -> str:
     return choice
 
 
-def _project_raw(ws: _Workspace, dtype_c: int, comps, strides, shape, dX, dY, dZ, tol,
-                 max_iters, method: str = "cg") -> dict:
-    """Project device components (CG or the direct spectral solve) into ws.out."""
-    nx, ny, nz = shape
-    st = _native.CGStats()
-    fs = [ptr(c) if c is not None else None for c in comps]
-    if method == "spectral":
-        _native.call("sw_project_spectral", dtype_c, *fs, *strides, nx, ny, nz, dX, dY, dZ,
-                     ptr(ws.out), ptr(ws.ws), ws.bytes, C.byref(st), stream_handle())
-    else:
-        _native.call("sw_project", dtype_c, *fs, *strides, nx, ny, nz, dX, dY, dZ, float(tol),
-                     int(max_iters), ptr(ws.out), ptr(ws.ws), ws.bytes, C.byref(st),
-                     stream_handle())
-    d = st.as_dict()
-    d["method"] = method
-    return d
+_CG_REASONS = _native.CG_REASONS
 
 
-def _unpad(ws: _Workspace, shape, dt: torch.dtype, dev) -> list[torch.Tensor]:
+def _stats_dict(st: torch.Tensor, method: str = "cg") -> dict:
+    """A host stats row [iters, reason, rel, max_div] as the info dict."""
+    v = st.tolist()
+    return {"iters": int(v[0]), "reason": _CG_REASONS.get(int(v[1]), str(int(v[1]))),
+            "rel": float(v[2]), "max_div": float(v[3]), "method": method}
+
+
+def _project_raw(comps, spacing, tol, max_iters, method: str = "cg"):
+    """Project device components (CG or the direct spectral solve): returns
+    the padded FP64 result (3, ncell) and the info dict."""
+    out, st = ops.project(*comps, list(spacing), float(tol), int(max_iters), method)
+    return out, _stats_dict(st, method)
+
+
+def _unpad(fs: torch.Tensor, shape, dt: torch.dtype, dev) -> list[torch.Tensor]:
     nx, ny, nz = shape
     outs = []
     for c in range(3):
         o = torch.empty((nx, ny, nz), dtype=dt, device=dev)
-        _native.call("sw_convert", 1, ws.out[c].data_ptr(), nx, ny, nz, dtype_code(dt), ptr(o), 0,
-                     ny * nz, nz, 1, 1.0, _native.SW_F32, None, 0, 0, 0, stream_handle())
+        ops.convert_(o, fs[c], 1, [nx, ny, nz], [0, ny * nz, nz, 1], 1.0, None, [0, 0, 0])
         outs.append(o)
     return outs
 
@@ -210,13 +184,10 @@ def project_vector_field(fx, fy, fz, dX, dY, dZ, tol, max_iters, *, info=None, m
     shape = _shape(comps[0])
     if any(_shape(c) != shape for c in comps) or len(shape) != 3:
         raise ValueError("fx, fy, fz must be 3-D arrays of the same shape")
-    nx, ny, nz = shape
-    ws = _Workspace(nx, ny, nz, dev)
-    st = _project_raw(ws, dtype_code(dt), comps, (ny * nz, nz, 1), shape, dX, dY, dZ, tol,
-                      max_iters, method)
+    fs, st = _project_raw(comps, (dX, dY, dZ), tol, max_iters, method)
     if info is not None:
         info.update(st)
-    outs = _unpad(ws, shape, dt, dev)
+    outs = _unpad(fs, shape, dt, dev)
     if is_tensor(fx):
         return tuple(outs)
     return tuple(o.cpu().numpy() for o in outs)
@@ -238,15 +209,11 @@ def elastic_solve_static(bz, dX, dY, dZ, mu, tol=1e-6, max_iters=1500, *, verbos
         raise ValueError("bz must be a 3-D array")
     nx, ny, nz = shape
     m, ms = _material(mu, shape, dt, dev)
-    ws = _Workspace(nx, ny, nz, dev)
-    st = _native.CGStats()
-    _native.call("sw_static_solve", dtype_code(dt), ptr(b), ptr(m), ms, ny * nz, nz, 1, nx, ny,
-                 nz, dX, dY, dZ, float(tol), int(max_iters), ws.out.data_ptr(), ptr(ws.ws),
-                 ws.bytes, C.byref(st), stream_handle())
+    out, st = ops.static_solve(b, m, float(ms), [dX, dY, dZ], float(tol), int(max_iters))
     u = torch.empty(shape, dtype=dt, device=dev)
-    _native.call("sw_convert", 1, ws.out.data_ptr(), nx, ny, nz, dtype_code(dt), ptr(u), 0,
-                 ny * nz, nz, 1, 1.0, _native.SW_F32, None, 0, 0, 0, stream_handle())
-    d = st.as_dict()
+    ops.convert_(u, out[0], 1, [nx, ny, nz], [0, ny * nz, nz, 1], 1.0, None, [0, 0, 0])
+    d = _stats_dict(st)
+    d.pop("method")
     if verbose:
         print(f"CG (GPU): it={d['iters']}/{max_iters}, rel={d['rel']:.3e}, {d['reason']}")
     if info is not None:
@@ -385,49 +352,69 @@ def _gather_forces(bx, by, bz, opts, shape, n_steps, dt, dev, np_dt) -> _Forces:
 
 
 class _Run:
-    """Device state of one shear_fdtd solve."""
+    """Device state of one shear_fdtd solve: the tensors the time-loop ops
+    read and write (``bundle()``) and its scalar settings."""
 
     def __init__(self, shape, spacing, dT, n_steps, prec, kahan, dev):
-        lib = _native.load()
         self.dev = dev
         self.shape = shape
         self.nx, self.ny, self.nz = shape
-        self.pz = int(lib.sw_pitch(self.nz))
+        self.pz = ops.pitch(self.nz)
         self.ncell = self.nx * self.ny * self.pz
         self.prec = prec
         self.dt = _field_dtype(prec)
-        d = _native.FdtdDesc()
-        d.precision = prec
-        d.nx, d.ny, d.nz, d.pz = self.nx, self.ny, self.nz, self.pz
-        d.n_steps = n_steps
-        d.dX, d.dY, d.dZ = spacing
-        d.dT = dT
-        d.kahan = 1 if kahan else 0
-        self.desc = d
+        self.spacing = tuple(float(h) for h in spacing)
+        self.dT = float(dT)
+        self.n_steps = int(n_steps)
+        self.kahan = 1 if kahan else 0
+        self.vel_damp = 0.0
+        self.kernel = 0          # 0 TMA-staged step kernels, 1 direct loads
+        self.xchunk = 0
+        self.steps_per_pass = 0
+        self.has_eta = 0
+        self.snap_stride = 0
+        self.stall_test = 0      # testing switch of the step kernels (sw_fdtd_desc.stall_test)
         nbuf, ncomp = (3, 3) if prec == _native.SW_PLAIN_F64 else (3, 9)
         self.state = torch.empty((nbuf, ncomp, self.ncell), dtype=self.dt, device=dev)
-        for i in range(nbuf):
-            d.state[i] = self.state[i].data_ptr()
         # material coefficients: one allocation, component 0 the mu term,
         # component 1 the eta term (used only with viscosity)
         self.coef = torch.zeros((2, self.ncell), dtype=self.dt, device=dev)
-        d.coef_m = self.coef[0].data_ptr()
         self.inv_rho = None
         if prec == _native.SW_PLAIN_F64:
             self.inv_rho = torch.zeros(self.ncell, dtype=self.dt, device=dev)
-            d.inv_rho = self.inv_rho.data_ptr()
         self.flags = torch.zeros(1, dtype=torch.int32, device=dev)
-        d.flags = self.flags.data_ptr()
         # device step counter: lets the library replay the loop as CUDA graphs
         self.clock = torch.zeros(1, dtype=torch.int32, device=dev)
-        d.clock = self.clock.data_ptr()
         # launch-wide tile queue of this solve's step launches
         self.queue = torch.zeros(2, dtype=torch.int32, device=dev)
-        d.queue = self.queue.data_ptr()
-        self.keep = []  # tensors referenced by the descriptor
+        # force patterns and term table (set by set_patterns)
+        self.patterns = torch.zeros((1, 3, 0), dtype=self.dt, device=dev)
+        self.term_off = torch.zeros(self.n_steps + 1, dtype=torch.int32, device=dev)
+        self.term_pat = torch.zeros(1, dtype=torch.int32, device=dev)
+        self.term_scale = torch.zeros(1, dtype=torch.float64, device=dev)
+        self.snaps = None
+        self.trace_cells = None
+        self.traces = None
+        self.keep = []  # inputs the device work still reads
 
-    def p(self):
-        return C.byref(self.desc)
+    def fparams(self) -> list[float]:
+        return [*self.spacing, self.dT, float(self.vel_damp)]
+
+    def iparams(self) -> list[int]:
+        return [self.prec, self.nx, self.ny, self.nz, self.n_steps, self.kahan,
+                self.snap_stride, self.xchunk, self.steps_per_pass, self.kernel, self.has_eta,
+                self.stall_test]
+
+    def bundle(self) -> tuple:
+        """Arguments shared by the fdtd ops (shearwave_b200.ops)."""
+        return (self.state, self.coef, self.inv_rho, self.patterns, self.term_off,
+                self.term_pat, self.term_scale, self.snaps, self.trace_cells, self.traces,
+                self.flags, self.clock, self.queue, self.fparams(), self.iparams())
+
+    @property
+    def desc(self) -> _native.FdtdDesc:
+        """The C-ABI descriptor of this solve (built from the tensors)."""
+        return ops.make_desc(*self.bundle())
 
     def materials(self, rho, mu, eta, in_dt):
         dev = self.dev
@@ -437,45 +424,33 @@ class _Run:
         if eta is not None:
             eta_mode = 1
             e, es = _material(eta, self.shape, in_dt, dev)
-            self.desc.coef_e = self.coef[1].data_ptr()
-        _native.call("sw_fdtd_materials", self.p(), dtype_code(in_dt), ptr(r), rs, ptr(m), ms,
-                     eta_mode, ptr(e), es, stream_handle())
+            self.has_eta = 1
+        ops.fdtd_materials_(*self.bundle(), r, float(rs), m, float(ms), eta_mode, e, float(es))
         self.rho_dev, self.rho_s = r, rs
         self.keep += [r, m, e]
 
     def set_patterns(self, pats: torch.Tensor, term_off, term_pat, term_scale):
         self.patterns = pats
         self.term_off = torch.as_tensor(np.asarray(term_off, np.int32), device=self.dev)
-        self.term_pat = torch.as_tensor(np.asarray(term_pat, np.int32), device=self.dev)
-        self.term_scale = torch.as_tensor(np.asarray(term_scale, np.float64), device=self.dev)
-        d = self.desc
-        d.patterns = pats.data_ptr()
-        d.n_patterns = int(pats.shape[0])
-        d.term_off = self.term_off.data_ptr()
-        d.term_pat = self.term_pat.data_ptr() if len(term_pat) else self.term_off.data_ptr()
-        d.term_scale = self.term_scale.data_ptr() if len(term_scale) else None
-        if not len(term_scale):
-            self.term_scale = torch.zeros(1, dtype=torch.float64, device=self.dev)
-            d.term_scale = self.term_scale.data_ptr()
+        if len(term_pat):
+            self.term_pat = torch.as_tensor(np.asarray(term_pat, np.int32), device=self.dev)
+            self.term_scale = torch.as_tensor(np.asarray(term_scale, np.float64),
+                                              device=self.dev)
 
     def pattern_from_tensor(self, fs: torch.Tensor, dst: torch.Tensor, spacing_dt2: float):
         """Store a projected force (3 padded FP64 components) as a pattern of this form."""
+        strides = [self.ncell, self.ny * self.pz, self.pz, 1]
         if self.prec == _native.SW_PLAIN_F64:
-            _native.call("sw_convert", 3, fs.data_ptr(), self.nx, self.ny, self.nz,
-                         _native.SW_F64, dst.data_ptr(), self.ncell, self.ny * self.pz, self.pz,
-                         1, 1.0, _native.SW_F64, None, 0, 0, 0, stream_handle())
+            ops.convert_(dst, fs, 3, list(self.shape), strides, 1.0, None, [0, 0, 0])
         else:
             # dT^2 f_S / rho in FP32
             r = self.rho_dev
             if r is None:
-                scale, rptr, rs = spacing_dt2 / self.rho_s, None, (0, 0, 0)
-                rdt = _native.SW_F32
+                ops.convert_(dst, fs, 3, list(self.shape), strides, spacing_dt2 / self.rho_s,
+                             None, [0, 0, 0])
             else:
-                scale, rptr, rs = spacing_dt2, ptr(r), (self.ny * self.nz, self.nz, 1)
-                rdt = dtype_code(r.dtype)
-            _native.call("sw_convert", 3, fs.data_ptr(), self.nx, self.ny, self.nz,
-                         _native.SW_F32, dst.data_ptr(), self.ncell, self.ny * self.pz, self.pz,
-                         1, scale, rdt, rptr, *rs, stream_handle())
+                ops.convert_(dst, fs, 3, list(self.shape), strides, spacing_dt2, r,
+                             [self.ny * self.nz, self.nz, 1])
 
 
 def validate_inputs(bx, by, bz, rho, mu, eta, opts, shape, n_steps) -> None:
@@ -576,22 +551,22 @@ class _Solve:
             self.tev[0].record()
         run = self.run = _Run(shape, (dX, dY, dZ), dT, n_steps, self.prec,
                               opts.get("kahan", False), dev)
-        run.desc.vel_damp = float(opts.get("vel_damp", 0.0))
-        run.desc.kernel = 0 if kern == "tma" else 1
-        run.desc.xchunk = int(opts.get("xchunk", 0) or 0)
+        run.vel_damp = float(opts.get("vel_damp", 0.0))
+        run.kernel = 0 if kern == "tma" else 1
+        run.xchunk = int(opts.get("xchunk", 0) or 0)
         spp = int(opts.get("steps_per_pass", 0) or 0)
         if spp not in (0, 1, 2):
             raise ValueError("steps_per_pass must be 1 or 2 (0 = automatic)")
-        run.desc.steps_per_pass = spp
+        run.steps_per_pass = spp
         if not opts.get("cuda_graph", True):
-            run.desc.clock = None
+            run.clock = None
         run.materials(rho, mu, eta, dt)
         iu = iv = None
         if opts.get("initial_u") is not None:
             iu = to_device(opts["initial_u"], dt, dev)
         if opts.get("initial_v") is not None:
             iv = to_device(opts["initial_v"], dt, dev)
-        _native.call("sw_fdtd_init", run.p(), ptr(iu), ptr(iv), stream_handle())
+        ops.fdtd_init_(*run.bundle(), iu, iv)
 
         self.n_sep = len(self.forces.separable)
         n_pat = self.n_sep + (1 if self.forces.stream4d is not None else 0)
@@ -602,23 +577,21 @@ class _Solve:
         if snapshot_stride:
             self.snaps = torch.zeros((n_steps // snapshot_stride, nx, ny, nz, 3), dtype=dt,
                                      device=dev)
-            run.desc.snap_stride = snapshot_stride
-            run.desc.snaps = self.snaps.data_ptr()
+            run.snap_stride = snapshot_stride
+            run.snaps = self.snaps
         self.traces = None
         if trace_cells is not None and return_traces:
             tc = torch.as_tensor(trace_cells.reshape(-1), dtype=torch.int32, device=dev)
             self.traces = torch.zeros((trace_cells.shape[0], n_steps), dtype=dt, device=dev)
-            run.keep.append(tc)
-            run.desc.n_traces = int(trace_cells.shape[0])
-            run.desc.trace_cells = tc.data_ptr()
-            run.desc.traces = self.traces.data_ptr()
+            run.trace_cells = tc
+            run.traces = self.traces
 
     # ---- phases ---------------------------------------------------------
     def needs_per_step_host(self, callback) -> bool:
         """Whether the time loop must return to the host between steps."""
         return (callback is not None or self.forces.stream4d is not None
                 or bool(self.reproject_every) or bool(self.verbose)
-                or self.run.desc.n_traces > 0 or self.run.desc.kernel != 0)
+                or self.run.traces is not None or self.run.kernel != 0)
 
     def separable_inputs(self):
         """(pattern index, device components) of every separable force term."""
@@ -661,9 +634,7 @@ class _Solve:
         nx, ny, nz = self.shape
         if self.tev is not None:
             self.tev[2].record()
-        u = torch.empty((nx, ny, nz, 3), dtype=dt, device=dev)
-        v = torch.empty((nx, ny, nz, 3), dtype=dt, device=dev)
-        _native.call("sw_fdtd_finish", run.p(), self.n_steps, ptr(u), ptr(v), stream_handle())
+        u, v = ops.fdtd_finish(*run.bundle(), self.n_steps, True)
         outs = [u, v]
         if self.snaps is not None:
             outs.append(self.snaps)
@@ -696,7 +667,7 @@ class _Solve:
     def finish_collect(self, handle):
         """Wait for a finish_enqueue handle and return the solve's result."""
         handle["event"].synchronize()
-        nonfinite = bool(int(handle["flag"][0]))
+        nonfinite = bool(int(handle["flag"][0]) & _native.FLAG_NONFINITE)
         if self.info is not None:
             tev = self.tev
             tev[3].synchronize()
@@ -708,6 +679,15 @@ class _Solve:
                 t_finish_ms=tev[2].elapsed_time(tev[3]),
                 n_push_steps=int(sum(1 for i in range(self.n_steps)
                                      if self.term_off[i + 1] > self.term_off[i])))
+        flags = int(handle["flag"][0])
+        if flags & _native.FLAG_TIMEOUT:
+            raise RuntimeError(
+                "shear_fdtd: a step kernel's bounded device wait ran out and its tiles of this "
+                "solve were abandoned (SW_ETIMEOUT); the result is incomplete")
+        if flags & _native.FLAG_REFUSED:
+            raise RuntimeError(
+                "shear_fdtd: a step launch refused to issue a TMA copy to a misaligned "
+                "shared-memory destination (SW_ETIMEOUT); the result is incomplete")
         if nonfinite:
             warnings.warn("shear_fdtd: non-finite displacement encountered (unstable dT?)",
                           RuntimeWarning, stacklevel=3)
@@ -715,7 +695,7 @@ class _Solve:
             return tuple(handle["outs"])
         return tuple(h.numpy() for h in handle["outs"])
 
-    def run_loop(self, callback, ws: "_Workspace"):
+    def run_loop(self, callback):
         """The time loop of solver.py:194-239 for this solve alone."""
         run, dt, dev = self.run, self.dt, self.dev
         nx, ny, nz = self.shape
@@ -728,10 +708,8 @@ class _Solve:
             events.update(range(self.reproject_every, n_steps + 1, self.reproject_every))
         if self.verbose:
             events.update(range(self.progress_every, n_steps + 1, self.progress_every))
-        u_cb = torch.empty((nx, ny, nz, 3), dtype=dt, device=dev) if callback else None
         self.mark_steps_begin()
         it = 0
-        strm = stream_handle()
         while it < n_steps:
             if per_step:
                 end = it + 1
@@ -742,22 +720,20 @@ class _Solve:
                 # per-step projection of b[..., it] (solver.py:198-199)
                 comps = [None if b is None else (b[..., it] if b.dim() == 4 else b).contiguous()
                          for b in f.stream4d]
-                st = _project_raw(ws, dtype_code(dt), comps, (ny * nz, nz, 1), self.shape, dX,
-                                  dY, dZ, self.tol, self.max_iters, self.method)
+                fs, st = _project_raw(comps, (dX, dY, dZ), self.tol, self.max_iters,
+                                      self.method)
                 self.cg_log.append(st)
-                self.store_pattern(self.n_sep, ws.out)
-            _native.call("sw_fdtd_steps", run.p(), it, end - it, strm)
+                self.store_pattern(self.n_sep, fs)
+            ops.fdtd_steps_(*run.bundle(), it, end - it)
             if callback is not None:
-                _native.call("sw_fdtd_finish", run.p(), end, ptr(u_cb), None, strm)
+                u_cb, _ = ops.fdtd_finish(*run.bundle(), end, False)
                 callback(end - 1, u_cb.cpu().numpy())
             if self.verbose and end % self.progress_every == 0:
                 print(f"FDTD it={end}/{n_steps}")
             if self.reproject_every and end % self.reproject_every == 0:
-                stats = (_native.CGStats * 2)()
-                _native.call("sw_fdtd_reproject", run.p(), end, float(self.tol),
-                             int(self.max_iters), ws.out.data_ptr(), ptr(ws.ws), ws.bytes, stats,
-                             strm)
-                self.cg_log += [stats[0].as_dict(), stats[1].as_dict()]
+                st = ops.fdtd_reproject_(*run.bundle(), end, float(self.tol),
+                                         int(self.max_iters))
+                self.cg_log += [_stats_dict(st[0]), _stats_dict(st[1])]
             it = end
 
 
@@ -819,22 +795,18 @@ def shear_fdtd(
 
 def _solve_alone(sv: _Solve, callback, return_device):
     """Projection, time loop and outputs of one solve."""
-    nx, ny, nz = sv.shape
-    dX, dY, dZ = sv.spacing
-    ws = _Workspace(nx, ny, nz, sv.dev)
     if sv.verbose and sv.n_sep:
         print("Pre-computing Helmholtz projection (separable force)...")
     for k, comps in sv.separable_inputs():
-        st = _project_raw(ws, dtype_code(sv.dt), comps, (ny * nz, nz, 1), sv.shape, dX, dY, dZ,
-                          sv.tol, sv.max_iters, sv.method)
+        fs, st = _project_raw(comps, sv.spacing, sv.tol, sv.max_iters, sv.method)
         sv.cg_log.append(st)
-        sv.store_pattern(k, ws.out)
+        sv.store_pattern(k, fs)
     sv.build_terms()
-    sv.run_loop(callback, ws)
+    sv.run_loop(callback)
     return sv.finish(return_device)
 
 
-def shear_fdtd_batch(problems, *, precision=None, return_device=False):
+def shear_fdtd_batch(problems, *, precision=None, return_device=False, errors="raise"):
     """Run many independent ``shear_fdtd`` problems together on one GPU.
 
     ``problems`` is a sequence of dicts of ``shear_fdtd`` keyword arguments
@@ -850,7 +822,15 @@ def shear_fdtd_batch(problems, *, precision=None, return_device=False):
     forces, ``reproject_every``, ``verbose``, traces or the direct kernels)
     are run one after another through :func:`shear_fdtd` on the same GPU.
     Returns a list of ``shear_fdtd`` results in input order.
+
+    A solve whose device work was abandoned (a step kernel's bounded wait
+    ran out) fails alone: the other solves' results are unaffected.  With
+    ``errors="raise"`` (default) the first such error is raised once every
+    solve has been collected; with ``errors="return"`` the failed solve's
+    slot holds the exception instead of a result.
     """
+    if errors not in ("raise", "return"):
+        raise ValueError("errors must be 'raise' or 'return'")
     solves, results = [], [None] * len(problems)
     for i, p in enumerate(problems):
         opts = dict(p.get("opts") or {})
@@ -867,10 +847,17 @@ def shear_fdtd_batch(problems, *, precision=None, return_device=False):
     precs = {sv.prec for _, sv in solves}
     groups = [[(i, sv) for i, sv in solves if sv.prec == pr] for pr in sorted(precs)]
     copy_stream = None if return_device else torch.cuda.Stream(device=solves[0][1].dev)
+    first_error = None
     for group in groups:
         handles = _run_batch_group([sv for _, sv in group], return_device, copy_stream)
         for (i, sv), h in zip(group, handles):
-            results[i] = sv.finish_collect(h)
+            try:
+                results[i] = sv.finish_collect(h)
+            except RuntimeError as e:
+                results[i] = e
+                first_error = first_error or e
+    if first_error is not None and errors == "raise":
+        raise first_error
     return results
 
 
@@ -882,69 +869,57 @@ def _run_batch_group(solves, return_device, copy_stream):
     (``copy_stream``) are enqueued right there, so they run while the
     longer solves are still stepping.  Returns one finish handle per solve.
     """
-    lib = _native.load()
-    dev = solves[0].dev
-    strm = stream_handle()
     # ---- batched projection of every separable pattern ----
-    jobs, owners, bufs = [], [], []
+    jobs, owners = [], []
     for sv in solves:
-        nx, ny, nz = sv.shape
         if sv.method == "spectral":  # direct solves: one after another, each ~1 ms
-            ws = _Workspace(nx, ny, nz, dev)
             for k, comps in sv.separable_inputs():
-                st = _project_raw(ws, dtype_code(sv.dt), comps, (ny * nz, nz, 1), sv.shape,
-                                  *sv.spacing, sv.tol, sv.max_iters, "spectral")
+                fs, st = _project_raw(comps, sv.spacing, sv.tol, sv.max_iters, "spectral")
                 sv.cg_log.append(st)
-                sv.store_pattern(k, ws.out)
+                sv.store_pattern(k, fs)
             continue
         for k, comps in sv.separable_inputs():
-            ws = _Workspace(nx, ny, nz, dev)
-            j = _native.ProjectJob()
-            j.in_dtype = dtype_code(sv.dt)
-            j.fx, j.fy, j.fz = (ptr(c) if c is not None else None for c in comps)
-            j.sx, j.sy, j.sz = ny * nz, nz, 1
-            j.nx, j.ny, j.nz = nx, ny, nz
-            j.dX, j.dY, j.dZ = sv.spacing
-            j.tol = float(sv.tol)
-            j.max_iters = int(sv.max_iters)
-            j.out = ws.out.data_ptr()
-            j.workspace = ws.ws.data_ptr()
-            j.workspace_bytes = ws.bytes
-            jobs.append(j)
+            jobs.append((comps, sv))
             owners.append((sv, k))
-            bufs.append(ws)
     if jobs:
-        dtypes = {j.in_dtype for j in jobs}
-        for dtc in dtypes:
-            idx = [q for q, j in enumerate(jobs) if j.in_dtype == dtc]
-            arr = (_native.ProjectJob * len(idx))(*[jobs[q] for q in idx])
-            stats = (_native.CGStats * len(idx))()
-            tb = int(lib.sw_project_batch_table_bytes(len(idx)))
-            table = torch.empty(tb, dtype=torch.uint8, device=dev)
-            _native.call("sw_project_batch", arr, len(idx), table.data_ptr(), tb, stats, strm)
-            for q, st in zip(idx, stats):
+        dtypes = sorted({sv.dt for _, sv in jobs}, key=str)
+        for dt in dtypes:
+            idx = [q for q, (_, sv) in enumerate(jobs) if sv.dt == dt]
+            comps = [jobs[q][0] for q in idx]
+            outs, stats = ops.project_batch(
+                [c[0] for c in comps], [c[1] for c in comps], [c[2] for c in comps],
+                [h for q in idx for h in jobs[q][1].spacing],
+                [float(jobs[q][1].tol) for q in idx], [int(jobs[q][1].max_iters) for q in idx])
+            for q, fs, st in zip(idx, outs, stats):
                 sv, k = owners[q]
-                sv.cg_log.append(st.as_dict())
-                sv.store_pattern(k, bufs[q].out)
+                sv.cg_log.append(_stats_dict(st))
+                sv.store_pattern(k, fs)
     for sv in solves:
         sv.build_terms()
         sv.mark_steps_begin()
     # ---- batched time loop ----
     n = len(solves)
-    descs = (_native.FdtdDesc * n)(*[sv.run.desc for sv in solves])
-    tb = int(lib.sw_fdtd_batch_table_bytes(n))
-    table = torch.empty(tb + 64, dtype=torch.uint8, device=dev)
-    base = (table.data_ptr() + 63) // 64 * 64
     handles = [None] * n
     it = 0
     for end in sorted({sv.n_steps for sv in solves}):
         if end > it:
-            _native.call("sw_fdtd_batch_steps", descs, None, n, it, end - it, base, tb, strm)
+            _batch_steps([sv.run for sv in solves], [], it, end - it)
             it = end
         for k, sv in enumerate(solves):
             if sv.n_steps == end:
                 handles[k] = sv.finish_enqueue(return_device, copy_stream)
     return handles
+
+
+def _batch_steps(runs, begins, it0, nsteps):
+    """One fdtd_batch_steps_ call over the solves' device state (begins: an
+    empty list starts every solve at step 0)."""
+    b = [r.bundle() for r in runs]
+    ops.fdtd_batch_steps_([x[0] for x in b], [x[1] for x in b], [x[3] for x in b],
+                          [x[4] for x in b], [x[5] for x in b], [x[6] for x in b],
+                          [x[7] for x in b], [x[10] for x in b], [x[12] for x in b],
+                          [f for x in b for f in x[13]], [i for x in b for i in x[14]],
+                          list(begins), int(it0), int(nsteps))
 
 
 def shear_fdtd_jax(bx, by, bz, rho, mu, dX, dY, dZ, dT, n_steps, opts=None, callback=None,

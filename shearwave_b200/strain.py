@@ -13,8 +13,8 @@ from __future__ import annotations
 import numpy as np
 import torch
 
-from . import _native
-from ._device import dtype_code, is_tensor, ptr, require_cuda, stream_handle, to_device
+from . import ops
+from ._device import is_tensor, require_cuda, to_device
 
 __all__ = ["compute_strain_fields", "compute_strain_invariants", "compute_strain_tensor"]
 
@@ -44,10 +44,7 @@ def compute_strain_tensor(ux, uy, uz, dX, dY, dZ):
     dev = require_cuda()
     dt = _dtype(ux, uy, uz)
     a, b, c = (to_device(v, dt, dev) for v in (ux, uy, uz))
-    nx, ny, nz = a.shape
-    eps = torch.empty((nx, ny, nz, 6), dtype=dt, device=dev)
-    _native.call("sw_strain", dtype_code(dt), ptr(a), ptr(b), ptr(c), ny * nz, nz, 1, nx, ny, nz,
-                 dX, dY, dZ, ptr(eps), None, None, None, None, stream_handle())
+    eps = ops.strain(a, b, c, [dX, dY, dZ], True, False)[0]
     return eps if is_tensor(ux) else eps.cpu().numpy()
 
 
@@ -64,16 +61,9 @@ def compute_strain_invariants(epsilon):
         )
     dev = require_cuda()
     dt = _dtype(epsilon)
-    e = to_device(epsilon, dt, dev)
-    lead = tuple(e.shape[:-1])
-    n = int(np.prod(lead)) if lead else 1
-    outs = {k: torch.empty(lead, dtype=dt, device=dev)
-            for k in ("volumetric", "deviatoric", "max_shear")}
-    outs["von_mises"] = torch.empty(lead, dtype=torch.float64, device=dev)
-    _native.call("sw_strain_invariants", dtype_code(dt), ptr(e), n, ptr(outs["volumetric"]),
-                 ptr(outs["deviatoric"]), ptr(outs["max_shear"]), ptr(outs["von_mises"]),
-                 stream_handle())
+    e = to_device(epsilon, dt, dev).contiguous()
     order = ("volumetric", "deviatoric", "max_shear", "von_mises")
+    outs = dict(zip(order, ops.strain_invariants(e)))
     if is_tensor(epsilon):
         return {k: outs[k] for k in order}
     return {k: outs[k].cpu().numpy() for k in order}
@@ -94,19 +84,11 @@ def compute_strain_fields(u, dX, dY, dZ, *, return_tensor=True, return_device=Fa
             raise ValueError(f"Grid spacing {name} must be positive, got {val}")
     dev = require_cuda()
     dt = _dtype(u)
-    t = to_device(u, dt, dev)
-    nx, ny, nz, _ = t.shape
-    eps = torch.empty((nx, ny, nz, 6), dtype=dt, device=dev) if return_tensor else None
-    inv = {k: torch.empty((nx, ny, nz), dtype=dt, device=dev)
-           for k in ("volumetric", "deviatoric", "max_shear")}
-    inv["von_mises"] = torch.empty((nx, ny, nz), dtype=torch.float64, device=dev)
-    base = t.data_ptr()
-    es = t.element_size()
-    # AoS input: component c starts at element c, strides (ny*nz*3, nz*3, 3)
-    _native.call("sw_strain", dtype_code(dt), base, base + es, base + 2 * es, ny * nz * 3, nz * 3,
-                 3, nx, ny, nz, dX, dY, dZ, ptr(eps), ptr(inv["volumetric"]),
-                 ptr(inv["deviatoric"]), ptr(inv["max_shear"]), ptr(inv["von_mises"]),
-                 stream_handle())
+    t = to_device(u, dt, dev).contiguous()
+    # one kernel reads the AoS components in place (strides 3 nz ny, 3 nz, 3)
+    eps, *rest = ops.strain_aos(t, [dX, dY, dZ], bool(return_tensor))
+    eps = eps if return_tensor else None
+    inv = dict(zip(("volumetric", "deviatoric", "max_shear", "von_mises"), rest))
     dev_out = return_device or is_tensor(u)
     conv = (lambda x: x) if dev_out else (lambda x: None if x is None else x.cpu().numpy())
     return conv(eps), {k: conv(v) for k, v in inv.items()}

@@ -11,7 +11,8 @@ library set the cut (enum ``sw_tune_knob``):
   one solve whose tiles would not fill the GPU in whole waves) cut x into
   chunks so that about this many tiles fall to each CTA (more tiles balance
   better, each chunk re-reads two halo planes);
-* ``xchunk`` — planes per x chunk for every launch (0 = automatic);
+* ``xchunk`` — planes per x chunk for every launch (0 = automatic; 32 in
+  batched two-step launches);
 * ``tile_shape`` — the mixed step kernel's (z, y) tile: 0 picks, per grid,
   whichever of 64 x 8 and 32 x 16 covers the plane with fewer cells; 1 and
   2 force one;
@@ -43,7 +44,7 @@ KNOBS = {"ctas_per_sm": 0, "batch_tiles_per_cta": 1, "xchunk": 2, "tile_shape": 
          "steps_per_pass": 4}
 
 __all__ = ["KNOBS", "get_knobs", "set_knobs", "knobs", "workload_key", "autotune",
-           "apply_cached", "default_cache_path"]
+           "apply_cached", "default_cache_path", "fused_batch_candidates"]
 
 
 def get_knobs() -> dict:
@@ -140,6 +141,15 @@ def _candidates(n_problems):
     return fused + [dict(ctas_per_sm=2, xchunk=x, batch_tiles_per_cta=8, tile_shape=t,
                          steps_per_pass=1)
                     for t, x in itertools.product((0, 1, 2), (0, 32, 64))]
+
+
+def fused_batch_candidates(xchunks=(0, 16, 24, 48, 64)):
+    """Two steps per pass with each of ``xchunks`` planes per x chunk (0: the
+    library's 32).  The sweep a long batch should use: the two-step kernel
+    wins once the board sits at its power cap, which a shortened tuning run
+    does not reach, so the one-step shapes are left out of it."""
+    return [dict(ctas_per_sm=2, batch_tiles_per_cta=8, xchunk=x, tile_shape=0,
+                 steps_per_pass=2) for x in xchunks]
 
 
 def autotune(problems, *, precision="mixed", steps=64, repeats=2, candidates=None,

@@ -1,9 +1,9 @@
 """Generate the golden fixtures under tests/golden/ by running the reference itself.
 
-Run in a container that has the pinton-lab/shearwave sources at
-``/root/reference`` (override with ``SHEARWAVE_REF_SRC``):
+Point ``SHEARWAVE_REF_SRC`` at the ``src`` directory of a pinton-lab/shearwave
+checkout (the directory that holds the ``shearwave`` package) and run:
 
-    python tests/golden/make_golden.py [case ...]
+    SHEARWAVE_REF_SRC=<checkout>/src python tests/golden/make_golden.py [case ...]
 
 Each case is run twice through the reference's own NumPy code:
 
@@ -30,7 +30,10 @@ HERE = Path(__file__).resolve().parent
 sys.path.insert(0, str(HERE))
 import cases  # noqa: E402
 
-REF_SRC = os.environ.get("SHEARWAVE_REF_SRC", "/root/reference/src")
+REF_SRC = os.environ.get("SHEARWAVE_REF_SRC")
+if not REF_SRC or not (Path(REF_SRC) / "shearwave" / "solver.py").is_file():
+    sys.exit("make_golden.py: set SHEARWAVE_REF_SRC to the src directory of a "
+             "pinton-lab/shearwave checkout (it must contain shearwave/solver.py)")
 sys.path.insert(0, REF_SRC)
 import shearwave.radiation_force as ref_arf  # noqa: E402
 import shearwave.solver as ref_solver  # noqa: E402

@@ -82,3 +82,26 @@ def test_batch_with_host_stepped_member(cuda):
     ref = _alone(probs[1], "mixed")
     for a, b in zip(got[1], ref):
         assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_long_batch_replays_graphs_bitwise(cuda, precision):
+    """Runs of >= 64 steps with the same solves running replay CUDA graphs of
+    the batched launches (one host call per 32 steps); the results stay bit
+    for bit those of the solves run alone, and the host makes far fewer
+    enqueue calls than kernels run."""
+    import shearwave_b200 as sw
+    import shearwave_b200._native as native
+    from shearwave_b200 import workloads as W
+
+    probs = [W.problem_inclusions(sh, 300, seed=40 + i, tol=1e-9)
+             for i, sh in enumerate([(22, 20, 30), (18, 26, 24), (30, 16, 20)])]
+    k0, h0 = native.launch_count(), native.host_enqueue_count()
+    got = sw.shear_fdtd_batch(probs, precision=precision)
+    kernels, enqueues = native.launch_count() - k0, native.host_enqueue_count() - h0
+    # 288 of the 300 steps run as 9 graph replays: >= 9 x 16 kernels without a host call
+    assert kernels - enqueues >= 140, (kernels, enqueues)
+    for p, res in zip(probs, got):
+        ref = _alone(p, precision)
+        for a, b in zip(res, ref):
+            assert np.array_equal(a, b)

@@ -209,3 +209,38 @@ def test_async_completion_resolves_each_request_once_and_bounds_run_ahead():
     assert sorted(eng.ended) == list(range(9))
     assert eng.max_outstanding <= 3
     assert srv.stats()["completed"] == 9
+
+
+class AbandoningEngine(AsyncFakeEngine):
+    """A device that abandoned one request's tiles: its result raises, as the
+    real engine's finish_collect does for a timed-out solve (SW_ETIMEOUT)."""
+
+    def finish_end(self, h, token):
+        out = super().finish_end(h, token)
+        if h["id"] == 2:
+            raise RuntimeError("shear_fdtd: ... (SW_ETIMEOUT); the result is incomplete")
+        return out
+
+
+class AbandoningSyncEngine(FakeEngine):
+    def finish(self, h):
+        if h["id"] == 2:
+            raise RuntimeError("shear_fdtd: ... (SW_ETIMEOUT); the result is incomplete")
+        return super().finish(h)
+
+
+@pytest.mark.parametrize("engine", [AbandoningEngine, AbandoningSyncEngine])
+def test_device_failure_fails_that_request_only(engine):
+    eng = engine()
+    with ShearServer(eng, hbm_budget=100, chunk_steps=4) as srv:
+        futs = [srv.submit(_req(i, n_steps=6 + i)) for i in range(5)]
+        with pytest.raises(RuntimeError, match="SW_ETIMEOUT"):
+            futs[2].result(timeout=10)
+        others = [futs[i].result(timeout=10) for i in (0, 1, 3, 4)]
+        # the server keeps serving after the failure
+        late = srv.submit(_req(9, n_steps=3)).result(timeout=10)
+    assert others == [("result", i) for i in (0, 1, 3, 4)]
+    assert late == ("result", 9)
+    st = srv.stats()
+    assert st["failed"] == 1 and st["completed"] == 5
+    assert not eng.live  # every request's memory was released

@@ -523,6 +523,9 @@ def main(argv=None) -> int:
                     help="mixed form: time steps fused per pass over HBM (0 = library default)")
     ap.add_argument("--no-tune", action="store_true",
                     help="skip the autotuner (library default launch shapes)")
+    ap.add_argument("--knobs", default=None,
+                    help="launch-shape knobs name=value,... set instead of the autotuner "
+                         "(shearwave_b200.tune.KNOBS)")
     ap.add_argument("--tune-steps", type=int, default=128,
                     help="time steps of the shortened workload each autotuner candidate runs")
     ap.add_argument("--no-extras", action="store_true",
@@ -565,7 +568,12 @@ def main(argv=None) -> int:
     # ---- launch shapes chosen by the autotuner (shearwave_b200/tune.py) ----
     tune_info = None
     default_knobs = _knobs()
-    if not a.no_tune and not a.steps_per_pass:
+    if a.knobs:
+        from shearwave_b200 import tune
+
+        tune.set_knobs(**{k: int(v) for k, v in (kv.split("=") for kv in a.knobs.split(","))})
+        tune_info = {"knobs": tune.get_knobs(), "set_by": "--knobs"}
+    elif not a.no_tune and not a.steps_per_pass:
         from shearwave_b200 import tune
 
         t0 = time.perf_counter()

@@ -267,13 +267,22 @@ __device__ __forceinline__ void update_tile(const CgInst* __restrict__ tab, int 
   const TileCoord tc = tile_coord(g, in.ts, local);
   const int z = tc.z0 + threadIdx.x, y = tc.y0 + threadIdx.y;
   double acc = 0.0;
-  for (int x = tc.x0; x < tc.x1; ++x) {
-    if (!interior(g, x, y, z)) continue;
-    const long long i = (long long)x * g.sxy + (long long)y * g.pz + z;
-    in.x[i] = fma(alpha, pk[i], in.x[i]);
-    const double rn = fma(-alpha, in.ap[i], in.r[i]);
-    in.r[i] = rn;
-    acc += rn * rn;
+  if (y >= 1 && y <= g.ny - 2 && z >= 1 && z <= g.nz - 2) {
+    // the column's planes are independent: restrict lets the loads of later
+    // planes go ahead of the stores of earlier ones
+    double* __restrict__ X = in.x;
+    double* __restrict__ R = in.r;
+    const double* __restrict__ AP = in.ap;
+    const double* __restrict__ PK = pk;
+    const long long c0 = (long long)y * g.pz + z;
+#pragma unroll 4
+    for (int x = tc.x0; x < tc.x1; ++x) {
+      const long long i = (long long)x * g.sxy + c0;
+      X[i] = fma(alpha, PK[i], X[i]);
+      const double rn = fma(-alpha, AP[i], R[i]);
+      R[i] = rn;
+      acc += rn * rn;
+    }
   }
   double bs = block_sum(acc, red);
   if (flat_tid() == 0) in.partials[local] = make_double2(bs, 0.0);

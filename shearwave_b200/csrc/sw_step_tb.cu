@@ -51,11 +51,13 @@ struct TbCoord {
   int z0, y0, x0, x1;  // output tile: z in [z0, z0+OZ), y in [y0, y0+OY), x in [x0, x1)
 };
 
-__host__ __device__ inline TileSpace make_tiles_tb(const Geom& g, int xc) {
+__host__ __device__ inline TileSpace make_tiles_tb(const Geom& g, int xc, int lz) {
+  const int oz = lz == 32 ? TbShape<32>::OZ : TbShape<64>::OZ;
+  const int oy = lz == 32 ? TbShape<32>::OY : TbShape<64>::OY;
   TileSpace t;
-  // tiles [60 k, 60 k + 60) and [13 k, 13 k + 13) cover the interior 1..n-2
-  t.ntz = g.nz > 2 ? (g.nz - 2) / TmaF32TB::OZ + 1 : 0;
-  t.nty = g.ny > 2 ? (g.ny - 2) / TmaF32TB::OY + 1 : 0;
+  // tiles [oz k, oz k + oz) and [oy k, oy k + oy) cover the interior 1..n-2
+  t.ntz = g.nz > 2 ? (g.nz - 2) / oz + 1 : 0;
+  t.nty = g.ny > 2 ? (g.ny - 2) / oy + 1 : 0;
   const int nxi = g.nx > 2 ? g.nx - 2 : 0;
   t.xc = xc < 1 ? 1 : xc;
   t.nxc = nxi > 0 ? (nxi + t.xc - 1) / t.xc : 0;
@@ -63,14 +65,15 @@ __host__ __device__ inline TileSpace make_tiles_tb(const Geom& g, int xc) {
   return t;
 }
 
+template <int OZ, int OY>
 __device__ inline TbCoord tb_coord(const Geom& g, const TileSpace& t, int local) {
   TbCoord c;
   const int zt = local % t.ntz;
   const int rest = local / t.ntz;
   const int yt = rest % t.nty;
   const int xt = rest / t.nty;
-  c.z0 = TmaF32TB::OZ * zt;
-  c.y0 = TmaF32TB::OY * yt;
+  c.z0 = OZ * zt;
+  c.y0 = OY * yt;
   c.x0 = 1 + xt * t.xc;
   c.x1 = min(c.x0 + t.xc, g.nx - 1);
   return c;
@@ -167,27 +170,34 @@ struct TbPos {
 // (centres only; its full barrier waited on by the caller), then for every
 // plane q = x0-1 .. x1 level 1 at q and level 2 at q-1.  Returns the ring
 // positions after the tile, with ok = false when a wait gave up.
-template <bool VISC, bool DAMP, bool PUSH, bool SNAP>
+template <int LZ, bool VISC, bool DAMP, bool PUSH, bool SNAP>
 __device__ __forceinline__ TbPos tb_tile(const TmaF32TB* __restrict__ in, int local, int lit,
                                          const TbRings& k, TbPos p, int w, int lane) {
   using T = TmaF32TB;
-  constexpr int W = T::W, H = T::H, WB = T::WB, HB = T::HB, LZ = T::LZ;
+  using S = TbShape<LZ>;
+  constexpr int W = S::W, H = S::H, WB = S::WB, HB = S::HB;
   constexpr int AF = T::A_STAGE / 4, BF = T::B_STAGE / 4, LF = T::L_STAGE / 4;
-  constexpr int LP = LZ * T::LY;  // level-1 cells per component
+  constexpr int LP = LZ * S::LY;  // level-1 cells per component
   const Geom& g = in->g;
-  const TbCoord tc = tb_coord(g, in->ts, local);
+  const TbCoord tc = tb_coord<S::OZ, S::OY>(g, in->ts, local);
   float* __restrict__ D = in->state[(lit + 2) % 3];
   const unsigned nc = (unsigned)g.ncell;  // the host keeps ncell below 2^32
   const float damp = in->damp;
   const float hx = in->hx, hy = in->hy, hz = in->hz, hc = lap7_centre_coef(hx, hy, hz);
-  // this thread: level-1 row w (y = y0-1+w), z pair zp, zp+1 (zp = z0-2+2 lane)
-  const int y = tc.y0 - 1 + w, zp = tc.z0 - 2 + 2 * lane;
+  // this thread: level-1 row r (y = y0-1+r), z pair zp, zp+1 (zp = z0-2+2 pl):
+  // a warp owns one row of 32 pairs (LZ 64) or two rows of 16 (LZ 32)
+  const int r = S::RPW == 1 ? w : 2 * w + (lane >> 4);
+  const int pl = lane & (S::PAIRS - 1);
+  const int y = tc.y0 - 1 + r, zp = tc.z0 - 2 + 2 * pl;
   const bool yin = y >= 1 && y <= g.ny - 2;
   const bool zin_a = zp >= 1 && zp <= g.nz - 2, zin_b = zp + 1 >= 1 && zp + 1 <= g.nz - 2;
-  // level 2: rows 1..OY and pairs 1..30 are the output tile
-  const bool out_rc = w >= 1 && w <= T::OY && lane >= 1 && lane <= 30;
+  // a warp whose rows all lie outside the grid interior only writes zeros at
+  // level 1 (the shell that level 2 reads)
+  const bool warp_live = __any_sync(0xffffffffu, yin);
+  // level 2: rows 1..OY and pairs 1..PAIRS-2 are the output tile
+  const bool out_rc = r >= 1 && r <= S::OY && pl >= 1 && pl <= S::PAIRS - 2;
   const bool store = out_rc && yin && zp < g.pz;  // pz is even: the pair is in the row
-  const int o = (w + 1) * W + 2 + 2 * lane, ob = w * WB + 2 + 2 * lane, ol = w * LZ + 2 * lane;
+  const int o = (r + 1) * W + 2 + 2 * pl, ob = r * WB + 2 + 2 * pl, ol = r * LZ + 2 * pl;
   const int j10 = PUSH ? in->term_off[lit] : 0;
   const int j11 = PUSH ? in->term_off[lit + 1] : 0;
   const int j21 = PUSH ? in->term_off[lit + 2] : 0;
@@ -240,8 +250,19 @@ __device__ __forceinline__ TbPos tb_tile(const TmaF32TB* __restrict__ in, int lo
     const float* Bm = k.ringB + pt.s * BF;
     const float2 Mc = tb_ld2(Bm + ob);
     const float2 Ec = VISC ? tb_ld2(Bm + HB * WB + ob) : make_float2(0.f, 0.f);
-    {
-      const bool xin = q >= 1 && q <= g.nx - 2;
+    const bool xin = q >= 1 && q <= g.nx - 2;
+    if (!(xin && warp_live)) {
+      // every cell of the warp's rows is outside the interior: level 1 is the
+      // zero shell; keep this plane's level-0 centres for the next plane
+      const float* P = k.ringA + cur.s * AF;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        pu[c] = tb_ld2(P + o + c * H * W);
+        if (VISC) pd[c] = tb_ld2(P + o + (3 + c) * H * W);
+        tb_st2(Lw + ol + c * LP, 0.f, 0.f);
+        tb_st2(Lw + ol + (3 + c) * LP, 0.f, 0.f);
+      }
+    } else {
       const bool aa = xin && yin && zin_a, ab = xin && yin && zin_b;
       long long i = 0;  // the pair's cell, for the force patterns
       int jl0 = 0, jl1 = 0;
@@ -274,7 +295,7 @@ __device__ __forceinline__ TbPos tb_tile(const TmaF32TB* __restrict__ in, int lo
         }
       } else {
         // ---- level 2: step lit+2 at plane x = q-1 on the output tile ----
-        // (reads rows w-1..w+1 of plane q-1: wait until every warp wrote it)
+        // (reads rows r-1..r+1 of plane q-1: wait until every warp wrote it)
         if (!ws_wait(&k.Lfull[lprev.s], lprev.ph, k.abort_flag)) {
       p.ok = false;
       return p;
@@ -310,25 +331,26 @@ __device__ __forceinline__ TbPos tb_tile(const TmaF32TB* __restrict__ in, int lo
 // Tiles of push or snapshot steps (a few steps of a run) go through a
 // function of their own, so that their extra live values do not raise the
 // register pressure of the loop every other tile runs.
-template <bool VISC, bool DAMP, bool PUSH, bool SNAP>
+template <int LZ, bool VISC, bool DAMP, bool PUSH, bool SNAP>
 __device__ __noinline__ TbPos tb_tile_rare(const TmaF32TB* __restrict__ in, int local, int lit,
                                            TbRings k, TbPos p, int w, int lane) {
-  return tb_tile<VISC, DAMP, PUSH, SNAP>(in, local, lit, k, p, w, lane);
+  return tb_tile<LZ, VISC, DAMP, PUSH, SNAP>(in, local, lit, k, p, w, lane);
 }
 
 // The tile's switches, resolved once per tile into a specialised loop.
-template <bool VISC, bool DAMP>
+template <int LZ, bool VISC, bool DAMP>
 __device__ __forceinline__ TbPos tb_tile_ps(bool push, bool snap, const TmaF32TB* __restrict__ in,
                                             int local, int lit, const TbRings& k, TbPos p, int w,
                                             int lane) {
   if (push) {
-    if (snap) return tb_tile_rare<VISC, DAMP, true, true>(in, local, lit, k, p, w, lane);
-    return tb_tile_rare<VISC, DAMP, true, false>(in, local, lit, k, p, w, lane);
+    if (snap) return tb_tile_rare<LZ, VISC, DAMP, true, true>(in, local, lit, k, p, w, lane);
+    return tb_tile_rare<LZ, VISC, DAMP, true, false>(in, local, lit, k, p, w, lane);
   }
-  if (snap) return tb_tile_rare<VISC, DAMP, false, true>(in, local, lit, k, p, w, lane);
-  return tb_tile<VISC, DAMP, false, false>(in, local, lit, k, p, w, lane);
+  if (snap) return tb_tile_rare<LZ, VISC, DAMP, false, true>(in, local, lit, k, p, w, lane);
+  return tb_tile<LZ, VISC, DAMP, false, false>(in, local, lit, k, p, w, lane);
 }
 
+template <int LZ>
 __device__ __forceinline__ TbPos tb_tile_any(const TmaF32TB* __restrict__ in, int local, int lit,
                                              const TbRings& k, TbPos p, int w, int lane) {
   const bool visc = in->ncoef > 1, damp = in->use_damp != 0;
@@ -336,22 +358,24 @@ __device__ __forceinline__ TbPos tb_tile_any(const TmaF32TB* __restrict__ in, in
   const bool snap = in->snap_stride > 0 && in->snaps != nullptr &&
                     (((lit + 1) % in->snap_stride) == 0 || ((lit + 2) % in->snap_stride) == 0);
   if (visc) {
-    if (damp) return tb_tile_ps<true, true>(push, snap, in, local, lit, k, p, w, lane);
-    return tb_tile_ps<true, false>(push, snap, in, local, lit, k, p, w, lane);
+    if (damp) return tb_tile_ps<LZ, true, true>(push, snap, in, local, lit, k, p, w, lane);
+    return tb_tile_ps<LZ, true, false>(push, snap, in, local, lit, k, p, w, lane);
   }
-  if (damp) return tb_tile_ps<false, true>(push, snap, in, local, lit, k, p, w, lane);
-  return tb_tile_ps<false, false>(push, snap, in, local, lit, k, p, w, lane);
+  if (damp) return tb_tile_ps<LZ, false, true>(push, snap, in, local, lit, k, p, w, lane);
+  return tb_tile_ps<LZ, false, false>(push, snap, in, local, lit, k, p, w, lane);
 }
 
-template <bool BATCH>
+template <bool BATCH, int LZ>
 __global__ void __launch_bounds__(TmaF32TB::THREADS, 1)
     step_f32_fused2(const __grid_constant__ TmaF32TB one, const TmaF32TB* __restrict__ tab,
                     int ninst, int ntiles, int it, const int* __restrict__ it_dev, int* queues) {
+  using S = TbShape<LZ>;
   if (it_dev != nullptr) it += *it_dev;  // step counter kept on the device (graph replays)
   // batched launches take tiles from a launch-wide queue (see step_f32_tma)
   int* queue = queues;
   using T = TmaF32TB;
-  constexpr int NA = T::NA, NB = T::NB, NL = T::NL, WB = T::WB, HB = T::HB;
+  constexpr int NA = T::NA, NB = T::NB, NL = T::NL, WB = S::WB, HB = S::HB;
+  constexpr uint32_t A_BYTES = S::W * S::H * 6 * 4;
   constexpr int AF = T::A_STAGE / 4, BF = T::B_STAGE / 4, LF = T::L_STAGE / 4;
   extern __shared__ unsigned char smem_raw[];
   unsigned char* base = smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u);
@@ -418,7 +442,7 @@ __global__ void __launch_bounds__(TmaF32TB::THREADS, 1)
         lg->solve[lg->n_taken & 7] = k;
         ++lg->n_taken;
         const Geom& g = in->g;
-        const TbCoord tc = tb_coord(g, in->ts, local);
+        const TbCoord tc = tb_coord<S::OZ, S::OY>(g, in->ts, local);
         const CUtensorMap* tma = &in->tm[lit % 3];
         const uint32_t bbytes = WB * HB * 4 * in->ncoef;
         bool first = true;
@@ -437,7 +461,7 @@ __global__ void __launch_bounds__(TmaF32TB::THREADS, 1)
           }
           const int pl = min(max(p, 0), g.nx - 1);  // planes outside the grid feed only the shell
           fence_proxy_async_smem();
-          mbar_arrive_expect_tx(&hd->fullA[sa], T::A_BYTES);
+          mbar_arrive_expect_tx(&hd->fullA[sa], A_BYTES);
           tma_load_4d(ringA + sa * AF, tma, &hd->fullA[sa], tc.z0 - 4, tc.y0 - 2, pl, 0);
           arm_record(lg->armedA, lg->parA, sa, pa.ph);
           pa.next();
@@ -473,7 +497,7 @@ __global__ void __launch_bounds__(TmaF32TB::THREADS, 1)
       const T* in = BATCH ? &tab[solve_slots(base)[p.ca.s]] : &one;
       const int local = BATCH ? t - in->tile_base : t;
       const int lit = it - in->it_begin;
-      p = tb_tile_any(in, local, lit, k, p, warp, lane);
+      p = tb_tile_any<LZ>(in, local, lit, k, p, warp, lane);
       if (!p.ok) break;
       if (lane == 0) ++lg->done[warp];
     }
@@ -504,21 +528,23 @@ static int tb_set_attr() {
   static bool done = false;
   if (done) return SW_OK;
   const int bytes = (int)tb_smem_bytes();
-  cudaError_t e = cudaFuncSetAttribute(step_f32_fused2<false>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(step_f32_fused2<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             bytes);
-  if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(fused step smem)");
+  const void* fns[4] = {(const void*)step_f32_fused2<false, 64>,
+                        (const void*)step_f32_fused2<true, 64>,
+                        (const void*)step_f32_fused2<false, 32>,
+                        (const void*)step_f32_fused2<true, 32>};
+  for (const void* f : fns) {
+    cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(fused step smem)");
+  }
   done = true;
   return SW_OK;
 }
 
 // planes per x chunk: minimise waves x (level-1 planes per tile) on 148 SMs
-static int tb_xchunk(const Geom& g) {
+static int tb_xchunk(const Geom& g, int lz) {
   const long long nxi = g.nx > 2 ? g.nx - 2 : 0;
   if (nxi == 0 || g.nz <= 2 || g.ny <= 2) return 1;
-  const TileSpace one = make_tiles_tb(g, (int)nxi);
+  const TileSpace one = make_tiles_tb(g, (int)nxi, lz);
   const long long cols = (long long)one.ntz * one.nty;
   const long long slots = kNumSMs;
   long long best_nc = 1, best = -1;
@@ -534,14 +560,34 @@ static int tb_xchunk(const Geom& g) {
   return (int)((nxi + best_nc - 1) / best_nc);
 }
 
-int make_tma_f32_tb(const StepArgs& a, int xchunk, TmaF32TB* t) {
+// Cells the two levels compute per interior plane for tile width lz: the
+// tiles times (level-1 region + output tile).
+long long tb_work(const Geom& g, int lz) {
+  const TileSpace t = make_tiles_tb(g, 1, lz);
+  const long long per = lz == 32
+                            ? (long long)TbShape<32>::LZ * TbShape<32>::LY +
+                                  (long long)TbShape<32>::OZ * TbShape<32>::OY
+                            : (long long)TbShape<64>::LZ * TbShape<64>::LY +
+                                  (long long)TbShape<64>::OZ * TbShape<64>::OY;
+  return (long long)t.ntz * t.nty * per;
+}
+
+int tb_tile_width(const Geom& g) {
+  const int knob = tune_get(SW_TUNE_TILE_SHAPE);
+  if (knob == 1) return 64;
+  if (knob == 2) return 32;
+  return tb_work(g, 32) < tb_work(g, 64) ? 32 : 64;
+}
+
+int make_tma_f32_tb(const StepArgs& a, int xchunk, TmaF32TB* t, int lz) {
   *t = TmaF32TB{};
   if (a.g.ncell >= (1LL << 32)) {  // the kernel offsets components by a 32-bit cell count
     set_error("grid too large for the two-step kernel (%lld cells)", a.g.ncell);
     return SW_ERANGE;
   }
+  t->lz = lz == 32 || lz == 64 ? lz : tb_tile_width(a.g);
   t->g = a.g;
-  t->ts = make_tiles_tb(a.g, xchunk > 0 ? xchunk : tb_xchunk(a.g));
+  t->ts = make_tiles_tb(a.g, xchunk > 0 ? xchunk : tb_xchunk(a.g, t->lz), t->lz);
   if (a.coef_e == nullptr) {
     t->ncoef = 1;
   } else if ((const char*)a.coef_e == (const char*)a.coef_m + a.g.ncell * 4) {
@@ -554,10 +600,15 @@ int make_tma_f32_tb(const StepArgs& a, int xchunk, TmaF32TB* t) {
     set_error("the two-steps-per-pass kernel runs without the compensated sum");
     return SW_EINVAL;
   }
+  const bool n32 = t->lz == 32;
+  const uint32_t W = n32 ? TbShape<32>::W : TbShape<64>::W;
+  const uint32_t H = n32 ? TbShape<32>::H : TbShape<64>::H;
+  const uint32_t WB = n32 ? TbShape<32>::WB : TbShape<64>::WB;
+  const uint32_t HB = n32 ? TbShape<32>::HB : TbShape<64>::HB;
   const uint64_t dims[4] = {(uint64_t)a.g.pz, (uint64_t)a.g.ny, (uint64_t)a.g.nx, 9};
   const uint64_t strides[3] = {(uint64_t)a.g.pz * 4, (uint64_t)a.g.sxy * 4,
                                (uint64_t)a.g.ncell * 4};
-  const uint32_t boxA[4] = {TmaF32TB::W, TmaF32TB::H, 1, 6};
+  const uint32_t boxA[4] = {W, H, 1, 6};
   for (int b = 0; b < 3; ++b) {
     t->state[b] = (float*)a.state[b];
     int rc = encode_tmap_4d(&t->tm[b], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, a.state[b], dims, strides,
@@ -566,7 +617,7 @@ int make_tma_f32_tb(const StepArgs& a, int xchunk, TmaF32TB* t) {
   }
   const uint64_t mdims[4] = {(uint64_t)a.g.pz, (uint64_t)a.g.ny, (uint64_t)a.g.nx,
                              (uint64_t)t->ncoef};
-  const uint32_t boxM[4] = {TmaF32TB::WB, TmaF32TB::HB, 1, (uint32_t)t->ncoef};
+  const uint32_t boxM[4] = {WB, HB, 1, (uint32_t)t->ncoef};
   int rc = encode_tmap_4d(&t->tmm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, (void*)a.coef_m, mdims,
                           strides, boxM);
   if (rc != SW_OK) return rc;
@@ -592,41 +643,51 @@ int make_tma_f32_tb(const StepArgs& a, int xchunk, TmaF32TB* t) {
 
 int launch_fused2_prepare() { return tb_set_attr(); }
 
-const void* step_f32_fused2_ptr() { return reinterpret_cast<const void*>(step_f32_fused2<false>); }
+const void* step_f32_fused2_ptr(int lz) {
+  return lz == 32 ? reinterpret_cast<const void*>(step_f32_fused2<false, 32>)
+                  : reinterpret_cast<const void*>(step_f32_fused2<false, 64>);
+}
 
-const void* step_f32_fused2_batch_ptr() {
-  return reinterpret_cast<const void*>(step_f32_fused2<true>);
+const void* step_f32_fused2_batch_ptr(int lz) {
+  return lz == 32 ? reinterpret_cast<const void*>(step_f32_fused2<true, 32>)
+                  : reinterpret_cast<const void*>(step_f32_fused2<true, 64>);
+}
+
+static void launch_tb(const void* fn, int grid, cudaStream_t s, const TmaF32TB& one,
+                      const TmaF32TB* tab, int ninst, int ntiles, int it, int* queues) {
+  const int* itd = nullptr;
+  void* args[] = {(void*)&one, (void*)&tab, (void*)&ninst, (void*)&ntiles, (void*)&it,
+                  (void*)&itd, (void*)&queues};
+  cudaLaunchKernel(fn, dim3(grid), dim3(TmaF32TB::THREADS), args, tb_smem_bytes(), s);
 }
 
 void launch_fused2_raw(const TmaF32TB& t, int it, cudaStream_t s) {
   if (t.ts.count == 0) return;
-  step_f32_fused2<false><<<std::min(t.ts.count, kNumSMs), TmaF32TB::THREADS, tb_smem_bytes(),
-                           s>>>(t, nullptr, 1, t.ts.count, it, nullptr, nullptr);
+  launch_tb(step_f32_fused2_ptr(t.lz), std::min(t.ts.count, kNumSMs), s, t, nullptr, 1,
+            t.ts.count, it, nullptr);
 }
 
 int launch_fused2(const StepArgs& a, int xchunk, int it, cudaStream_t s) {
   int rc = tb_set_attr();
   if (rc != SW_OK) return rc;
   TmaF32TB t;
-  rc = make_tma_f32_tb(a, xchunk, &t);
+  rc = make_tma_f32_tb(a, xchunk, &t, 0);
   if (rc != SW_OK) return rc;
   if (t.ts.count == 0) return SW_OK;
-  const int grid = std::min(t.ts.count, kNumSMs);
-  step_f32_fused2<false><<<grid, TmaF32TB::THREADS, tb_smem_bytes(), s>>>(
-      t, nullptr, 1, t.ts.count, it, nullptr, nullptr);
+  launch_fused2_raw(t, it, s);
   count_launches(1);
   SW_CHECK_LAUNCH("fused two-step kernel");
   return SW_OK;
 }
 
-int launch_fused2_batch(const void* d_tab, int ninst, int ntiles, int it, int* queues,
+int launch_fused2_batch(const void* d_tab, int ninst, int ntiles, int it, int* queues, int lz,
                         cudaStream_t s) {
   int rc = tb_set_attr();
   if (rc != SW_OK) return rc;
   if (ntiles == 0) return SW_OK;
   TmaF32TB dummy{};
-  step_f32_fused2<true><<<std::min(ntiles, kNumSMs), TmaF32TB::THREADS, tb_smem_bytes(), s>>>(
-      dummy, (const TmaF32TB*)d_tab, ninst, ntiles, it, nullptr, queues);
+  launch_tb(step_f32_fused2_batch_ptr(lz), std::min(ntiles, kNumSMs), s, dummy,
+            (const TmaF32TB*)d_tab, ninst, ntiles, it, queues);
   count_launches(1);
   SW_CHECK_LAUNCH("fused two-step kernel (batch)");
   return SW_OK;

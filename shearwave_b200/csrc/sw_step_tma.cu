@@ -1015,7 +1015,7 @@ int launch_steps_tma(const StepArgs& a, int xchunk, int it0, int nsteps, cudaStr
     if (t.ts.count == 0) return SW_OK;
     TmaF32TB tb;
     if (fuse) {
-      rc = make_tma_f32_tb(a, 0, &tb);
+      rc = make_tma_f32_tb(a, 0, &tb, 0);
       if (rc != SW_OK) return rc;
       rc = launch_fused2_prepare();
       if (rc != SW_OK) return rc;
@@ -1024,7 +1024,7 @@ int launch_steps_tma(const StepArgs& a, int xchunk, int it0, int nsteps, cudaStr
     unsigned long long n_launch = 0;
     int done = 0;
     if (fuse && tb.ts.count > 0)
-      rc = graph_loop(const_cast<void*>(step_f32_fused2_ptr()), tb,
+      rc = graph_loop(const_cast<void*>(step_f32_fused2_ptr(tb.lz)), tb,
                       std::min(tb.ts.count, kNumSMs), TmaF32TB::THREADS, tb_smem_bytes(), 2, 16,
                       a.clock, a.queue, it0, nsteps, s, &done);
     else
@@ -1146,6 +1146,23 @@ static int batch_tile_width(const sw_fdtd_desc* descs, const std::vector<int>& r
   return c32 < c64 ? 32 : 64;
 }
 
+// Tile width of a batched two-step launch: the one whose tiles compute fewer
+// cells over the running solves (weighted by their interior planes), or the
+// SW_TUNE_TILE_SHAPE knob's.
+static int batch_tb_width(const sw_fdtd_desc* descs, const std::vector<int>& run) {
+  const int knob = tune_get(SW_TUNE_TILE_SHAPE);
+  if (knob == 1) return 64;
+  if (knob == 2) return 32;
+  long long w64 = 0, w32 = 0;
+  for (int i : run) {
+    const Geom g = make_geom(descs[i].nx, descs[i].ny, descs[i].nz, descs[i].pz);
+    const long long nxi = std::max(0, descs[i].nx - 2);
+    w64 += tb_work(g, 64) * nxi;
+    w32 += tb_work(g, 32) * nxi;
+  }
+  return w32 < w64 ? 32 : 64;
+}
+
 // Table of the solves running at step `it`, in batch_order, with their tile
 // ranges laid end to end.
 template <typename Inst>
@@ -1207,6 +1224,7 @@ int batch_steps_mixed(const sw_fdtd_desc* descs, const int32_t* begins, int n, i
   int cur_kind = -1;  // 0 single, 1 fused
   std::vector<TmaF32> tsingle;
   std::vector<TmaF32TB> tfused;
+  int tb_lz = 64;  // tile width of the fused launches (per rebuild)
   int ntiles = 0;
   if (fuse_ok) {
     int rc = launch_fused2_prepare();
@@ -1236,6 +1254,7 @@ int batch_steps_mixed(const sw_fdtd_desc* descs, const int32_t* begins, int n, i
         std::vector<int> run;
         for (int i = 0; i < n; ++i)
           if (cur[i]) run.push_back(i);
+        tb_lz = batch_tb_width(descs, run);
         for (int i : batch_order(descs, run)) {
           StepArgs a;
           int rc = make_step_args(&descs[i], &a);
@@ -1244,7 +1263,8 @@ int batch_steps_mixed(const sw_fdtd_desc* descs, const int32_t* begins, int n, i
           // planes per x chunk: the solve's own, else the SW_TUNE_XCHUNK knob,
           // else 32 (each chunk re-reads four halo planes of level 0)
           const int kx = tune_get(SW_TUNE_XCHUNK);
-          rc = make_tma_f32_tb(a, descs[i].xchunk > 0 ? descs[i].xchunk : (kx > 0 ? kx : 32), &t);
+          rc = make_tma_f32_tb(a, descs[i].xchunk > 0 ? descs[i].xchunk : (kx > 0 ? kx : 32), &t,
+                               tb_lz);
           if (rc != SW_OK) return rc;
           t.it_begin = begins ? begins[i] : 0;
           t.tile_base = ntiles;
@@ -1280,7 +1300,7 @@ int batch_steps_mixed(const sw_fdtd_desc* descs, const int32_t* begins, int n, i
       if (stop - it >= 64) {
         int done = 0;
         TmaF32TB dummy{};
-        rc = graph_loop<TmaF32TB>(const_cast<void*>(step_f32_fused2_batch_ptr()), dummy,
+        rc = graph_loop<TmaF32TB>(const_cast<void*>(step_f32_fused2_batch_ptr(tb_lz)), dummy,
                                   std::min(ntiles, kNumSMs), TmaF32TB::THREADS, tb_smem_bytes(),
                                   2, 16, queues + 2, queues, it, stop - it, s, &done,
                                   (const TmaF32TB*)tab_fused, (int)tfused.size(), ntiles);
@@ -1290,7 +1310,7 @@ int batch_steps_mixed(const sw_fdtd_desc* descs, const int32_t* begins, int n, i
           continue;
         }
       }
-      rc = launch_fused2_batch(tab_fused, (int)tfused.size(), ntiles, it, queues, s);
+      rc = launch_fused2_batch(tab_fused, (int)tfused.size(), ntiles, it, queues, tb_lz, s);
       it += 2;
     } else {
       bool kr = false;  // the compensation ring layout if any running solve needs it

@@ -93,33 +93,47 @@ struct TmaF64 {
   int stall_test;
 };
 
+// Tile shapes of the two-steps-per-pass kernel (one per launch): output
+// tiles of OZ x OY cells starting at z = OZ kz, y = OY ky; step t+1 is
+// computed on the LZ x LY region around the tile (z from z0-2, y from y0-1:
+// the tile plus one cell of halo, and one more column each side in z so
+// that z pairs stay 8-byte aligned), step t+2 on the tile.  Each of the 15
+// consumer warps owns RPW level-1 rows of LZ/2 z pairs:
+//   LZ 64: one row of 32 pairs per warp, 64 x 15 -> 60 x 13 output cells;
+//   LZ 32: two rows of 16 pairs per warp, 32 x 30 -> 28 x 28 output cells
+//          (the narrower tile wastes less of a grid whose interior is not a
+//          multiple of 60 cells wide).
+//   level-0 box (u and d, 6 components): W x H from (z0-4, y0-2);
+//   coefficient box: WB x HB from (z0-4, y0-1).
+template <int LZ_>
+struct TbShape {
+  static constexpr int LZ = LZ_;
+  static constexpr int PAIRS = LZ / 2;  // z pairs per level-1 row
+  static constexpr int RPW = 64 / LZ;   // level-1 rows per consumer warp
+  static constexpr int LY = 15 * RPW;
+  static constexpr int OZ = LZ - 4, OY = LY - 2;
+  static constexpr int W = LZ + 4, H = OY + 4;
+  static constexpr int WB = LZ + 4, HB = LY;
+};
+
+constexpr int cmax(int a, int b) { return a > b ? a : b; }
+
 // Kernel-side view of one mixed-form solve for the two-steps-per-pass kernel
-// (no compensated sum).  Output tiles are OZ x OY cells starting at
-// z = 60 kz, y = 13 ky; step t+1 is computed on the LZ x LY region around
-// the tile (z from z0-2, y from y0-1: the tile plus one cell of halo, and one
-// more column each side in z so that z pairs stay 8-byte aligned), step t+2
-// on the tile.  A CTA has LY consumer warps, one level-1 row of 32 z pairs
-// each.
-//   tm[b]  : state buffer b (pz, ny, nx, 9), box (W, H, 1, 6) from (z0-4,
-//            y0-2): u and d with two cells of halo (and alignment) around
-//            the tile
-//   tmm    : coefficients (pz, ny, nx, ncoef), box (WB, HB, 1, ncoef) from
-//            (z0-4, y0-1): the level-1 rows
+// (no compensated sum).  The ring stages are sized for either tile shape.
+//   tm[b]  : state buffer b (pz, ny, nx, 9), box (W, H, 1, 6) of the shape
+//   tmm    : coefficients (pz, ny, nx, ncoef), box (WB, HB, 1, ncoef)
 struct TmaF32TB {
   // 15 consumer warps + the producer = 16 warps: four per scheduler, which
   // leaves each thread up to 128 registers (17 warps would cap it at 96)
-  static constexpr int OZ = 60, OY = 13;  // output tile (z, y)
-  static constexpr int LZ = 64, LY = 15;  // step-(t+1) region
-  static constexpr int W = 68, H = OY + 4;
-  static constexpr int WB = 68, HB = LY;
   // ring stages: level 0 (planes q, q+1 held, two in flight), points, level 1
   static constexpr int NA = 4, NB = 3, NL = 3;
-  static constexpr int A_BYTES = W * H * 6 * 4;
-  static constexpr int M_BYTES = WB * HB * 2 * 4;
-  static constexpr int A_STAGE = round128(A_BYTES);
-  static constexpr int B_STAGE = round128(M_BYTES);
-  static constexpr int L_STAGE = round128(LZ * LY * 6 * 4);
-  static constexpr int CONSUMER_WARPS = LY;
+  static constexpr int A_STAGE =
+      round128(cmax(TbShape<64>::W * TbShape<64>::H, TbShape<32>::W * TbShape<32>::H) * 6 * 4);
+  static constexpr int B_STAGE = round128(
+      cmax(TbShape<64>::WB * TbShape<64>::HB, TbShape<32>::WB * TbShape<32>::HB) * 2 * 4);
+  static constexpr int L_STAGE = round128(
+      cmax(TbShape<64>::LZ * TbShape<64>::LY, TbShape<32>::LZ * TbShape<32>::LY) * 6 * 4);
+  static constexpr int CONSUMER_WARPS = 15;
   static constexpr int THREADS = 32 * (CONSUMER_WARPS + 1);
   CUtensorMap tm[3];
   CUtensorMap tmm;
@@ -139,17 +153,23 @@ struct TmaF32TB {
   int tile_base;
   int wait_k;
   int stall_test;
+  int lz;  // tile shape (TbShape<lz>): every solve of a launch has the launch's
 };
 
 size_t tma_smem_bytes(int precision);
 size_t tb_smem_bytes();
-int make_tma_f32_tb(const StepArgs& a, int xchunk, TmaF32TB* t);
+// Two-step tile width for a grid (64 or 32; the SW_TUNE_TILE_SHAPE knob can
+// force one) and the cells both levels compute for a width (tiles x region).
+int tb_tile_width(const Geom& g);
+long long tb_work(const Geom& g, int lz);
+// lz 0: tb_tile_width(a.g)
+int make_tma_f32_tb(const StepArgs& a, int xchunk, TmaF32TB* t, int lz);
 int launch_fused2(const StepArgs& a, int xchunk, int it, cudaStream_t s);
 int launch_fused2_prepare();                                   // kernel attributes, once
 void launch_fused2_raw(const TmaF32TB& t, int it, cudaStream_t s);  // enqueue one launch
-const void* step_f32_fused2_ptr();  // the single-solve fused kernel (for graph nodes)
-const void* step_f32_fused2_batch_ptr();  // the batched fused kernel (for graph nodes)
-int launch_fused2_batch(const void* d_tab, int ninst, int ntiles, int it, int* queues,
+const void* step_f32_fused2_ptr(int lz);        // the single-solve fused kernel (graph nodes)
+const void* step_f32_fused2_batch_ptr(int lz);  // the batched fused kernel (graph nodes)
+int launch_fused2_batch(const void* d_tab, int ninst, int ntiles, int it, int* queues, int lz,
                         cudaStream_t s);
 int tma_xchunk(const Geom& g, int tz, int ty, long long want_tiles);
 // Mixed-step tile width for a grid (64 or 32; the SW_TUNE_TILE_SHAPE knob

@@ -401,8 +401,9 @@ def make_desc(state, coef, inv_rho, patterns, term_off, term_pat, term_scale, sn
     d.coef_m = coef[0].data_ptr()
     d.coef_e = coef[1].data_ptr() if iparams[I_ETA] else None
     d.inv_rho = _p(inv_rho)
-    d.patterns = patterns.data_ptr()
-    d.n_patterns = int(patterns.shape[0])
+    # an empty placeholder (before the projection) is no pattern at all
+    d.patterns = patterns.data_ptr() if patterns.numel() else None
+    d.n_patterns = int(patterns.shape[0]) if patterns.numel() else 0
     d.term_off = _p(term_off)
     d.term_pat = _p(term_pat)
     d.term_scale = _p(term_scale)
@@ -529,6 +530,7 @@ def _(*args):
 
 @_op("fdtd_batch_steps_", mutates=("state", "flags", "queue"))
 def fdtd_batch_steps_(state: Sequence[Tensor], coef: Sequence[Tensor],
+                      inv_rho: Sequence[Optional[Tensor]],
                       patterns: Sequence[Tensor], term_off: Sequence[Tensor],
                       term_pat: Sequence[Tensor], term_scale: Sequence[Tensor],
                       snaps: Sequence[Optional[Tensor]], flags: Sequence[Tensor],
@@ -544,7 +546,7 @@ def fdtd_batch_steps_(state: Sequence[Tensor], coef: Sequence[Tensor],
     descs = (_native.FdtdDesc * n)()
     nf, ni = len(fparams) // n, len(iparams) // n
     for k in range(n):
-        descs[k] = make_desc(state[k], coef[k], None, patterns[k], term_off[k], term_pat[k],
+        descs[k] = make_desc(state[k], coef[k], inv_rho[k], patterns[k], term_off[k], term_pat[k],
                              term_scale[k], snaps[k], None, None, flags[k], None, queue[k],
                              fparams[nf * k: nf * (k + 1)], iparams[ni * k: ni * (k + 1)])
     beg = (C.c_int32 * n)(*[int(b) for b in begins]) if len(begins) else None

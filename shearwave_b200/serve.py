@@ -97,6 +97,9 @@ class GpuEngine:
         ncell = nx * ny * pz
         es = 8 if (p.get("opts") or {}).get("precision", self.precision) == "fp64" else 4
         nterms = 1 + len((p.get("opts") or {}).get("force_terms") or ())
+        for b in (p["bx"], p["by"], p["bz"]):
+            if b is not None and len(b.shape) == 4:  # 4-D forces: one pattern per step at most
+                nterms = max(nterms, int(b.shape[3]) + nterms - 1)
         state = 3 * (3 if es == 8 else 9) * ncell * es
         coef = 2 * ncell * es
         pats = nterms * 3 * ncell * es
@@ -111,7 +114,7 @@ class GpuEngine:
         self.native.call("sw_set_device", self.dev.index)
 
     def admit(self, p):
-        from .solver import _project_raw, _Solve
+        from .solver import _project_inputs, _Solve
 
         with self.torch.cuda.stream(self.stream):
             opts = dict(p.get("opts") or {})
@@ -122,10 +125,7 @@ class GpuEngine:
             if sv.needs_per_step_host(None):
                 raise ValueError("the server runs batchable requests only (no 4-D forces, "
                                  "reproject_every, verbose, traces or direct kernels)")
-            for k, comps in sv.separable_inputs():
-                fs, st = _project_raw(comps, sv.spacing, sv.tol, sv.max_iters, sv.method)
-                sv.cg_log.append(st)
-                sv.store_pattern(k, fs)
+            _project_inputs([sv])
             sv.build_terms()
             sv.mark_steps_begin()
             return sv
@@ -313,7 +313,7 @@ class ShearServer:
                     continue
             try:
                 req.handle = self.engine.admit(req.problem)
-            except (ValueError, MemoryError) as e:  # bad request or no memory: fail it alone
+            except Exception as e:  # bad request, no memory or a device error: fail it alone
                 self.failed += 1
                 req.future.set_exception(e)
                 continue

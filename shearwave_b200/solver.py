@@ -569,7 +569,22 @@ class _Solve:
         ops.fdtd_init_(*run.bundle(), iu, iv)
 
         self.n_sep = len(self.forces.separable)
-        n_pat = self.n_sep + (1 if self.forces.stream4d is not None else 0)
+        # 4-D forces: every step whose force slice is non-zero is projected up
+        # front (one batched CG over the slices) and kept on the device as a
+        # pattern of its own, so the time loop streams them from HBM with no
+        # host work between steps -- unless the patterns would take more
+        # than opts["force_stream_bytes"] (4 GiB), in which case each slice
+        # is projected on the host's cue just before its step
+        self.stream_steps = None
+        n_pat = self.n_sep
+        if self.forces.stream4d is not None:
+            nzs = [it for it in range(n_steps) if not self.forces.zero_steps[it]]
+            need = len(nzs) * 3 * run.ncell * run.state.element_size()
+            if need <= int(opts.get("force_stream_bytes", 4 << 30)):
+                self.stream_steps = nzs
+                n_pat += len(nzs)
+            else:
+                n_pat += 1
         self.pats = torch.zeros((max(n_pat, 1), 3, run.ncell), dtype=dt, device=dev)
         self.cg_log = []
 
@@ -589,13 +604,31 @@ class _Solve:
     # ---- phases ---------------------------------------------------------
     def needs_per_step_host(self, callback) -> bool:
         """Whether the time loop must return to the host between steps."""
-        return (callback is not None or self.forces.stream4d is not None
+        return (callback is not None or self._host_projects_4d()
                 or bool(self.reproject_every) or bool(self.verbose)
                 or self.run.traces is not None or self.run.kernel != 0)
+
+    def _host_projects_4d(self) -> bool:
+        return self.forces.stream4d is not None and self.stream_steps is None
 
     def separable_inputs(self):
         """(pattern index, device components) of every separable force term."""
         return [(k, comps) for k, (comps, _env) in enumerate(self.forces.separable)]
+
+    def _slice(self, it):
+        """The force components of step it in 4-D mode (solver.py:198-199)."""
+        return [None if b is None else (b[..., it] if b.dim() == 4 else b).contiguous()
+                for b in self.forces.stream4d]
+
+    def stream_inputs(self):
+        """(pattern index, device components) of every 4-D force slice that is
+        projected up front (the non-zero steps, in step order)."""
+        if self.stream_steps is None:
+            return []
+        return [(self.n_sep + j, self._slice(it)) for j, it in enumerate(self.stream_steps)]
+
+    def projection_inputs(self):
+        return self.separable_inputs() + self.stream_inputs()
 
     def store_pattern(self, k: int, fs_out: torch.Tensor):
         """Store a projected pattern (3 padded FP64 components) as term k."""
@@ -603,6 +636,8 @@ class _Solve:
 
     def build_terms(self):
         f = self.forces
+        if self.stream_steps is not None:
+            self._stream_index = {it: j for j, it in enumerate(self.stream_steps)}
         term_off, term_pat, term_scale = [0], [], []
         for it in range(self.n_steps):
             for k, (_c, env) in enumerate(f.separable):
@@ -611,7 +646,8 @@ class _Solve:
                     term_pat.append(k)
                     term_scale.append(s)
             if f.stream4d is not None and not f.zero_steps[it]:
-                term_pat.append(self.n_sep)
+                term_pat.append(self.n_sep + (self._stream_index[it] if self.stream_steps
+                                              is not None else 0))
                 term_scale.append(1.0)
             term_off.append(len(term_pat))
         self.term_off = term_off
@@ -702,7 +738,7 @@ class _Solve:
         n_steps = self.n_steps
         dX, dY, dZ = self.spacing
         f = self.forces
-        per_step = callback is not None or f.stream4d is not None
+        per_step = callback is not None or self._host_projects_4d()
         events = set()
         if self.reproject_every:
             events.update(range(self.reproject_every, n_steps + 1, self.reproject_every))
@@ -716,12 +752,10 @@ class _Solve:
             else:
                 later = [e for e in events if e > it]
                 end = min(later) if later else n_steps
-            if f.stream4d is not None and not f.zero_steps[it]:
+            if self._host_projects_4d() and not f.zero_steps[it]:
                 # per-step projection of b[..., it] (solver.py:198-199)
-                comps = [None if b is None else (b[..., it] if b.dim() == 4 else b).contiguous()
-                         for b in f.stream4d]
-                fs, st = _project_raw(comps, (dX, dY, dZ), self.tol, self.max_iters,
-                                      self.method)
+                fs, st = _project_raw(self._slice(it), (dX, dY, dZ), self.tol,
+                                      self.max_iters, self.method)
                 self.cg_log.append(st)
                 self.store_pattern(self.n_sep, fs)
             ops.fdtd_steps_(*run.bundle(), it, end - it)
@@ -779,7 +813,10 @@ def shear_fdtd(
     fuses two time steps per pass over HBM, except with ``kahan``; 1 one
     step per launch; 0 (default) two in batches, one for a lone solve), ``cuda_graph`` (True: long step runs replay one instantiated CUDA
     graph of 32 steps), ``force_terms`` (extra separable terms:
-    list of ``((bx, by, bz), env)``), ``snapshot_stride`` (alias of the
+    list of ``((bx, by, bz), env)``), ``force_stream_bytes`` (4-D forces: the
+    non-zero slices are projected up front and streamed from the device
+    while their patterns fit in this many bytes, 4 GiB by default; above it
+    each slice is projected just before its step), ``snapshot_stride`` (alias of the
     keyword), ``info`` (dict filled with CG statistics, phase times and a
     non-finite flag).
 
@@ -797,10 +834,7 @@ def _solve_alone(sv: _Solve, callback, return_device):
     """Projection, time loop and outputs of one solve."""
     if sv.verbose and sv.n_sep:
         print("Pre-computing Helmholtz projection (separable force)...")
-    for k, comps in sv.separable_inputs():
-        fs, st = _project_raw(comps, sv.spacing, sv.tol, sv.max_iters, sv.method)
-        sv.cg_log.append(st)
-        sv.store_pattern(k, fs)
+    _project_inputs([sv])
     sv.build_terms()
     sv.run_loop(callback)
     return sv.finish(return_device)
@@ -869,31 +903,8 @@ def _run_batch_group(solves, return_device, copy_stream):
     (``copy_stream``) are enqueued right there, so they run while the
     longer solves are still stepping.  Returns one finish handle per solve.
     """
-    # ---- batched projection of every separable pattern ----
-    jobs, owners = [], []
-    for sv in solves:
-        if sv.method == "spectral":  # direct solves: one after another, each ~1 ms
-            for k, comps in sv.separable_inputs():
-                fs, st = _project_raw(comps, sv.spacing, sv.tol, sv.max_iters, "spectral")
-                sv.cg_log.append(st)
-                sv.store_pattern(k, fs)
-            continue
-        for k, comps in sv.separable_inputs():
-            jobs.append((comps, sv))
-            owners.append((sv, k))
-    if jobs:
-        dtypes = sorted({sv.dt for _, sv in jobs}, key=str)
-        for dt in dtypes:
-            idx = [q for q, (_, sv) in enumerate(jobs) if sv.dt == dt]
-            comps = [jobs[q][0] for q in idx]
-            outs, stats = ops.project_batch(
-                [c[0] for c in comps], [c[1] for c in comps], [c[2] for c in comps],
-                [h for q in idx for h in jobs[q][1].spacing],
-                [float(jobs[q][1].tol) for q in idx], [int(jobs[q][1].max_iters) for q in idx])
-            for q, fs, st in zip(idx, outs, stats):
-                sv, k = owners[q]
-                sv.cg_log.append(_stats_dict(st))
-                sv.store_pattern(k, fs)
+    # ---- batched projection of every pattern ----
+    _project_inputs(solves)
     for sv in solves:
         sv.build_terms()
         sv.mark_steps_begin()
@@ -911,11 +922,39 @@ def _run_batch_group(solves, return_device, copy_stream):
     return handles
 
 
+def _project_inputs(solves, chunk=16):
+    """Project every force pattern of the solves (separable terms and the
+    non-zero 4-D slices) and store them: the spectral solves one by one, the
+    CG solves as batched CGs of up to ``chunk`` fields (every CG launch
+    advances all of them, each with its own stopping rule)."""
+    jobs = []
+    for sv in solves:
+        for k, comps in sv.projection_inputs():
+            if sv.method == "spectral":  # direct solves: one after another, each ~1 ms
+                fs, st = _project_raw(comps, sv.spacing, sv.tol, sv.max_iters, "spectral")
+                sv.cg_log.append(st)
+                sv.store_pattern(k, fs)
+            else:
+                jobs.append((comps, sv, k))
+    for dt in sorted({sv.dt for _, sv, _ in jobs}, key=str):
+        same = [j for j in jobs if j[1].dt == dt]
+        for a in range(0, len(same), chunk):
+            part = same[a:a + chunk]
+            outs, stats = ops.project_batch(
+                [c[0] for c, _, _ in part], [c[1] for c, _, _ in part],
+                [c[2] for c, _, _ in part], [h for _, sv, _ in part for h in sv.spacing],
+                [float(sv.tol) for _, sv, _ in part], [int(sv.max_iters) for _, sv, _ in part])
+            for (_, sv, k), fs, st in zip(part, outs, stats):
+                sv.cg_log.append(_stats_dict(st))
+                sv.store_pattern(k, fs)
+
+
 def _batch_steps(runs, begins, it0, nsteps):
     """One fdtd_batch_steps_ call over the solves' device state (begins: an
     empty list starts every solve at step 0)."""
     b = [r.bundle() for r in runs]
-    ops.fdtd_batch_steps_([x[0] for x in b], [x[1] for x in b], [x[3] for x in b],
+    ops.fdtd_batch_steps_([x[0] for x in b], [x[1] for x in b], [x[2] for x in b],
+                          [x[3] for x in b],
                           [x[4] for x in b], [x[5] for x in b], [x[6] for x in b],
                           [x[7] for x in b], [x[10] for x in b], [x[12] for x in b],
                           [f for x in b for f in x[13]], [i for x in b for i in x[14]],

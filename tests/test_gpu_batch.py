@@ -105,3 +105,28 @@ def test_long_batch_replays_graphs_bitwise(cuda, precision):
         ref = _alone(p, precision)
         for a, b in zip(res, ref):
             assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_4d_force_streamed_from_the_device(cuda, precision):
+    """4-D forces: the non-zero slices are projected up front (batched CG)
+    and streamed as patterns; bit for bit the per-step host projection of the
+    reference's loop (solver.py:198-199), which a zero byte budget forces;
+    the solve also joins a batch unchanged."""
+    import shearwave_b200 as sw
+    from shearwave_b200 import workloads as W
+
+    p = W.problem_inclusions((20, 16, 24), 30, seed=77, tol=1e-9)
+    t = np.arange(30, dtype=np.float32)
+    env = (np.sin(0.3 * t) * (t < 18)).astype(np.float32)
+    b4 = (p["bz"][..., None] * env[None, None, None, :]).astype(np.float32)
+    opts = {k: v for k, v in p["opts"].items() if k != "env_t"}
+    q = dict(p, bz=b4, opts=opts)
+    args = (None, None, b4, p["rho"], p["mu"], p["dX"], p["dY"], p["dZ"], p["dT"], 30)
+    streamed = sw.shear_fdtd(*args, dict(opts, precision=precision))
+    host = sw.shear_fdtd(*args, dict(opts, precision=precision, force_stream_bytes=0))
+    for a, b in zip(streamed, host):
+        assert np.array_equal(a, b)
+    batched = sw.shear_fdtd_batch([q, _problems()[0]], precision=precision)
+    for a, b in zip(batched[0], streamed):
+        assert np.array_equal(a, b)

@@ -84,15 +84,18 @@ def test_against_oracle(cuda, shape):
         assert rel_l2(b, r) <= 1e-4
 
 
-FUSED_GRIDS = [(5, 7, 9), (17, 13, 11), (3, 20, 70), (40, 9, 133), (12, 33, 65), (70, 16, 64)]
+FUSED_GRIDS = [(5, 7, 9), (17, 13, 11), (3, 20, 70), (40, 9, 133), (12, 33, 65), (70, 16, 64),
+               (9, 71, 37)]
 
 
 @pytest.mark.parametrize("shape", FUSED_GRIDS)
 @pytest.mark.parametrize("kahan", [True, False])
-def test_two_steps_per_pass_matches_one(cuda, shape, kahan):
+@pytest.mark.parametrize("tile_shape", [1, 2])
+def test_two_steps_per_pass_matches_one(cuda, shape, kahan, tile_shape):
     """The fused two-step kernel reproduces two one-step launches bit for bit
     (both use the same per-cell arithmetic; with the compensated sum the
-    one-step kernel runs both).
+    one-step kernel runs both), with either tile shape (tile_shape 1: 64-wide
+    level-1 rows, one per warp; 2: 32-wide, two rows per warp).
 
     Odd n_steps (the last step runs alone), snapshots every 5 steps (both
     parities of the fused pair), pushes, damping and viscosity.
@@ -100,6 +103,7 @@ def test_two_steps_per_pass_matches_one(cuda, shape, kahan):
     p, opts = _problem(shape, seed=11 + sum(shape), n_steps=25)
     opts = dict(opts, kahan=kahan)
     import shearwave_b200 as sw
+    from shearwave_b200 import tune
 
     def run(spp):
         return sw.shear_fdtd(p["bx"], p["by"], p["bz"], p["rho"], p["mu"], p["dX"], p["dY"],
@@ -107,7 +111,8 @@ def test_two_steps_per_pass_matches_one(cuda, shape, kahan):
                              dict(opts, precision="mixed", steps_per_pass=spp),
                              snapshot_stride=5)
 
-    a, b = run(2), run(1)
+    with tune.knobs(tile_shape=tile_shape):
+        a, b = run(2), run(1)
     for x, y in zip(a, b):
         assert np.array_equal(x, y)
 
@@ -179,17 +184,21 @@ def test_unstable_run_is_flagged(cuda, precision):
     assert not info["nonfinite"]
 
 
-def test_two_steps_per_pass_batched(cuda):
+@pytest.mark.parametrize("tile_shape", [0, 1, 2])
+def test_two_steps_per_pass_batched(cuda, tile_shape):
     """A batch run with two steps per pass (solves of different lengths, so
     one-step launches fill the odd ends) equals each solve run alone with one
-    step per launch, bit for bit."""
+    step per launch, bit for bit, whichever tile shape the launches use."""
     import shearwave_b200 as sw
+    from shearwave_b200 import tune
 
     probs = []
-    for k, (shape, n) in enumerate([((30, 20, 90), 16), ((17, 13, 11), 9), ((40, 9, 133), 21)]):
+    for k, (shape, n) in enumerate([((30, 20, 90), 16), ((17, 13, 11), 9), ((40, 9, 133), 21),
+                                    ((9, 71, 37), 12)]):
         p, opts = _problem(shape, seed=40 + k, n_steps=n)
         probs.append(dict(p, opts=dict(opts, precision="mixed", steps_per_pass=2)))
-    batch = sw.shear_fdtd_batch(probs)
+    with tune.knobs(tile_shape=tile_shape):
+        batch = sw.shear_fdtd_batch(probs)
     for p, got in zip(probs, batch):
         alone = sw.shear_fdtd(p["bx"], p["by"], p["bz"], p["rho"], p["mu"], p["dX"], p["dY"],
                               p["dZ"], p["dT"], p["n_steps"], dict(p["opts"], steps_per_pass=1))

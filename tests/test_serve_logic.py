@@ -244,3 +244,21 @@ def test_device_failure_fails_that_request_only(engine):
     st = srv.stats()
     assert st["failed"] == 1 and st["completed"] == 5
     assert not eng.live  # every request's memory was released
+
+
+def test_admission_error_fails_that_request_only():
+    """An unexpected error while admitting a request (a device call failing)
+    fails that request; it never leaves its future unresolved."""
+
+    class Broken(FakeEngine):
+        def admit(self, p):
+            if p["id"] == 1:
+                raise RuntimeError("sw_fdtd_materials failed")
+            return super().admit(p)
+
+    with ShearServer(Broken(), hbm_budget=100, chunk_steps=4) as srv:
+        futs = [srv.submit(_req(i)) for i in range(3)]
+        with pytest.raises(RuntimeError, match="sw_fdtd_materials"):
+            futs[1].result(timeout=10)
+        assert futs[0].result(timeout=10) == ("result", 0)
+        assert futs[2].result(timeout=10) == ("result", 2)

@@ -337,24 +337,40 @@ def run_reference(a, rank, world):
 # ---------------------------------------------------------------------------
 # serving: config-4 request stream through the continuous-batching server
 # ---------------------------------------------------------------------------
+def c4_requests(n_requests: int, seed: int = 0, pool: int = 0):
+    """The config-4 request list: n seeded requests, or, with ``pool`` > 0,
+    ``pool`` distinct seeded requests drawn in a seeded order for n arrivals
+    (a long stream whose inputs would not fit in host memory, or could not be
+    generated between arrivals)."""
+    from shearwave_b200 import workloads as W
+
+    rng = np.random.default_rng(1234 + seed)
+    if pool <= 0 or pool >= n_requests:
+        return [W.problem_c4(rng) for _ in range(n_requests)]
+    distinct = [W.problem_c4(rng) for _ in range(pool)]
+    order = np.random.default_rng(99 + seed).integers(0, pool, size=n_requests)
+    return [distinct[int(k)] for k in order]
+
+
 def serving_run(n_requests: int, rate_hz: float, seed: int = 0, probs=None,
-                n_fp64: int = 2) -> dict:
+                n_fp64: int = 2, pool: int = 0) -> dict:
     """Poisson arrivals of config-4 requests (log-uniform 64^3..256^3 cubes,
     1 or 4 pushes, nT 500..4000, inclusion media, HBM budget 150 GB)."""
     from shearwave_b200 import workloads as W
     from shearwave_b200.serve import ShearServer, poisson_arrivals, run_stream
 
     if probs is None:
-        rng = np.random.default_rng(1234 + seed)
-        probs = [W.problem_c4(rng) for _ in range(n_requests)]
+        probs = c4_requests(n_requests, seed, pool)
     arrivals = poisson_arrivals(rate_hz, n_requests, seed=seed)
     with ShearServer(hbm_budget=150e9, chunk_steps=50) as srv:
-        run_stream(srv, probs, arrivals)
+        failed = run_stream(srv, probs, arrivals, keep=False)
     st = srv.stats()
     out = {"requests": n_requests, "rate_hz": rate_hz,
            "latency_s": st["latency_s"], "queue_s": st["queue_s"],
-           "gcell_steps_per_s": st["gcell_steps_per_s"], "failed": st.get("failed", 0),
+           "gcell_steps_per_s": st["gcell_steps_per_s"], "failed": int(failed),
+           "wall_s": st["wall_s"],
            "cell_steps": int(sum(W.cell_steps(p) for p in probs)),
+           "distinct_requests": len({id(p) for p in probs}),
            "workload": "config-4 requests (log-uniform 64^3..256^3, 1 or 4 pushes, "
                        "nT 500..4000), Poisson arrivals, budget 150 GB, mixed form"}
     if n_fp64 > 0:
@@ -362,7 +378,7 @@ def serving_run(n_requests: int, rate_hz: float, seed: int = 0, probs=None,
     return out
 
 
-def serving_sweep(rates, n_requests: int, n_fp64: int, seed: int = 0) -> dict:
+def serving_sweep(rates, n_requests: int, n_fp64: int, seed: int = 0, pool: int = 0) -> dict:
     """The config-4 stream at several arrival rates (the same seeded requests
     at every rate), and the first ``n_fp64`` requests solved one at a time in
     plain FP64 (device-resident inputs, CUDA events) as the comparison."""
@@ -370,12 +386,13 @@ def serving_sweep(rates, n_requests: int, n_fp64: int, seed: int = 0) -> dict:
 
     from shearwave_b200 import workloads as W
 
-    rng = np.random.default_rng(1234 + seed)
-    probs = [W.problem_c4(rng) for _ in range(n_requests)]
+    probs = c4_requests(n_requests, seed, pool)
     runs = [serving_run(n_requests, r, seed, probs, n_fp64=0) for r in rates]
-    out = {"rates": [{k: r[k] for k in ("rate_hz", "latency_s", "queue_s", "gcell_steps_per_s")}
+    out = {"rates": [{k: r[k] for k in ("rate_hz", "latency_s", "queue_s", "gcell_steps_per_s",
+                                        "wall_s", "failed")}
                      for r in runs],
-           "requests": n_requests, "workload": runs[0]["workload"]}
+           "requests": n_requests, "distinct_requests": runs[0]["distinct_requests"],
+           "workload": runs[0]["workload"]}
     if n_fp64 > 0:
         out["fp64_one_at_a_time"] = _fp64_one_at_a_time(probs[:n_fp64])
     return out
@@ -515,6 +532,9 @@ def main(argv=None) -> int:
                     help="requests of the config-4 serving stream run after the timing (0: skip)")
     ap.add_argument("--serve-rate", type=float, default=4.0,
                     help="mean Poisson arrival rate of the serving stream (requests/s)")
+    ap.add_argument("--serve-pool", type=int, default=0,
+                    help="distinct seeded requests the serving stream draws from (0: every "
+                         "request distinct)")
     ap.add_argument("--serve-sweep", default=None,
                     help="comma-separated arrival rates (requests/s): run the serving stream "
                          "at each rate instead of --serve-rate, plus plain-FP64 one-at-a-time "
@@ -731,9 +751,11 @@ def main(argv=None) -> int:
     if rank == 0 and world == 1 and a.serve_requests > 0:
         if a.serve_sweep:
             rates = [float(r) for r in a.serve_sweep.split(",")]
-            line["serving_sweep"] = serving_sweep(rates, a.serve_requests, 6, seed=rank)
+            line["serving_sweep"] = serving_sweep(rates, a.serve_requests, 6, seed=rank,
+                                                  pool=a.serve_pool)
         else:
-            line["serving"] = serving_run(a.serve_requests, a.serve_rate, seed=rank)
+            line["serving"] = serving_run(a.serve_requests, a.serve_rate, seed=rank,
+                                          pool=a.serve_pool)
 
     if rank == 0 and world == 1 and not a.no_cpu:
         line["cpu_baseline"] = cpu_baseline(probs)

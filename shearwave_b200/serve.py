@@ -399,9 +399,35 @@ def poisson_arrivals(rate_hz: float, n: int, seed: int = 0) -> np.ndarray:
     return np.cumsum(rng.exponential(1.0 / rate_hz, size=n))
 
 
-def run_stream(server: ShearServer, problems, arrivals_s, timeout_s=None):
-    """Submit ``problems`` at ``arrivals_s`` (seconds from now) and wait for all."""
+def run_stream(server: ShearServer, problems, arrivals_s, timeout_s=None, keep=True):
+    """Submit ``problems`` at ``arrivals_s`` (seconds from now) and wait for all.
+
+    Returns the results in submission order (None for a cancelled request).
+    With ``keep=False`` nothing holds on to a result once its request has
+    finished (a long stream's outputs would not fit in host memory), and the
+    return value is the number of requests that failed.
+    """
     t0 = time.perf_counter()
+    if not keep:
+        left = threading.Semaphore(0)
+        failed = [0]
+
+        def done(f):
+            if f.cancelled() or f.exception() is not None:
+                failed[0] += 1
+            left.release()
+
+        n = 0
+        for p, ta in zip(problems, arrivals_s):
+            dt = ta - (time.perf_counter() - t0)
+            if dt > 0:
+                time.sleep(dt)
+            server.submit(p).add_done_callback(done)
+            n += 1
+        for _ in range(n):
+            if not left.acquire(timeout=timeout_s):
+                raise TimeoutError("request stream did not finish in time")
+        return failed[0]
     futs = []
     for p, ta in zip(problems, arrivals_s):
         dt = ta - (time.perf_counter() - t0)

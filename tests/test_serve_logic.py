@@ -262,3 +262,21 @@ def test_admission_error_fails_that_request_only():
             futs[1].result(timeout=10)
         assert futs[0].result(timeout=10) == ("result", 0)
         assert futs[2].result(timeout=10) == ("result", 2)
+
+
+@pytest.mark.parametrize("engine", ENGINES)
+def test_stream_without_results_counts_failures(engine):
+    """A long stream that keeps no results reports how many requests failed
+    and completes the rest."""
+    from shearwave_b200.serve import poisson_arrivals, run_stream
+
+    kinds = [dict(n_steps=4), dict(n_steps=7), dict(n_steps=3, bad=True)]
+    problems = [_req(i, **kinds[i % 3]) for i in range(30)]
+    arrivals = poisson_arrivals(2000.0, len(problems), seed=3)
+    eng = engine()
+    with ShearServer(eng, hbm_budget=100, chunk_steps=3) as srv:
+        failed = run_stream(srv, problems, arrivals, timeout_s=10, keep=False)
+    assert failed == 10
+    st = srv.stats()
+    assert st["completed"] == 20 and st["failed"] == 10
+    assert not eng.live

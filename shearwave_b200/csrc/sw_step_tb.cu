@@ -27,7 +27,7 @@
 // below), and level 1 reuses a slot once every warp has read it, so warps
 // drift up to a plane apart instead of meeting at a barrier; every wait is
 // bounded and an abort stops each warp on its own.  Level-1 cells outside
-// the grid interior are the zero shell.  Both levels use lap7f, so
+// the grid interior are the zero shell.  Both levels use lap7_pair, so
 // two steps here equal two one-step launches bit for bit.  A pass reads
 // buffer t mod 3 and writes buffer (t+2) mod 3.
 //
@@ -99,27 +99,23 @@ template <bool VISC, bool DAMP, bool PUSH, bool SNAP, int RS, int CS>
 __device__ __forceinline__ void tb_pair_step(const float* __restrict__ P,
                                              const float* __restrict__ Pn, int o, float2 M,
                                              float2 E, float2 (&pu)[3], float2 (&pd)[3],
-                                             bool act_a, bool act_b, float hx, float hy, float hz,
-                                             float hc, float damp,
-                                             const TmaF32TB* __restrict__ in, int j0, int j1,
-                                             unsigned nc, long long i, float* __restrict__ out,
-                                             unsigned ocs, float* __restrict__ snap) {
+                                             bool act_a, bool act_b, const Lap7Pair& lk,
+                                             float damp, const TmaF32TB* __restrict__ in, int j0,
+                                             int j1, unsigned nc, long long i,
+                                             float* __restrict__ out, unsigned ocs,
+                                             float* __restrict__ snap) {
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
     const int oc = o + c * CS, od = oc + 3 * CS;
     const float2 C = tb_ld2(P + oc), L = tb_ld2(P + oc - 2), R = tb_ld2(P + oc + 2);
     const float2 N = tb_ld2(P + oc + RS), S = tb_ld2(P + oc - RS), X = tb_ld2(Pn + oc);
-    const float lua = lap7f(X.x + pu[c].x, N.x + S.x, C.y + L.y, C.x, hx, hy, hz, hc);
-    const float lub = lap7f(X.y + pu[c].y, N.y + S.y, R.x + C.x, C.y, hx, hy, hz, hc);
+    const float2 lu = lap7_pair(C, L, R, X, pu[c], N, S, lk);
     const float2 Cd = tb_ld2(P + od);
-    float inca = Cd.x + M.x * lua, incb = Cd.y + M.y * lub;
+    float2 inc = ffma2(M, lu, Cd);
     if (VISC) {
       const float2 Ld = tb_ld2(P + od - 2), Rd = tb_ld2(P + od + 2);
       const float2 Nd = tb_ld2(P + od + RS), Sd = tb_ld2(P + od - RS), Xd = tb_ld2(Pn + od);
-      const float lda = lap7f(Xd.x + pd[c].x, Nd.x + Sd.x, Cd.y + Ld.y, Cd.x, hx, hy, hz, hc);
-      const float ldb = lap7f(Xd.y + pd[c].y, Nd.y + Sd.y, Rd.x + Cd.x, Cd.y, hx, hy, hz, hc);
-      inca += E.x * lda;
-      incb += E.y * ldb;
+      inc = ffma2(E, lap7_pair(Cd, Ld, Rd, Xd, pd[c], Nd, Sd, lk), inc);
       pd[c] = Cd;
     }
     pu[c] = C;
@@ -127,21 +123,16 @@ __device__ __forceinline__ void tb_pair_step(const float* __restrict__ P,
       for (int j = j0; j < j1; ++j) {
         const float2 Pt = __ldg(reinterpret_cast<const float2*>(
             in->pat + ((long long)in->term_pat[j] * 3 + c) * nc + i));
-        const float sc = (float)in->term_scale[j];
-        inca += Pt.x * sc;
-        incb += Pt.y * sc;
+        inc = ffma2(Pt, splat2((float)in->term_scale[j]), inc);
       }
     }
-    if (DAMP) {
-      inca *= damp;
-      incb *= damp;
-    }
-    const float ua = C.x + inca, ub = C.y + incb;
-    tb_st2(out + (size_t)c * ocs, act_a ? ua : 0.f, act_b ? ub : 0.f);
-    tb_st2(out + (size_t)(3 + c) * ocs, act_a ? inca : 0.f, act_b ? incb : 0.f);
+    if (DAMP) inc = fmul2(inc, splat2(damp));
+    const float2 un = fadd2(C, inc);
+    tb_st2(out + (size_t)c * ocs, act_a ? un.x : 0.f, act_b ? un.y : 0.f);
+    tb_st2(out + (size_t)(3 + c) * ocs, act_a ? inc.x : 0.f, act_b ? inc.y : 0.f);
     if (SNAP && snap != nullptr) {
-      if (act_a) snap[c] = ua;
-      if (act_b) snap[3 + c] = ub;
+      if (act_a) snap[c] = un.x;
+      if (act_b) snap[3 + c] = un.y;
     }
   }
 }
@@ -183,7 +174,8 @@ __device__ __forceinline__ TbPos tb_tile(const TmaF32TB* __restrict__ in, int lo
   float* __restrict__ D = in->state[(lit + 2) % 3];
   const unsigned nc = (unsigned)g.ncell;  // the host keeps ncell below 2^32
   const float damp = in->damp;
-  const float hx = in->hx, hy = in->hy, hz = in->hz, hc = lap7_centre_coef(hx, hy, hz);
+  const Lap7Pair lk =
+      lap7_pair_coefs(in->hx, in->hy, in->hz, lap7_centre_coef(in->hx, in->hy, in->hz));
   // this thread: level-1 row r (y = y0-1+r), z pair zp, zp+1 (zp = z0-2+2 pl):
   // a warp owns one row of 32 pairs (LZ 64) or two rows of 16 (LZ 32)
   const int r = S::RPW == 1 ? w : 2 * w + (lane >> 4);
@@ -276,8 +268,8 @@ __device__ __forceinline__ TbPos tb_tile(const TmaF32TB* __restrict__ in, int lo
       if (SNAP && snap1 && store && q >= tc.x0 && q < tc.x1)
         sp = in->snaps + ((((long long)slot1 * g.nx + q) * g.ny + y) * g.nz + zp) * 3;
       tb_pair_step<VISC, DAMP, PUSH, SNAP, W, H * W>(
-          k.ringA + cur.s * AF, k.ringA + nxt.s * AF, o, Mc, Ec, pu, pd, aa, ab, hx, hy, hz, hc,
-          damp, in, jl0, jl1, nc, i, Lw + ol, (unsigned)LP, sp);
+          k.ringA + cur.s * AF, k.ringA + nxt.s * AF, o, Mc, Ec, pu, pd, aa, ab, lk, damp, in,
+          jl0, jl1, nc, i, Lw + ol, (unsigned)LP, sp);
     }
     __syncwarp();
     if (lane == 0) {
@@ -307,8 +299,8 @@ __device__ __forceinline__ TbPos tb_tile(const TmaF32TB* __restrict__ in, int lo
           if (SNAP && snap2)
             sp = in->snaps + ((((long long)slot2 * g.nx + x) * g.ny + y) * g.nz + zp) * 3;
           tb_pair_step<VISC, DAMP, PUSH, SNAP, LZ, LP>(Lc, Lw, ol, Mp, Ep, qu, qd, zin_a, zin_b,
-                                                       hx, hy, hz, hc, damp, in, j11, j21, nc, i,
-                                                       D + i, nc, sp);
+                                                       lk, damp, in, j11, j21, nc, i, D + i, nc,
+                                                       sp);
         }
       }
       __syncwarp();

@@ -108,7 +108,7 @@ template <bool VISC, bool KAHAN, bool DAMP, bool PUSH, int HW>
 __device__ __forceinline__ void f32_pair_plane(
     const float* __restrict__ Pc, const float* __restrict__ Pn, const float* __restrict__ Bc,
     const float* __restrict__ Bm, int o, int ob, int W, float2 (&pu)[3], float2 (&pd)[3],
-    bool act_a, bool act_b, float hx, float hy, float hz, float hc, float damp,
+    bool act_a, bool act_b, const Lap7Pair& lk, float damp,
     const TmaF32* __restrict__ in, int j0, int j1, unsigned nc, long long i,
     float* __restrict__ Di, float2 (&un)[3]) {
   // HW: halo-box cells per component; a point box holds PT cells per component
@@ -120,48 +120,36 @@ __device__ __forceinline__ void f32_pair_plane(
     const int oc = o + c * HW, od = oc + 3 * HW;
     const float2 C = lds2(Pc + oc), L = lds2(Pc + oc - 2), R = lds2(Pc + oc + 2);
     const float2 N = lds2(Pc + oc + W), S = lds2(Pc + oc - W), X = lds2(Pn + oc);
-    const float lua = lap7f(X.x + pu[c].x, N.x + S.x, C.y + L.y, C.x, hx, hy, hz, hc);
-    const float lub = lap7f(X.y + pu[c].y, N.y + S.y, R.x + C.x, C.y, hx, hy, hz, hc);
+    const float2 lu = lap7_pair(C, L, R, X, pu[c], N, S, lk);
     const float2 Cd = lds2(Pc + od);
-    float inca = Cd.x + M.x * lua, incb = Cd.y + M.y * lub;
+    float2 inc = ffma2(M, lu, Cd);
     if (VISC) {
       const float2 Ld = lds2(Pc + od - 2), Rd = lds2(Pc + od + 2);
       const float2 Nd = lds2(Pc + od + W), Sd = lds2(Pc + od - W), Xd = lds2(Pn + od);
-      const float lda = lap7f(Xd.x + pd[c].x, Nd.x + Sd.x, Cd.y + Ld.y, Cd.x, hx, hy, hz, hc);
-      const float ldb = lap7f(Xd.y + pd[c].y, Nd.y + Sd.y, Rd.x + Cd.x, Cd.y, hx, hy, hz, hc);
-      inca += E.x * lda;
-      incb += E.y * ldb;
+      inc = ffma2(E, lap7_pair(Cd, Ld, Rd, Xd, pd[c], Nd, Sd, lk), inc);
       pd[c] = Cd;
     }
     pu[c] = C;
     if (PUSH) {
       for (int j = j0; j < j1; ++j) {
         const float2 P = ldg2(in->pat + ((long long)in->term_pat[j] * 3 + c) * nc + i);
-        const float sc = (float)in->term_scale[j];
-        inca += P.x * sc;
-        incb += P.y * sc;
+        inc = ffma2(P, splat2((float)in->term_scale[j]), inc);
       }
     }
-    if (DAMP) {
-      inca *= damp;
-      incb *= damp;
-    }
-    float ua, ub;
+    if (DAMP) inc = fmul2(inc, splat2(damp));
+    float2 un2;
     if (KAHAN) {
       const float2 K = lds2(Bc + c * PT + ob);
-      const float ya = inca - K.x, yb = incb - K.y;
-      ua = C.x + ya;
-      ub = C.y + yb;
-      stg2(Di + (size_t)(6 + c) * nc, act_a ? (ua - C.x) - ya : 0.f,
-           act_b ? (ub - C.y) - yb : 0.f);
+      const float2 yk = fsub2(inc, K);
+      un2 = fadd2(C, yk);
+      const float2 cn = fsub2(fsub2(un2, C), yk);
+      stg2(Di + (size_t)(6 + c) * nc, act_a ? cn.x : 0.f, act_b ? cn.y : 0.f);
     } else {
-      ua = C.x + inca;  // the compensation planes are neither read nor written
-      ub = C.y + incb;
+      un2 = fadd2(C, inc);  // the compensation planes are neither read nor written
     }
-    ua = act_a ? ua : 0.f;
-    ub = act_b ? ub : 0.f;
+    const float ua = act_a ? un2.x : 0.f, ub = act_b ? un2.y : 0.f;
     stg2(Di + (size_t)c * nc, ua, ub);
-    stg2(Di + (size_t)(3 + c) * nc, act_a ? inca : 0.f, act_b ? incb : 0.f);
+    stg2(Di + (size_t)(3 + c) * nc, act_a ? inc.x : 0.f, act_b ? inc.y : 0.f);
     un[c] = make_float2(ua, ub);
   }
 }
@@ -230,7 +218,8 @@ __device__ __forceinline__ bool f32_tile(const TmaF32* __restrict__ in, int loca
   const int slot = snap ? (lit + 1) / in->snap_stride - 1 : 0;
   const unsigned nc = (unsigned)g.ncell;  // the host keeps ncell below 2^32
   const float damp = in->damp;
-  const float hx = in->hx, hy = in->hy, hz = in->hz, hc = lap7_centre_coef(hx, hy, hz);
+  const Lap7Pair lk =
+      lap7_pair_coefs(in->hx, in->hy, in->hz, lap7_centre_coef(in->hx, in->hy, in->hz));
   const int o = (row + 1) * Wb + lz + 4, ob = row * TZW + lz;
   // Plane x-1 enters only through its centre values (x neighbours of the
   // Laplacians), which each thread keeps in registers from the plane it
@@ -262,8 +251,8 @@ __device__ __forceinline__ bool f32_tile(const TmaF32* __restrict__ in, int loca
       const float* Bs = q.stage_b(sb);
       float2 un[3];
       f32_pair_plane<VISC, KAHAN, DAMP, PUSH, HWB>(q.stage_a(s_cur), q.stage_a(s_next), Bs + CF,
-                                                   Bs + MF, o, ob, Wb, pu, pd, act_a, act_b, hx,
-                                                   hy, hz, hc, damp, in, j0, j1, nc, i, D + i, un);
+                                                   Bs + MF, o, ob, Wb, pu, pd, act_a, act_b, lk,
+                                                   damp, in, j0, j1, nc, i, D + i, un);
       if (snap) {
         float* sp = in->snaps + ((((long long)slot * g.nx + x) * g.ny + y) * g.nz + z) * 3;
 #pragma unroll

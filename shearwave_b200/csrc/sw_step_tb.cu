@@ -342,13 +342,37 @@ __device__ __forceinline__ TbPos tb_tile_ps(bool push, bool snap, const TmaF32TB
   return tb_tile<LZ, VISC, DAMP, false, false>(in, local, lit, k, p, w, lane);
 }
 
+// Whether the tile's pair of steps (lit+1, lit+2) adds force terms.
+__device__ __forceinline__ bool tb_pushes(const TmaF32TB* __restrict__ in, int lit) {
+  return in->term_off != nullptr && in->term_off[lit + 2] > in->term_off[lit];
+}
+// Whether the tile's pair of steps writes a snapshot.
+__device__ __forceinline__ bool tb_snaps(const TmaF32TB* __restrict__ in, int lit) {
+  return in->snap_stride > 0 && in->snaps != nullptr &&
+         (((lit + 1) % in->snap_stride) == 0 || ((lit + 2) % in->snap_stride) == 0);
+}
+
+// A tile without force terms or snapshots, every path inlined: the launch
+// variant that runs only such tiles holds no call, so none of its registers
+// go to the stack around one.
+template <int LZ>
+__device__ __forceinline__ TbPos tb_tile_common(const TmaF32TB* __restrict__ in, int local,
+                                                int lit, const TbRings& k, TbPos p, int w,
+                                                int lane) {
+  const bool visc = in->ncoef > 1, damp = in->use_damp != 0;
+  if (visc) {
+    if (damp) return tb_tile<LZ, true, true, false, false>(in, local, lit, k, p, w, lane);
+    return tb_tile<LZ, true, false, false, false>(in, local, lit, k, p, w, lane);
+  }
+  if (damp) return tb_tile<LZ, false, true, false, false>(in, local, lit, k, p, w, lane);
+  return tb_tile<LZ, false, false, false, false>(in, local, lit, k, p, w, lane);
+}
+
 template <int LZ>
 __device__ __forceinline__ TbPos tb_tile_any(const TmaF32TB* __restrict__ in, int local, int lit,
                                              const TbRings& k, TbPos p, int w, int lane) {
   const bool visc = in->ncoef > 1, damp = in->use_damp != 0;
-  const bool push = in->term_off != nullptr && in->term_off[lit + 2] > in->term_off[lit];
-  const bool snap = in->snap_stride > 0 && in->snaps != nullptr &&
-                    (((lit + 1) % in->snap_stride) == 0 || ((lit + 2) % in->snap_stride) == 0);
+  const bool push = tb_pushes(in, lit), snap = tb_snaps(in, lit);
   if (visc) {
     if (damp) return tb_tile_ps<LZ, true, true>(push, snap, in, local, lit, k, p, w, lane);
     return tb_tile_ps<LZ, true, false>(push, snap, in, local, lit, k, p, w, lane);
@@ -357,14 +381,31 @@ __device__ __forceinline__ TbPos tb_tile_any(const TmaF32TB* __restrict__ in, in
   return tb_tile_ps<LZ, false, false>(push, snap, in, local, lit, k, p, w, lane);
 }
 
-template <bool BATCH, int LZ>
+// Launch variants.  Tiles whose pair of steps adds force terms or writes a
+// snapshot need more live values than the others; their code runs in
+// functions of its own, and a kernel that can call those keeps some of the
+// common loop's values on the stack (measured: ~3 local loads per warp and
+// plane, 12 % slower).  So a batched pair of steps is two launches on the
+// same queue: kTbCommon runs every other tile with all paths inlined and
+// raises queues[3] when it skipped one; kTbRare then runs only the skipped
+// tiles, and returns at once when the flag is down (every launch of a run
+// without pushes or snapshots).  kTbAll runs every tile (the single-solve
+// kernel).
+constexpr int kTbAll = 0, kTbCommon = 1, kTbRare = 2;
+
+template <bool BATCH, int LZ, int MODE>
 __global__ void __launch_bounds__(TmaF32TB::THREADS, 1)
     step_f32_fused2(const __grid_constant__ TmaF32TB one, const TmaF32TB* __restrict__ tab,
                     int ninst, int ntiles, int it, const int* __restrict__ it_dev, int* queues) {
   using S = TbShape<LZ>;
-  if (it_dev != nullptr) it += *it_dev;  // step counter kept on the device (graph replays)
+  static_assert(MODE == kTbAll || BATCH, "split launches need the batch table's flag word");
   // batched launches take tiles from a launch-wide queue (see step_f32_tma)
   int* queue = queues;
+  if (MODE == kTbRare && *reinterpret_cast<volatile int*>(queue + 3) == 0) {
+    queue_cta_done(queue, true);  // no tile was deferred to this launch
+    return;
+  }
+  if (it_dev != nullptr) it += *it_dev;  // step counter kept on the device (graph replays)
   using T = TmaF32TB;
   constexpr int NA = T::NA, NB = T::NB, NL = T::NL, WB = S::WB, HB = S::HB;
   constexpr uint32_t A_BYTES = S::W * S::H * 6 * 4;
@@ -384,7 +425,7 @@ __global__ void __launch_bounds__(TmaF32TB::THREADS, 1)
     if (threadIdx.x == 0)
       for (int k = 0; k < (BATCH ? ninst : 1); ++k)
         if (int* fl = flags_of(k)) atomicOr(fl, kFlagRefused);
-    queue_cta_done(queue);
+    queue_cta_done(queue, MODE == kTbRare);
     return;
   }
   AbortLog* lg = abort_log(base);
@@ -417,6 +458,7 @@ __global__ void __launch_bounds__(TmaF32TB::THREADS, 1)
       RingPos<NB> pb;
       int stride_next = blockIdx.x;
       bool ok = true;
+      bool deferred = false;  // this CTA raised the deferred-tile flag
       while (ok && !*abort_flag) {
         const int t = next_tile(queue, stride_next);
         if (t >= ntiles) {  // end of this CTA's work: arm one stage without a copy
@@ -431,6 +473,15 @@ __global__ void __launch_bounds__(TmaF32TB::THREADS, 1)
         const int local = BATCH ? t - in->tile_base : t;
         const int lit = it - in->it_begin;
         if (lit < 0 || lit + 1 >= in->n_steps || solve_abandoned(in->flags)) continue;
+        if (MODE != kTbAll) {
+          const bool rare = tb_pushes(in, lit) || tb_snaps(in, lit);
+          if (MODE == kTbCommon && rare) {
+            if (!deferred) atomicExch(queue + 3, 1);  // kTbRare runs it
+            deferred = true;
+            continue;
+          }
+          if (MODE == kTbRare && !rare) continue;  // kTbCommon ran it
+        }
         lg->solve[lg->n_taken & 7] = k;
         ++lg->n_taken;
         const Geom& g = in->g;
@@ -489,7 +540,8 @@ __global__ void __launch_bounds__(TmaF32TB::THREADS, 1)
       const T* in = BATCH ? &tab[solve_slots(base)[p.ca.s]] : &one;
       const int local = BATCH ? t - in->tile_base : t;
       const int lit = it - in->it_begin;
-      p = tb_tile_any<LZ>(in, local, lit, k, p, warp, lane);
+      p = MODE == kTbCommon ? tb_tile_common<LZ>(in, local, lit, k, p, warp, lane)
+                            : tb_tile_any<LZ>(in, local, lit, k, p, warp, lane);
       if (!p.ok) break;
       if (lane == 0) ++lg->done[warp];
     }
@@ -501,7 +553,7 @@ __global__ void __launch_bounds__(TmaF32TB::THREADS, 1)
     drain_ring(hd->fullB, lg->armedB, lg->parB, NB);
     flag_unfinished(lg, T::CONSUMER_WARPS, BATCH ? ninst : 1, kFlagTimeout, flags_of);
   }
-  queue_cta_done(queue);
+  queue_cta_done(queue, MODE == kTbRare);
 }
 
 }  // namespace
@@ -520,10 +572,12 @@ static int tb_set_attr() {
   static bool done = false;
   if (done) return SW_OK;
   const int bytes = (int)tb_smem_bytes();
-  const void* fns[4] = {(const void*)step_f32_fused2<false, 64>,
-                        (const void*)step_f32_fused2<true, 64>,
-                        (const void*)step_f32_fused2<false, 32>,
-                        (const void*)step_f32_fused2<true, 32>};
+  const void* fns[6] = {(const void*)step_f32_fused2<false, 64, kTbAll>,
+                        (const void*)step_f32_fused2<true, 64, kTbCommon>,
+                        (const void*)step_f32_fused2<true, 64, kTbRare>,
+                        (const void*)step_f32_fused2<false, 32, kTbAll>,
+                        (const void*)step_f32_fused2<true, 32, kTbCommon>,
+                        (const void*)step_f32_fused2<true, 32, kTbRare>};
   for (const void* f : fns) {
     cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(fused step smem)");
@@ -636,13 +690,16 @@ int make_tma_f32_tb(const StepArgs& a, int xchunk, TmaF32TB* t, int lz) {
 int launch_fused2_prepare() { return tb_set_attr(); }
 
 const void* step_f32_fused2_ptr(int lz) {
-  return lz == 32 ? reinterpret_cast<const void*>(step_f32_fused2<false, 32>)
-                  : reinterpret_cast<const void*>(step_f32_fused2<false, 64>);
+  return lz == 32 ? reinterpret_cast<const void*>(step_f32_fused2<false, 32, kTbAll>)
+                  : reinterpret_cast<const void*>(step_f32_fused2<false, 64, kTbAll>);
 }
 
-const void* step_f32_fused2_batch_ptr(int lz) {
-  return lz == 32 ? reinterpret_cast<const void*>(step_f32_fused2<true, 32>)
-                  : reinterpret_cast<const void*>(step_f32_fused2<true, 64>);
+const void* step_f32_fused2_batch_ptr(int lz, bool rare) {
+  if (rare)
+    return lz == 32 ? reinterpret_cast<const void*>(step_f32_fused2<true, 32, kTbRare>)
+                    : reinterpret_cast<const void*>(step_f32_fused2<true, 64, kTbRare>);
+  return lz == 32 ? reinterpret_cast<const void*>(step_f32_fused2<true, 32, kTbCommon>)
+                  : reinterpret_cast<const void*>(step_f32_fused2<true, 64, kTbCommon>);
 }
 
 static void launch_tb(const void* fn, int grid, cudaStream_t s, const TmaF32TB& one,
@@ -678,9 +735,10 @@ int launch_fused2_batch(const void* d_tab, int ninst, int ntiles, int it, int* q
   if (rc != SW_OK) return rc;
   if (ntiles == 0) return SW_OK;
   TmaF32TB dummy{};
-  launch_tb(step_f32_fused2_batch_ptr(lz), std::min(ntiles, kNumSMs), s, dummy,
-            (const TmaF32TB*)d_tab, ninst, ntiles, it, queues);
-  count_launches(1);
+  for (bool rare : {false, true})
+    launch_tb(step_f32_fused2_batch_ptr(lz, rare), std::min(ntiles, kNumSMs), s, dummy,
+              (const TmaF32TB*)d_tab, ninst, ntiles, it, queues);
+  count_launches(2, 2);
   SW_CHECK_LAUNCH("fused two-step kernel (batch)");
   return SW_OK;
 }

@@ -107,6 +107,29 @@ def test_long_batch_replays_graphs_bitwise(cuda, precision):
             assert np.array_equal(a, b)
 
 
+def test_pushes_and_snapshots_inside_replayed_runs_bitwise(cuda):
+    """Pairs of steps with force terms or snapshots run in the second launch
+    of each two-step pair (the first one defers them); here they fall inside
+    graph-replayed runs (a push from step 100, snapshots every 6 steps on one
+    solve, none on the others), and every solve still matches its lone run
+    bit for bit."""
+    import shearwave_b200 as sw
+    from shearwave_b200 import workloads as W
+
+    probs = [W.problem_inclusions(sh, 300, seed=60 + i, tol=1e-9)
+             for i, sh in enumerate([(22, 20, 30), (18, 26, 24), (30, 16, 20)])]
+    env = np.zeros(300, np.float32)
+    env[100:104] = np.linspace(1.0, 0.25, 4)
+    probs[0]["opts"]["force_terms"] = [((None, None, 0.5 * probs[0]["bz"][::-1]), env)]
+    probs[1]["snapshot_stride"] = 6
+    got = sw.shear_fdtd_batch(probs, precision="mixed")
+    for p, res in zip(probs, got):
+        ref = _alone(p, "mixed")
+        assert len(res) == len(ref)
+        for a, b in zip(res, ref):
+            assert np.array_equal(a, b)
+
+
 @pytest.mark.parametrize("precision", ["mixed", "fp64"])
 def test_4d_force_streamed_from_the_device(cuda, precision):
     """4-D forces: the non-zero slices are projected up front (batched CG)

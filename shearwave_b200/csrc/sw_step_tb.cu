@@ -86,6 +86,27 @@ __device__ __forceinline__ void tb_st2(float* p, float a, float b) {
   *reinterpret_cast<float2*>(p) = make_float2(a, b);
 }
 
+// The force terms of a push tile's two steps, written by the producer when
+// it takes the tile and read by the consumers: each term's pattern (its
+// component 0) and scale, for step lit (level 1) and lit+1 (level 2).  Two
+// buffers, by the parity of the tile's ordinal in the CTA: the producer
+// fills the one of tile n+2 only after every consumer warp has released a
+// plane of tile n+1 (a tile spans at least NA planes), so no warp still
+// reads it.  A pair of steps with more than kTbTermCap terms at one step
+// runs in one-step launches instead (the solver keeps such solves out of
+// this kernel; the producer refuses the tile if one gets here).
+constexpr int kTbTermCap = 32;
+struct TbTermRef {
+  const float* base;
+  float scale;
+  int pad;
+};
+struct TbTermBuf {
+  int n[2];
+  int pad[2];
+  TbTermRef t[2][kTbTermCap];
+};
+
 // One level of the two-step pass for one thread's z pair: the step from the
 // plane whose centre pair is at `P + o` (row stride `RS`, component stride
 // `CS`), with the plane after it at `Pn` and the centre values of the plane
@@ -100,8 +121,8 @@ __device__ __forceinline__ void tb_pair_step(const float* __restrict__ P,
                                              const float* __restrict__ Pn, int o, float2 M,
                                              float2 E, float2 (&pu)[3], float2 (&pd)[3],
                                              bool act_a, bool act_b, const Lap7Pair& lk,
-                                             float damp, const TmaF32TB* __restrict__ in, int j0,
-                                             int j1, unsigned nc, long long i,
+                                             float damp, const TbTermRef* __restrict__ terms,
+                                             int nterms, unsigned nc, long long i,
                                              float* __restrict__ out, unsigned ocs,
                                              float* __restrict__ snap) {
 #pragma unroll
@@ -120,10 +141,11 @@ __device__ __forceinline__ void tb_pair_step(const float* __restrict__ P,
     }
     pu[c] = C;
     if (PUSH) {
-      for (int j = j0; j < j1; ++j) {
-        const float2 Pt = __ldg(reinterpret_cast<const float2*>(
-            in->pat + ((long long)in->term_pat[j] * 3 + c) * nc + i));
-        inc = ffma2(Pt, splat2((float)in->term_scale[j]), inc);
+      for (int j = 0; j < nterms; ++j) {
+        const TbTermRef r = terms[j];
+        const float2 Pt =
+            __ldg(reinterpret_cast<const float2*>(r.base + (long long)c * nc + i));
+        inc = ffma2(Pt, splat2(r.scale), inc);
       }
     }
     if (DAMP) inc = fmul2(inc, splat2(damp));
@@ -146,6 +168,7 @@ struct TbRings {
   uint64_t* Lfull;
   uint64_t* Lempty;
   volatile int* abort_flag;
+  const TbTermBuf* terms;  // the two term buffers
 };
 
 // A consumer warp's next stage of each ring (level-0 planes, point-wise
@@ -154,6 +177,7 @@ struct TbPos {
   RingPos<TmaF32TB::NA> ca;
   RingPos<TmaF32TB::NB> cb;
   RingPos<TmaF32TB::NL> lw;
+  int ord = 0;  // tiles this warp has finished (picks the term buffer)
   bool ok = true;
 };
 
@@ -190,9 +214,10 @@ __device__ __forceinline__ TbPos tb_tile(const TmaF32TB* __restrict__ in, int lo
   const bool out_rc = r >= 1 && r <= S::OY && pl >= 1 && pl <= S::PAIRS - 2;
   const bool store = out_rc && yin && zp < g.pz;  // pz is even: the pair is in the row
   const int o = (r + 1) * W + 2 + 2 * pl, ob = r * WB + 2 + 2 * pl, ol = r * LZ + 2 * pl;
-  const int j10 = PUSH ? in->term_off[lit] : 0;
-  const int j11 = PUSH ? in->term_off[lit + 1] : 0;
-  const int j21 = PUSH ? in->term_off[lit + 2] : 0;
+  // the force terms of steps lit (level 1) and lit+1 (level 2)
+  const TbTermBuf& tbuf = k.terms[p.ord & 1];
+  const int n1 = PUSH ? tbuf.n[0] : 0;
+  const int n2 = PUSH ? tbuf.n[1] : 0;
   const bool snap1 = SNAP && ((lit + 1) % in->snap_stride) == 0;
   const bool snap2 = SNAP && ((lit + 2) % in->snap_stride) == 0;
   const int slot1 = snap1 ? (lit + 1) / in->snap_stride - 1 : 0;
@@ -257,19 +282,18 @@ __device__ __forceinline__ TbPos tb_tile(const TmaF32TB* __restrict__ in, int lo
     } else {
       const bool aa = xin && yin && zin_a, ab = xin && yin && zin_b;
       long long i = 0;  // the pair's cell, for the force patterns
-      int jl0 = 0, jl1 = 0;
+      int nl = 0;
       if (PUSH) {
         i = (long long)min(max(q, 0), g.nx - 1) * g.sxy +
             (long long)min(max(y, 0), g.ny - 1) * g.pz + max(zp, 0);
-        jl0 = (aa || ab) ? j10 : 0;
-        jl1 = (aa || ab) ? j11 : 0;
+        nl = (aa || ab) ? n1 : 0;
       }
       float* sp = nullptr;
       if (SNAP && snap1 && store && q >= tc.x0 && q < tc.x1)
         sp = in->snaps + ((((long long)slot1 * g.nx + q) * g.ny + y) * g.nz + zp) * 3;
       tb_pair_step<VISC, DAMP, PUSH, SNAP, W, H * W>(
-          k.ringA + cur.s * AF, k.ringA + nxt.s * AF, o, Mc, Ec, pu, pd, aa, ab, lk, damp, in,
-          jl0, jl1, nc, i, Lw + ol, (unsigned)LP, sp);
+          k.ringA + cur.s * AF, k.ringA + nxt.s * AF, o, Mc, Ec, pu, pd, aa, ab, lk, damp,
+          tbuf.t[0], nl, nc, i, Lw + ol, (unsigned)LP, sp);
     }
     __syncwarp();
     if (lane == 0) {
@@ -299,7 +323,7 @@ __device__ __forceinline__ TbPos tb_tile(const TmaF32TB* __restrict__ in, int lo
           if (SNAP && snap2)
             sp = in->snaps + ((((long long)slot2 * g.nx + x) * g.ny + y) * g.nz + zp) * 3;
           tb_pair_step<VISC, DAMP, PUSH, SNAP, LZ, LP>(Lc, Lw, ol, Mp, Ep, qu, qd, zin_a, zin_b,
-                                                       lk, damp, in, j11, j21, nc, i, D + i, nc,
+                                                       lk, damp, tbuf.t[1], n2, nc, i, D + i, nc,
                                                        sp);
         }
       }
@@ -320,28 +344,6 @@ __device__ __forceinline__ TbPos tb_tile(const TmaF32TB* __restrict__ in, int lo
   return p;
 }
 
-// Tiles of push or snapshot steps (a few steps of a run) go through a
-// function of their own, so that their extra live values do not raise the
-// register pressure of the loop every other tile runs.
-template <int LZ, bool VISC, bool DAMP, bool PUSH, bool SNAP>
-__device__ __noinline__ TbPos tb_tile_rare(const TmaF32TB* __restrict__ in, int local, int lit,
-                                           TbRings k, TbPos p, int w, int lane) {
-  return tb_tile<LZ, VISC, DAMP, PUSH, SNAP>(in, local, lit, k, p, w, lane);
-}
-
-// The tile's switches, resolved once per tile into a specialised loop.
-template <int LZ, bool VISC, bool DAMP>
-__device__ __forceinline__ TbPos tb_tile_ps(bool push, bool snap, const TmaF32TB* __restrict__ in,
-                                            int local, int lit, const TbRings& k, TbPos p, int w,
-                                            int lane) {
-  if (push) {
-    if (snap) return tb_tile_rare<LZ, VISC, DAMP, true, true>(in, local, lit, k, p, w, lane);
-    return tb_tile_rare<LZ, VISC, DAMP, true, false>(in, local, lit, k, p, w, lane);
-  }
-  if (snap) return tb_tile_rare<LZ, VISC, DAMP, false, true>(in, local, lit, k, p, w, lane);
-  return tb_tile<LZ, VISC, DAMP, false, false>(in, local, lit, k, p, w, lane);
-}
-
 // Whether the tile's pair of steps (lit+1, lit+2) adds force terms.
 __device__ __forceinline__ bool tb_pushes(const TmaF32TB* __restrict__ in, int lit) {
   return in->term_off != nullptr && in->term_off[lit + 2] > in->term_off[lit];
@@ -352,46 +354,52 @@ __device__ __forceinline__ bool tb_snaps(const TmaF32TB* __restrict__ in, int li
          (((lit + 1) % in->snap_stride) == 0 || ((lit + 2) % in->snap_stride) == 0);
 }
 
-// A tile without force terms or snapshots, every path inlined: the launch
-// variant that runs only such tiles holds no call, so none of its registers
-// go to the stack around one.
-template <int LZ>
-__device__ __forceinline__ TbPos tb_tile_common(const TmaF32TB* __restrict__ in, int local,
-                                                int lit, const TbRings& k, TbPos p, int w,
-                                                int lane) {
-  const bool visc = in->ncoef > 1, damp = in->use_damp != 0;
-  if (visc) {
-    if (damp) return tb_tile<LZ, true, true, false, false>(in, local, lit, k, p, w, lane);
-    return tb_tile<LZ, true, false, false, false>(in, local, lit, k, p, w, lane);
-  }
-  if (damp) return tb_tile<LZ, false, true, false, false>(in, local, lit, k, p, w, lane);
-  return tb_tile<LZ, false, false, false, false>(in, local, lit, k, p, w, lane);
-}
-
-template <int LZ>
-__device__ __forceinline__ TbPos tb_tile_any(const TmaF32TB* __restrict__ in, int local, int lit,
-                                             const TbRings& k, TbPos p, int w, int lane) {
-  const bool visc = in->ncoef > 1, damp = in->use_damp != 0;
-  const bool push = tb_pushes(in, lit), snap = tb_snaps(in, lit);
-  if (visc) {
-    if (damp) return tb_tile_ps<LZ, true, true>(push, snap, in, local, lit, k, p, w, lane);
-    return tb_tile_ps<LZ, true, false>(push, snap, in, local, lit, k, p, w, lane);
-  }
-  if (damp) return tb_tile_ps<LZ, false, true>(push, snap, in, local, lit, k, p, w, lane);
-  return tb_tile_ps<LZ, false, false>(push, snap, in, local, lit, k, p, w, lane);
-}
-
 // Launch variants.  Tiles whose pair of steps adds force terms or writes a
-// snapshot need more live values than the others; their code runs in
-// functions of its own, and a kernel that can call those keeps some of the
-// common loop's values on the stack (measured: ~3 local loads per warp and
-// plane, 12 % slower).  So a batched pair of steps is two launches on the
-// same queue: kTbCommon runs every other tile with all paths inlined and
-// raises queues[3] when it skipped one; kTbRare then runs only the skipped
-// tiles, and returns at once when the flag is down (every launch of a run
-// without pushes or snapshots).  kTbAll runs every tile (the single-solve
-// kernel).
+// snapshot need more live values than the others: in one kernel with the
+// common loop they raise its register demand (with those paths in called
+// functions the common loop kept values on the stack, ~3 local loads per
+// warp and plane; with the force terms read from the solve's tables they
+// spilled inside their own loop, 4.9x slower tiles).  So a batched pair of
+// steps is two launches on the same queue: kTbCommon runs every tile
+// without pushes or snapshots and raises queues[3] when it skipped one;
+// kTbRare then runs only the skipped tiles, and returns at once when the
+// flag is down (every launch of a run without pushes or snapshots).  kTbAll
+// runs every tile (the single-solve kernel).  The force terms come from a
+// term buffer in shared memory, so no variant spills.
 constexpr int kTbAll = 0, kTbCommon = 1, kTbRare = 2;
+
+// The tile's switches (viscosity, damping, force terms, snapshot), resolved
+// once per tile into a specialised loop, every path inlined.  A kTbCommon
+// launch meets no tile with force terms or a snapshot, so its variant holds
+// only the loops without them (102 registers); the others hold all (128).
+template <int LZ, int MODE, bool VISC, bool DAMP>
+__device__ __forceinline__ TbPos tb_tile_ps(bool push, bool snap, const TmaF32TB* __restrict__ in,
+                                            int local, int lit, const TbRings& k, TbPos p, int w,
+                                            int lane) {
+  if (MODE != kTbCommon) {
+    if (push) {
+      if (snap) return tb_tile<LZ, VISC, DAMP, true, true>(in, local, lit, k, p, w, lane);
+      return tb_tile<LZ, VISC, DAMP, true, false>(in, local, lit, k, p, w, lane);
+    }
+    if (snap) return tb_tile<LZ, VISC, DAMP, false, true>(in, local, lit, k, p, w, lane);
+  }
+  return tb_tile<LZ, VISC, DAMP, false, false>(in, local, lit, k, p, w, lane);
+}
+
+template <int LZ, int MODE>
+__device__ __forceinline__ TbPos tb_tile_sw(const TmaF32TB* __restrict__ in, int local, int lit,
+                                            const TbRings& k, TbPos p, int w, int lane) {
+  const bool visc = in->ncoef > 1, damp = in->use_damp != 0;
+  const bool push = MODE != kTbCommon && tb_pushes(in, lit);
+  const bool snap = MODE != kTbCommon && tb_snaps(in, lit);
+  if (visc) {
+    if (damp) return tb_tile_ps<LZ, MODE, true, true>(push, snap, in, local, lit, k, p, w, lane);
+    return tb_tile_ps<LZ, MODE, true, false>(push, snap, in, local, lit, k, p, w, lane);
+  }
+  if (damp) return tb_tile_ps<LZ, MODE, false, true>(push, snap, in, local, lit, k, p, w, lane);
+  return tb_tile_ps<LZ, MODE, false, false>(push, snap, in, local, lit, k, p, w, lane);
+}
+
 
 template <bool BATCH, int LZ, int MODE>
 __global__ void __launch_bounds__(TmaF32TB::THREADS, 1)
@@ -419,6 +427,7 @@ __global__ void __launch_bounds__(TmaF32TB::THREADS, 1)
   float* ringL = ringB + NB * BF;
   uint64_t* Lfull = reinterpret_cast<uint64_t*>(ringL + NL * LF);  // after the rings
   uint64_t* Lempty = Lfull + NL;
+  TbTermBuf* terms = reinterpret_cast<TbTermBuf*>(Lempty + NL);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   auto flags_of = [&](int k) -> int* { return BATCH ? tab[k].flags : one.flags; };
   if ((smem_addr(ringA) & 127u) != 0u) {
@@ -482,6 +491,13 @@ __global__ void __launch_bounds__(TmaF32TB::THREADS, 1)
           }
           if (MODE == kTbRare && !rare) continue;  // kTbCommon ran it
         }
+        const bool push = tb_pushes(in, lit);
+        if (push && (in->term_off[lit + 1] - in->term_off[lit] > kTbTermCap ||
+                     in->term_off[lit + 2] - in->term_off[lit + 1] > kTbTermCap)) {
+          if (in->flags != nullptr) atomicOr(in->flags, kFlagRefused);  // see kTbTermCap
+          continue;
+        }
+        const int ord = lg->n_taken;  // the tile's ordinal: its term buffer
         lg->solve[lg->n_taken & 7] = k;
         ++lg->n_taken;
         const Geom& g = in->g;
@@ -501,6 +517,17 @@ __global__ void __launch_bounds__(TmaF32TB::THREADS, 1)
             }
             tile_slots(base)[sa] = t;
             solve_slots(base)[sa] = k;
+            if (push) {  // every warp has left tile ord-2, which used this buffer
+              TbTermBuf& tb = terms[ord & 1];
+              const unsigned nc = (unsigned)g.ncell;
+              for (int lev = 0; lev < 2; ++lev) {
+                const int j0 = in->term_off[lit + lev], j1 = in->term_off[lit + lev + 1];
+                tb.n[lev] = j1 - j0;
+                for (int j = j0; j < j1; ++j)
+                  tb.t[lev][j - j0] = TbTermRef{in->pat + (long long)in->term_pat[j] * 3 * nc,
+                                                (float)in->term_scale[j], 0};
+              }
+            }
           }
           const int pl = min(max(p, 0), g.nx - 1);  // planes outside the grid feed only the shell
           fence_proxy_async_smem();
@@ -530,7 +557,7 @@ __global__ void __launch_bounds__(TmaF32TB::THREADS, 1)
     }
   } else {
     // ------------------------------- consumers ----------------------------
-    const TbRings k{ringA, ringB, ringL, hd, Lfull, Lempty, abort_flag};
+    const TbRings k{ringA, ringB, ringL, hd, Lfull, Lempty, abort_flag, terms};
     TbPos p;
     while (true) {
       // the tile's first plane, x0-2: centres only
@@ -540,9 +567,9 @@ __global__ void __launch_bounds__(TmaF32TB::THREADS, 1)
       const T* in = BATCH ? &tab[solve_slots(base)[p.ca.s]] : &one;
       const int local = BATCH ? t - in->tile_base : t;
       const int lit = it - in->it_begin;
-      p = MODE == kTbCommon ? tb_tile_common<LZ>(in, local, lit, k, p, warp, lane)
-                            : tb_tile_any<LZ>(in, local, lit, k, p, warp, lane);
+      p = tb_tile_sw<LZ, MODE>(in, local, lit, k, p, warp, lane);
       if (!p.ok) break;
+      ++p.ord;
       if (lane == 0) ++lg->done[warp];
     }
   }
@@ -562,10 +589,11 @@ __global__ void __launch_bounds__(TmaF32TB::THREADS, 1)
 // host side
 // ---------------------------------------------------------------------------
 // alignment slack + header + rings + the level-1 ring's full / empty barriers
+// + the two term buffers
 size_t tb_smem_bytes() {
   return 128 + kRingOffset + (size_t)TmaF32TB::NA * TmaF32TB::A_STAGE +
          (size_t)TmaF32TB::NB * TmaF32TB::B_STAGE + (size_t)TmaF32TB::NL * TmaF32TB::L_STAGE +
-         2 * TmaF32TB::NL * sizeof(uint64_t);
+         2 * TmaF32TB::NL * sizeof(uint64_t) + 2 * sizeof(TbTermBuf);
 }
 
 static int tb_set_attr() {

@@ -63,6 +63,10 @@ _PRECISION = {
     "float64": _native.SW_PLAIN_F64,
 }
 
+# Force terms of one step the two-steps-per-pass kernel holds (its shared
+# term buffer); a solve with more at any step runs one step per launch.
+_TWO_STEP_TERM_CAP = 32
+
 
 def _precision(opts: dict) -> int:
     p = opts.get("precision", "mixed")
@@ -651,6 +655,10 @@ class _Solve:
                 term_scale.append(1.0)
             term_off.append(len(term_pat))
         self.term_off = term_off
+        if max((b - a for a, b in zip(term_off, term_off[1:])), default=0) > _TWO_STEP_TERM_CAP:
+            # the two-steps-per-pass kernel holds at most this many force terms
+            # of one step; more run one step per launch
+            self.run.steps_per_pass = 1
         self.run.set_patterns(self.pats, term_off, term_pat, term_scale)
 
     def mark_steps_begin(self):

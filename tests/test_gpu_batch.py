@@ -130,6 +130,31 @@ def test_pushes_and_snapshots_inside_replayed_runs_bitwise(cuda):
             assert np.array_equal(a, b)
 
 
+@pytest.mark.parametrize("nterms", [5, 33])
+def test_many_force_terms_at_one_step_bitwise(cuda, nterms):
+    """Several force terms active at the same steps: up to 32 go through the
+    two-step kernel's shared term buffer, more make that solve run one step
+    per launch; either way the batched solve matches its lone run bit for
+    bit."""
+    import shearwave_b200 as sw
+    from shearwave_b200 import workloads as W
+
+    probs = [W.problem_inclusions(sh, 200, seed=80 + i, tol=1e-9)
+             for i, sh in enumerate([(20, 18, 24), (16, 22, 20)])]
+    rng = np.random.default_rng(nterms)
+    terms = []
+    for k in range(nterms):
+        env = np.zeros(200, np.float32)
+        env[100 + k % 3:104 + k % 3] = rng.uniform(0.1, 1.0, 4).astype(np.float32)
+        terms.append(((None, None, rng.uniform(-1, 1) * probs[0]["bz"]), env))
+    probs[0]["opts"]["force_terms"] = terms
+    got = sw.shear_fdtd_batch(probs, precision="mixed")
+    for p, res in zip(probs, got):
+        ref = _alone(p, "mixed")
+        for a, b in zip(res, ref):
+            assert np.array_equal(a, b)
+
+
 @pytest.mark.parametrize("precision", ["mixed", "fp64"])
 def test_4d_force_streamed_from_the_device(cuda, precision):
     """4-D forces: the non-zero slices are projected up front (batched CG)

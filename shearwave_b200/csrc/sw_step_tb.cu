@@ -354,66 +354,50 @@ __device__ __forceinline__ bool tb_snaps(const TmaF32TB* __restrict__ in, int li
          (((lit + 1) % in->snap_stride) == 0 || ((lit + 2) % in->snap_stride) == 0);
 }
 
-// Launch variants.  Tiles whose pair of steps adds force terms or writes a
-// snapshot need more live values than the others: in one kernel with the
-// common loop they raise its register demand (with those paths in called
-// functions the common loop kept values on the stack, ~3 local loads per
-// warp and plane; with the force terms read from the solve's tables they
-// spilled inside their own loop, 4.9x slower tiles).  So a batched pair of
-// steps is two launches on the same queue: kTbCommon runs every tile
-// without pushes or snapshots and raises queues[3] when it skipped one;
-// kTbRare then runs only the skipped tiles, and returns at once when the
-// flag is down (every launch of a run without pushes or snapshots).  kTbAll
-// runs every tile (the single-solve kernel).  The force terms come from a
-// term buffer in shared memory, so no variant spills.
-constexpr int kTbAll = 0, kTbCommon = 1, kTbRare = 2;
-
 // The tile's switches (viscosity, damping, force terms, snapshot), resolved
-// once per tile into a specialised loop, every path inlined.  A kTbCommon
-// launch meets no tile with force terms or a snapshot, so its variant holds
-// only the loops without them (102 registers); the others hold all (128).
-template <int LZ, int MODE, bool VISC, bool DAMP>
+// once per tile into a specialised loop, every path inlined.  Tiles of push
+// or snapshot steps need more live values than the others; with their paths
+// in called functions the common loop kept values on the stack around the
+// calls (~3 local loads per warp and plane), and with the force terms read
+// from the solve's tables inside the loop the push loop spilled (push tiles
+// 4.9x slower).  With the terms in the shared term buffer the whole kernel
+// fits 128 registers with nothing spilled.  (Running the push and snapshot
+// tiles in a second launch of their own, which kept the first launch's
+// variant at 102 registers, measured 1.4 % slower than this one launch.)
+template <int LZ, bool VISC, bool DAMP>
 __device__ __forceinline__ TbPos tb_tile_ps(bool push, bool snap, const TmaF32TB* __restrict__ in,
                                             int local, int lit, const TbRings& k, TbPos p, int w,
                                             int lane) {
-  if (MODE != kTbCommon) {
-    if (push) {
-      if (snap) return tb_tile<LZ, VISC, DAMP, true, true>(in, local, lit, k, p, w, lane);
-      return tb_tile<LZ, VISC, DAMP, true, false>(in, local, lit, k, p, w, lane);
-    }
-    if (snap) return tb_tile<LZ, VISC, DAMP, false, true>(in, local, lit, k, p, w, lane);
+  if (push) {
+    if (snap) return tb_tile<LZ, VISC, DAMP, true, true>(in, local, lit, k, p, w, lane);
+    return tb_tile<LZ, VISC, DAMP, true, false>(in, local, lit, k, p, w, lane);
   }
+  if (snap) return tb_tile<LZ, VISC, DAMP, false, true>(in, local, lit, k, p, w, lane);
   return tb_tile<LZ, VISC, DAMP, false, false>(in, local, lit, k, p, w, lane);
 }
 
-template <int LZ, int MODE>
+template <int LZ>
 __device__ __forceinline__ TbPos tb_tile_sw(const TmaF32TB* __restrict__ in, int local, int lit,
                                             const TbRings& k, TbPos p, int w, int lane) {
   const bool visc = in->ncoef > 1, damp = in->use_damp != 0;
-  const bool push = MODE != kTbCommon && tb_pushes(in, lit);
-  const bool snap = MODE != kTbCommon && tb_snaps(in, lit);
+  const bool push = tb_pushes(in, lit), snap = tb_snaps(in, lit);
   if (visc) {
-    if (damp) return tb_tile_ps<LZ, MODE, true, true>(push, snap, in, local, lit, k, p, w, lane);
-    return tb_tile_ps<LZ, MODE, true, false>(push, snap, in, local, lit, k, p, w, lane);
+    if (damp) return tb_tile_ps<LZ, true, true>(push, snap, in, local, lit, k, p, w, lane);
+    return tb_tile_ps<LZ, true, false>(push, snap, in, local, lit, k, p, w, lane);
   }
-  if (damp) return tb_tile_ps<LZ, MODE, false, true>(push, snap, in, local, lit, k, p, w, lane);
-  return tb_tile_ps<LZ, MODE, false, false>(push, snap, in, local, lit, k, p, w, lane);
+  if (damp) return tb_tile_ps<LZ, false, true>(push, snap, in, local, lit, k, p, w, lane);
+  return tb_tile_ps<LZ, false, false>(push, snap, in, local, lit, k, p, w, lane);
 }
 
 
-template <bool BATCH, int LZ, int MODE>
+template <bool BATCH, int LZ>
 __global__ void __launch_bounds__(TmaF32TB::THREADS, 1)
     step_f32_fused2(const __grid_constant__ TmaF32TB one, const TmaF32TB* __restrict__ tab,
                     int ninst, int ntiles, int it, const int* __restrict__ it_dev, int* queues) {
   using S = TbShape<LZ>;
-  static_assert(MODE == kTbAll || BATCH, "split launches need the batch table's flag word");
+  if (it_dev != nullptr) it += *it_dev;  // step counter kept on the device (graph replays)
   // batched launches take tiles from a launch-wide queue (see step_f32_tma)
   int* queue = queues;
-  if (MODE == kTbRare && *reinterpret_cast<volatile int*>(queue + 3) == 0) {
-    queue_cta_done(queue, true);  // no tile was deferred to this launch
-    return;
-  }
-  if (it_dev != nullptr) it += *it_dev;  // step counter kept on the device (graph replays)
   using T = TmaF32TB;
   constexpr int NA = T::NA, NB = T::NB, NL = T::NL, WB = S::WB, HB = S::HB;
   constexpr uint32_t A_BYTES = S::W * S::H * 6 * 4;
@@ -434,7 +418,7 @@ __global__ void __launch_bounds__(TmaF32TB::THREADS, 1)
     if (threadIdx.x == 0)
       for (int k = 0; k < (BATCH ? ninst : 1); ++k)
         if (int* fl = flags_of(k)) atomicOr(fl, kFlagRefused);
-    queue_cta_done(queue, MODE == kTbRare);
+    queue_cta_done(queue);
     return;
   }
   AbortLog* lg = abort_log(base);
@@ -467,7 +451,6 @@ __global__ void __launch_bounds__(TmaF32TB::THREADS, 1)
       RingPos<NB> pb;
       int stride_next = blockIdx.x;
       bool ok = true;
-      bool deferred = false;  // this CTA raised the deferred-tile flag
       while (ok && !*abort_flag) {
         const int t = next_tile(queue, stride_next);
         if (t >= ntiles) {  // end of this CTA's work: arm one stage without a copy
@@ -482,15 +465,6 @@ __global__ void __launch_bounds__(TmaF32TB::THREADS, 1)
         const int local = BATCH ? t - in->tile_base : t;
         const int lit = it - in->it_begin;
         if (lit < 0 || lit + 1 >= in->n_steps || solve_abandoned(in->flags)) continue;
-        if (MODE != kTbAll) {
-          const bool rare = tb_pushes(in, lit) || tb_snaps(in, lit);
-          if (MODE == kTbCommon && rare) {
-            if (!deferred) atomicExch(queue + 3, 1);  // kTbRare runs it
-            deferred = true;
-            continue;
-          }
-          if (MODE == kTbRare && !rare) continue;  // kTbCommon ran it
-        }
         const bool push = tb_pushes(in, lit);
         if (push && (in->term_off[lit + 1] - in->term_off[lit] > kTbTermCap ||
                      in->term_off[lit + 2] - in->term_off[lit + 1] > kTbTermCap)) {
@@ -567,7 +541,7 @@ __global__ void __launch_bounds__(TmaF32TB::THREADS, 1)
       const T* in = BATCH ? &tab[solve_slots(base)[p.ca.s]] : &one;
       const int local = BATCH ? t - in->tile_base : t;
       const int lit = it - in->it_begin;
-      p = tb_tile_sw<LZ, MODE>(in, local, lit, k, p, warp, lane);
+      p = tb_tile_sw<LZ>(in, local, lit, k, p, warp, lane);
       if (!p.ok) break;
       ++p.ord;
       if (lane == 0) ++lg->done[warp];
@@ -580,7 +554,7 @@ __global__ void __launch_bounds__(TmaF32TB::THREADS, 1)
     drain_ring(hd->fullB, lg->armedB, lg->parB, NB);
     flag_unfinished(lg, T::CONSUMER_WARPS, BATCH ? ninst : 1, kFlagTimeout, flags_of);
   }
-  queue_cta_done(queue, MODE == kTbRare);
+  queue_cta_done(queue);
 }
 
 }  // namespace
@@ -600,12 +574,10 @@ static int tb_set_attr() {
   static bool done = false;
   if (done) return SW_OK;
   const int bytes = (int)tb_smem_bytes();
-  const void* fns[6] = {(const void*)step_f32_fused2<false, 64, kTbAll>,
-                        (const void*)step_f32_fused2<true, 64, kTbCommon>,
-                        (const void*)step_f32_fused2<true, 64, kTbRare>,
-                        (const void*)step_f32_fused2<false, 32, kTbAll>,
-                        (const void*)step_f32_fused2<true, 32, kTbCommon>,
-                        (const void*)step_f32_fused2<true, 32, kTbRare>};
+  const void* fns[4] = {(const void*)step_f32_fused2<false, 64>,
+                        (const void*)step_f32_fused2<true, 64>,
+                        (const void*)step_f32_fused2<false, 32>,
+                        (const void*)step_f32_fused2<true, 32>};
   for (const void* f : fns) {
     cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(fused step smem)");
@@ -718,16 +690,13 @@ int make_tma_f32_tb(const StepArgs& a, int xchunk, TmaF32TB* t, int lz) {
 int launch_fused2_prepare() { return tb_set_attr(); }
 
 const void* step_f32_fused2_ptr(int lz) {
-  return lz == 32 ? reinterpret_cast<const void*>(step_f32_fused2<false, 32, kTbAll>)
-                  : reinterpret_cast<const void*>(step_f32_fused2<false, 64, kTbAll>);
+  return lz == 32 ? reinterpret_cast<const void*>(step_f32_fused2<false, 32>)
+                  : reinterpret_cast<const void*>(step_f32_fused2<false, 64>);
 }
 
-const void* step_f32_fused2_batch_ptr(int lz, bool rare) {
-  if (rare)
-    return lz == 32 ? reinterpret_cast<const void*>(step_f32_fused2<true, 32, kTbRare>)
-                    : reinterpret_cast<const void*>(step_f32_fused2<true, 64, kTbRare>);
-  return lz == 32 ? reinterpret_cast<const void*>(step_f32_fused2<true, 32, kTbCommon>)
-                  : reinterpret_cast<const void*>(step_f32_fused2<true, 64, kTbCommon>);
+const void* step_f32_fused2_batch_ptr(int lz) {
+  return lz == 32 ? reinterpret_cast<const void*>(step_f32_fused2<true, 32>)
+                  : reinterpret_cast<const void*>(step_f32_fused2<true, 64>);
 }
 
 static void launch_tb(const void* fn, int grid, cudaStream_t s, const TmaF32TB& one,
@@ -763,10 +732,9 @@ int launch_fused2_batch(const void* d_tab, int ninst, int ntiles, int it, int* q
   if (rc != SW_OK) return rc;
   if (ntiles == 0) return SW_OK;
   TmaF32TB dummy{};
-  for (bool rare : {false, true})
-    launch_tb(step_f32_fused2_batch_ptr(lz, rare), std::min(ntiles, kNumSMs), s, dummy,
-              (const TmaF32TB*)d_tab, ninst, ntiles, it, queues);
-  count_launches(2, 2);
+  launch_tb(step_f32_fused2_batch_ptr(lz), std::min(ntiles, kNumSMs), s, dummy,
+            (const TmaF32TB*)d_tab, ninst, ntiles, it, queues);
+  count_launches(1);
   SW_CHECK_LAUNCH("fused two-step kernel (batch)");
   return SW_OK;
 }

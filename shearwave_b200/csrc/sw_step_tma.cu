@@ -919,8 +919,7 @@ __global__ void clock_add(int* c, int by) { *c += by; }
 template <typename Inst>
 int graph_loop(void* func, const Inst& t, int grid, int threads, size_t smem, int per_launch,
                int seg, int* clock, int* queue, int it0, int nsteps, cudaStream_t s, int* done,
-               const Inst* tab = nullptr, int ninst = 1, int ntiles = -1,
-               void* func2 = nullptr) {
+               const Inst* tab = nullptr, int ninst = 1, int ntiles = -1) {
   *done = 0;
   const int seg_steps = per_launch * seg;
   const int reps = nsteps / seg_steps;
@@ -933,24 +932,19 @@ int graph_loop(void* func, const Inst& t, int grid, int threads, size_t smem, in
   const int* itd = clock;
   int* queues = queue;
   std::vector<int> offs(seg);
-  // each step launch is a node of `func`, followed by one of `func2` on the
-  // same arguments when given (the launch that runs the tiles `func` left)
-  const int per_node = func2 != nullptr ? 2 : 1;
   for (int k = 0; k < seg && e == cudaSuccess; ++k) {
     offs[k] = k * per_launch;
     void* args[] = {(void*)&t,        (void*)&tab, (void*)&ninst, (void*)&ntiles,
                     (void*)&offs[k], (void*)&itd, (void*)&queues};
-    for (int f = 0; f < per_node && e == cudaSuccess; ++f) {
-      cudaKernelNodeParams p{};
-      p.func = f == 0 ? func : func2;
-      p.gridDim = dim3(grid);
-      p.blockDim = dim3(threads);
-      p.sharedMemBytes = (unsigned)smem;
-      p.kernelParams = args;
-      cudaGraphNode_t node;
-      e = cudaGraphAddKernelNode(&node, g, prev ? &prev : nullptr, prev ? 1 : 0, &p);
-      prev = node;
-    }
+    cudaKernelNodeParams p{};
+    p.func = func;
+    p.gridDim = dim3(grid);
+    p.blockDim = dim3(threads);
+    p.sharedMemBytes = (unsigned)smem;
+    p.kernelParams = args;
+    cudaGraphNode_t node;
+    e = cudaGraphAddKernelNode(&node, g, prev ? &prev : nullptr, prev ? 1 : 0, &p);
+    prev = node;
   }
   int by = seg_steps;
   int* cl = clock;
@@ -973,8 +967,7 @@ int graph_loop(void* func, const Inst& t, int grid, int threads, size_t smem, in
   if (ex) cudaGraphExecDestroy(ex);  // freed once the enqueued replays complete
   if (g) cudaGraphDestroy(g);
   if (e != cudaSuccess) return cuda_status(e, "step-loop graph");
-  count_launches((unsigned long long)reps * (per_node * seg + 1) + 1,
-                 (unsigned long long)reps + 1);
+  count_launches((unsigned long long)reps * (seg + 1) + 1, (unsigned long long)reps + 1);
   *done = reps * seg_steps;
   return SW_OK;
 }
@@ -1190,9 +1183,8 @@ int build_batch(const sw_fdtd_desc* descs, const int32_t* begins, int n, int it,
 }
 
 // A batch table starts with the launch-wide tile queue and its finish count
-// (zeroed at the start of every call), the step counter of graph replays and
-// the flag of tiles deferred from a two-step launch to its second launch
-// (four ints); the solve arrays follow at kBatchHeader.
+// (zeroed at the start of every call) and the step counter of graph
+// replays; the solve arrays follow at kBatchHeader.
 constexpr size_t kBatchHeader = 256;
 
 // Mixed form: two steps per launch whenever every running solve runs both
@@ -1297,11 +1289,10 @@ int batch_steps_mixed(const sw_fdtd_desc* descs, const int32_t* begins, int n, i
       if (stop - it >= 64) {
         int done = 0;
         TmaF32TB dummy{};
-        rc = graph_loop<TmaF32TB>(
-            const_cast<void*>(step_f32_fused2_batch_ptr(tb_lz, false)), dummy,
-            std::min(ntiles, kNumSMs), TmaF32TB::THREADS, tb_smem_bytes(), 2, 16, queues + 2,
-            queues, it, stop - it, s, &done, (const TmaF32TB*)tab_fused, (int)tfused.size(),
-            ntiles, const_cast<void*>(step_f32_fused2_batch_ptr(tb_lz, true)));
+        rc = graph_loop<TmaF32TB>(const_cast<void*>(step_f32_fused2_batch_ptr(tb_lz)), dummy,
+                                  std::min(ntiles, kNumSMs), TmaF32TB::THREADS, tb_smem_bytes(),
+                                  2, 16, queues + 2, queues, it, stop - it, s, &done,
+                                  (const TmaF32TB*)tab_fused, (int)tfused.size(), ntiles);
         if (rc != SW_OK) return rc;
         if (done > 0) {
           it += done;

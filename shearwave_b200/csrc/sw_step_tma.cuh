@@ -170,9 +170,7 @@ int launch_fused2(const StepArgs& a, int xchunk, int it, cudaStream_t s);
 int launch_fused2_prepare();                                   // kernel attributes, once
 void launch_fused2_raw(const TmaF32TB& t, int it, cudaStream_t s);  // enqueue one launch
 const void* step_f32_fused2_ptr(int lz);        // the single-solve fused kernel (graph nodes)
-// the batched fused kernel (graph nodes): the launch of the common tiles, or
-// (rare) the launch after it that runs the tiles with pushes or snapshots
-const void* step_f32_fused2_batch_ptr(int lz, bool rare);
+const void* step_f32_fused2_batch_ptr(int lz);  // the batched fused kernel (graph nodes)
 int launch_fused2_batch(const void* d_tab, int ninst, int ntiles, int it, int* queues, int lz,
                         cudaStream_t s);
 int tma_xchunk(const Geom& g, int tz, int ty, long long want_tiles);

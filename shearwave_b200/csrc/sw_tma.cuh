@@ -158,16 +158,13 @@ __device__ inline int next_tile(int* queue, int& stride_next) {
 
 // End of a CTA of a queue-fed launch: the last CTA to finish resets the
 // launch-wide queue (queues[0]) and the finish count (queues[1]) for the next
-// launch of the stream, and with `clear_deferred` the flag of tiles deferred
-// to a second launch (queues[3]; queues[2] is a graph's step counter).
-// Every CTA has taken its last tile, and read the flag, by then.
-__device__ inline void queue_cta_done(int* queues, bool clear_deferred = false) {
+// launch of the stream.  Every CTA has taken its last tile by then.
+__device__ inline void queue_cta_done(int* queues) {
   if (queues == nullptr || threadIdx.x != 0) return;
   __threadfence();
   if (atomicAdd(queues + 1, 1) == (int)gridDim.x - 1) {
     atomicExch(queues, 0);
     atomicExch(queues + 1, 0);
-    if (clear_deferred) atomicExch(queues + 3, 0);
   }
 }
 

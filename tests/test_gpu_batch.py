@@ -108,11 +108,10 @@ def test_long_batch_replays_graphs_bitwise(cuda, precision):
 
 
 def test_pushes_and_snapshots_inside_replayed_runs_bitwise(cuda):
-    """Pairs of steps with force terms or snapshots run in the second launch
-    of each two-step pair (the first one defers them); here they fall inside
-    graph-replayed runs (a push from step 100, snapshots every 6 steps on one
-    solve, none on the others), and every solve still matches its lone run
-    bit for bit."""
+    """Push and snapshot tiles (force terms from the shared term buffer,
+    snapshot writes) inside graph-replayed runs of the two-step kernel: a
+    push from step 100, snapshots every 6 steps on one solve, none on the
+    others; every solve still matches its lone run bit for bit."""
     import shearwave_b200 as sw
     from shearwave_b200 import workloads as W
 

@@ -65,6 +65,32 @@ __host__ __device__ inline TileSpace make_tiles_tb(const Geom& g, int xc, int lz
   return t;
 }
 
+// Shape constants the producer needs per tile when a launch mixes shapes:
+// the output tile, and the bytes of a level-0 box and cells of a point box.
+struct TbDims {
+  int oz, oy;
+  uint32_t a_bytes, b_cells;
+};
+template <int LZ>
+__device__ constexpr TbDims tb_dims() {
+  using S = TbShape<LZ>;
+  return TbDims{S::OZ, S::OY, (uint32_t)(S::W * S::H * 6 * 4), (uint32_t)(S::WB * S::HB)};
+}
+
+__device__ inline TbCoord tb_coord_rt(const Geom& g, const TileSpace& t, int local, int oz,
+                                      int oy) {
+  TbCoord c;
+  const int zt = local % t.ntz;
+  const int rest = local / t.ntz;
+  const int yt = rest % t.nty;
+  const int xt = rest / t.nty;
+  c.z0 = oz * zt;
+  c.y0 = oy * yt;
+  c.x0 = 1 + xt * t.xc;
+  c.x1 = min(c.x0 + t.xc, g.nx - 1);
+  return c;
+}
+
 template <int OZ, int OY>
 __device__ inline TbCoord tb_coord(const Geom& g, const TileSpace& t, int local) {
   TbCoord c;
@@ -390,17 +416,18 @@ __device__ __forceinline__ TbPos tb_tile_sw(const TmaF32TB* __restrict__ in, int
 }
 
 
+// LZ 0 (batched launches): each solve's tiles have the solve's own shape
+// (TmaF32TB::lz), the one that computes fewer cells on its grid.
 template <bool BATCH, int LZ>
 __global__ void __launch_bounds__(TmaF32TB::THREADS, 1)
     step_f32_fused2(const __grid_constant__ TmaF32TB one, const TmaF32TB* __restrict__ tab,
                     int ninst, int ntiles, int it, const int* __restrict__ it_dev, int* queues) {
-  using S = TbShape<LZ>;
+  static_assert(LZ != 0 || BATCH, "a single solve has one shape");
   if (it_dev != nullptr) it += *it_dev;  // step counter kept on the device (graph replays)
   // batched launches take tiles from a launch-wide queue (see step_f32_tma)
   int* queue = queues;
   using T = TmaF32TB;
-  constexpr int NA = T::NA, NB = T::NB, NL = T::NL, WB = S::WB, HB = S::HB;
-  constexpr uint32_t A_BYTES = S::W * S::H * 6 * 4;
+  constexpr int NA = T::NA, NB = T::NB, NL = T::NL;
   constexpr int AF = T::A_STAGE / 4, BF = T::B_STAGE / 4, LF = T::L_STAGE / 4;
   extern __shared__ unsigned char smem_raw[];
   unsigned char* base = smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u);
@@ -475,9 +502,10 @@ __global__ void __launch_bounds__(TmaF32TB::THREADS, 1)
         lg->solve[lg->n_taken & 7] = k;
         ++lg->n_taken;
         const Geom& g = in->g;
-        const TbCoord tc = tb_coord<S::OZ, S::OY>(g, in->ts, local);
+        const TbDims dm = LZ == 32 || (LZ == 0 && in->lz == 32) ? tb_dims<32>() : tb_dims<64>();
+        const TbCoord tc = tb_coord_rt(g, in->ts, local, dm.oz, dm.oy);
         const CUtensorMap* tma = &in->tm[lit % 3];
-        const uint32_t bbytes = WB * HB * 4 * in->ncoef;
+        const uint32_t bbytes = dm.b_cells * 4 * in->ncoef;
         bool first = true;
         auto issueA = [&](int p) {
           const int sa = pa.s;
@@ -505,7 +533,7 @@ __global__ void __launch_bounds__(TmaF32TB::THREADS, 1)
           }
           const int pl = min(max(p, 0), g.nx - 1);  // planes outside the grid feed only the shell
           fence_proxy_async_smem();
-          mbar_arrive_expect_tx(&hd->fullA[sa], A_BYTES);
+          mbar_arrive_expect_tx(&hd->fullA[sa], dm.a_bytes);
           tma_load_4d(ringA + sa * AF, tma, &hd->fullA[sa], tc.z0 - 4, tc.y0 - 2, pl, 0);
           arm_record(lg->armedA, lg->parA, sa, pa.ph);
           pa.next();
@@ -541,7 +569,11 @@ __global__ void __launch_bounds__(TmaF32TB::THREADS, 1)
       const T* in = BATCH ? &tab[solve_slots(base)[p.ca.s]] : &one;
       const int local = BATCH ? t - in->tile_base : t;
       const int lit = it - in->it_begin;
-      p = tb_tile_sw<LZ>(in, local, lit, k, p, warp, lane);
+      if (LZ == 0)
+        p = in->lz == 32 ? tb_tile_sw<32>(in, local, lit, k, p, warp, lane)
+                         : tb_tile_sw<64>(in, local, lit, k, p, warp, lane);
+      else
+        p = tb_tile_sw<LZ == 0 ? 64 : LZ>(in, local, lit, k, p, warp, lane);
       if (!p.ok) break;
       ++p.ord;
       if (lane == 0) ++lg->done[warp];
@@ -574,10 +606,11 @@ static int tb_set_attr() {
   static bool done = false;
   if (done) return SW_OK;
   const int bytes = (int)tb_smem_bytes();
-  const void* fns[4] = {(const void*)step_f32_fused2<false, 64>,
+  const void* fns[5] = {(const void*)step_f32_fused2<false, 64>,
                         (const void*)step_f32_fused2<true, 64>,
                         (const void*)step_f32_fused2<false, 32>,
-                        (const void*)step_f32_fused2<true, 32>};
+                        (const void*)step_f32_fused2<true, 32>,
+                        (const void*)step_f32_fused2<true, 0>};
   for (const void* f : fns) {
     cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(fused step smem)");
@@ -695,6 +728,7 @@ const void* step_f32_fused2_ptr(int lz) {
 }
 
 const void* step_f32_fused2_batch_ptr(int lz) {
+  if (lz == 0) return reinterpret_cast<const void*>(step_f32_fused2<true, 0>);
   return lz == 32 ? reinterpret_cast<const void*>(step_f32_fused2<true, 32>)
                   : reinterpret_cast<const void*>(step_f32_fused2<true, 64>);
 }

@@ -1135,21 +1135,15 @@ static int batch_tile_width(const sw_fdtd_desc* descs, const std::vector<int>& r
   return c32 < c64 ? 32 : 64;
 }
 
-// Tile width of a batched two-step launch: the one whose tiles compute fewer
-// cells over the running solves (weighted by their interior planes), or the
-// SW_TUNE_TILE_SHAPE knob's.
-static int batch_tb_width(const sw_fdtd_desc* descs, const std::vector<int>& run) {
+// Tile width of a batched two-step launch: 0 = each solve's own (the shape
+// whose tiles compute fewer cells on its grid; on the config-3 batch 1.33
+// computed cells per output cell against 1.38 for the best single shape), or
+// the SW_TUNE_TILE_SHAPE knob's for all.
+static int batch_tb_width() {
   const int knob = tune_get(SW_TUNE_TILE_SHAPE);
   if (knob == 1) return 64;
   if (knob == 2) return 32;
-  long long w64 = 0, w32 = 0;
-  for (int i : run) {
-    const Geom g = make_geom(descs[i].nx, descs[i].ny, descs[i].nz, descs[i].pz);
-    const long long nxi = std::max(0, descs[i].nx - 2);
-    w64 += tb_work(g, 64) * nxi;
-    w32 += tb_work(g, 32) * nxi;
-  }
-  return w32 < w64 ? 32 : 64;
+  return 0;
 }
 
 // Table of the solves running at step `it`, in batch_order, with their tile
@@ -1243,7 +1237,7 @@ int batch_steps_mixed(const sw_fdtd_desc* descs, const int32_t* begins, int n, i
         std::vector<int> run;
         for (int i = 0; i < n; ++i)
           if (cur[i]) run.push_back(i);
-        tb_lz = batch_tb_width(descs, run);
+        tb_lz = batch_tb_width();
         for (int i : batch_order(descs, run)) {
           StepArgs a;
           int rc = make_step_args(&descs[i], &a);

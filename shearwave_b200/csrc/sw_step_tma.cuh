@@ -93,7 +93,7 @@ struct TmaF64 {
   int stall_test;
 };
 
-// Tile shapes of the two-steps-per-pass kernel (one per launch): output
+// Tile shapes of the two-steps-per-pass kernel (one per solve): output
 // tiles of OZ x OY cells starting at z = OZ kz, y = OY ky; step t+1 is
 // computed on the LZ x LY region around the tile (z from z0-2, y from y0-1:
 // the tile plus one cell of halo, and one more column each side in z so
@@ -155,7 +155,7 @@ struct TmaF32TB {
   int tile_base;
   int wait_k;
   int stall_test;
-  int lz;  // tile shape (TbShape<lz>): every solve of a launch has the launch's
+  int lz;  // this solve's tile shape (TbShape<lz>); a batched launch may mix them
 };
 
 size_t tma_smem_bytes(int precision);

@@ -26,6 +26,7 @@ import os
 import statistics
 import subprocess
 import sys
+import threading
 import time
 from pathlib import Path
 
@@ -102,6 +103,15 @@ class ClockSampler:
     def __init__(self, gpu_index: int):
         self.gpu = gpu_index
         self.proc = None
+        self.lines = []
+        self.reader = None
+        self.first = threading.Event()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line)
+            self.first.set()
+        self.first.set()
 
     def __enter__(self):
         try:
@@ -111,6 +121,13 @@ class ClockSampler:
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except Exception:
             self.proc = None
+            return self
+        self.reader = threading.Thread(target=self._read, daemon=True)
+        self.reader.start()
+        # nvidia-smi's start-up (driver and NVML initialisation) ends before
+        # the timed region begins: wait for its first sample, then drop it
+        self.first.wait(timeout=10)
+        self.skip = len(self.lines)
         return self
 
     def __exit__(self, *exc):
@@ -118,10 +135,12 @@ class ClockSampler:
         if self.proc is not None:
             self.proc.terminate()
             try:
-                self.out, _ = self.proc.communicate(timeout=5)
+                self.proc.wait(timeout=5)
             except Exception:
                 self.proc.kill()
-                self.out = ""
+            if self.reader is not None:
+                self.reader.join(timeout=5)
+            self.out = "".join(self.lines[self.skip:])
 
     def summary(self):
         rows = []

@@ -207,6 +207,9 @@ inline int step_slots(bool mixed = true) {
   return kNumSMs * (mixed ? tune_get(SW_TUNE_STEP_CTAS_PER_SM) : 2);
 }
 int cuda_status(cudaError_t e, const char* what);
+// Queue a host-to-device copy of a host-built table on stream s through a
+// page-locked staging slot (src may be reused as soon as this returns).
+int upload_staged(void* dst, const void* src, size_t bytes, cudaStream_t s);
 // Count kernels launched by this library (exported as sw_launch_count) and
 // the host-side enqueue calls that launched them (sw_host_enqueue_count):
 // `host` defaults to `n` (one call per kernel); a graph launch enqueues many

@@ -2,7 +2,12 @@
 #include <stdarg.h>
 #include <stdio.h>
 
+#include <string.h>
+
 #include <atomic>
+#include <map>
+#include <mutex>
+#include <vector>
 
 #include "sw_common.cuh"
 
@@ -31,6 +36,65 @@ int tune_get(int knob) { return (knob >= 0 && knob < SW_TUNE_COUNT) ? g_tune[kno
 int cuda_status(cudaError_t e, const char* what) {
   set_error("%s: %s (%s)", what, cudaGetErrorString(e), cudaGetErrorName(e));
   return SW_ECUDA;
+}
+
+// Page-locked staging of the small tables the host builds between launches
+// (batched solve tables).  A copy from pageable memory may wait for the
+// stream, which would stop the host from running ahead of the GPU; from a
+// page-locked slot the copy is queued and the call returns.  Each device has
+// a ring of slots, each with an event recorded after its copy: a slot is
+// refilled once that copy has run (the wait only happens when the host is
+// kRingSlots uploads ahead of the GPU).
+namespace {
+constexpr int kRingSlots = 32;
+struct StageSlot {
+  void* host = nullptr;
+  size_t cap = 0;
+  cudaEvent_t done = nullptr;
+  bool pending = false;
+};
+struct StageRing {
+  StageSlot slot[kRingSlots];
+  int next = 0;
+};
+std::mutex g_stage_mu;
+std::map<int, StageRing> g_stage;
+}  // namespace
+
+int upload_staged(void* dst, const void* src, size_t bytes, cudaStream_t s) {
+  if (bytes == 0) return SW_OK;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_status(e, "cudaGetDevice");
+  std::lock_guard<std::mutex> lock(g_stage_mu);
+  StageRing& ring = g_stage[dev];
+  StageSlot& sl = ring.slot[ring.next];
+  ring.next = (ring.next + 1) % kRingSlots;
+  if (sl.pending) {
+    e = cudaEventSynchronize(sl.done);  // the copy that last used this slot
+    if (e != cudaSuccess) return cuda_status(e, "table staging wait");
+    sl.pending = false;
+  }
+  if (sl.done == nullptr) {
+    e = cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming);
+    if (e != cudaSuccess) return cuda_status(e, "table staging event");
+  }
+  if (sl.cap < bytes) {
+    if (sl.host != nullptr) cudaFreeHost(sl.host);
+    sl.host = nullptr;
+    sl.cap = 0;
+    const size_t cap = bytes < 65536 ? 65536 : 2 * bytes;
+    e = cudaHostAlloc(&sl.host, cap, cudaHostAllocPortable);
+    if (e != cudaSuccess) return cuda_status(e, "table staging buffer");
+    sl.cap = cap;
+  }
+  memcpy(sl.host, src, bytes);
+  e = cudaMemcpyAsync(dst, sl.host, bytes, cudaMemcpyHostToDevice, s);
+  if (e != cudaSuccess) return cuda_status(e, "table upload");
+  e = cudaEventRecord(sl.done, s);
+  if (e != cudaSuccess) return cuda_status(e, "table staging event");
+  sl.pending = true;
+  return SW_OK;
 }
 
 }  // namespace sw

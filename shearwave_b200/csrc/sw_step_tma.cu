@@ -1258,13 +1258,11 @@ int batch_steps_mixed(const sw_fdtd_desc* descs, const int32_t* begins, int n, i
         int rc = build_batch<TmaF32>(descs, begins, n, it, tsingle, &ntiles);
         if (rc != SW_OK) return rc;
       }
-      cudaError_t e = kind == 1 ? cudaMemcpyAsync(tab_fused, tfused.data(),
-                                                  tfused.size() * sizeof(TmaF32TB),
-                                                  cudaMemcpyHostToDevice, s)
-                                : cudaMemcpyAsync(tab_single, tsingle.data(),
-                                                  tsingle.size() * sizeof(TmaF32),
-                                                  cudaMemcpyHostToDevice, s);
-      if (e != cudaSuccess) return cuda_status(e, "batch table upload");
+      const int urc = kind == 1 ? upload_staged(tab_fused, tfused.data(),
+                                                tfused.size() * sizeof(TmaF32TB), s)
+                                : upload_staged(tab_single, tsingle.data(),
+                                                tsingle.size() * sizeof(TmaF32), s);
+      if (urc != SW_OK) return urc;
       cur_kind = kind;
     }
     int rc;
@@ -1334,9 +1332,8 @@ int batch_steps(int precision, const sw_fdtd_desc* descs, const int32_t* begins,
       int rc = build_batch<Inst>(descs, begins, n, it, tab, &ntiles);
       if (rc != SW_OK) return rc;
       if (!tab.empty()) {
-        cudaError_t e = cudaMemcpyAsync(table, tab.data(), tab.size() * sizeof(Inst),
-                                        cudaMemcpyHostToDevice, s);
-        if (e != cudaSuccess) return cuda_status(e, "batch table upload");
+        const int urc = upload_staged(table, tab.data(), tab.size() * sizeof(Inst), s);
+        if (urc != SW_OK) return urc;
       }
       have = true;
     }

@@ -649,8 +649,8 @@ def main(argv=None) -> int:
     # launches one kernel per pair of time steps (one per single step at an
     # odd end); a batched run covers all running solves in each launch.
     # achieved = algorithmic bytes of the launches / their device time.
-    # the library fuses step pairs by default in batches, not for a lone solve
-    spl = 2 if a.steps_per_pass == 2 or (a.steps_per_pass == 0 and len(probs) > 1) else 1
+    # the library fuses step pairs by default, batched or alone
+    spl = 1 if a.steps_per_pass == 1 else 2
     if len(probs) > 1:
         step_ms = max(i["t_steps_ms"] for i in infos)
         steps_total = max(p["n_steps"] for p in probs)

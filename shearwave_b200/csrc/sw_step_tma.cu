@@ -994,9 +994,8 @@ int launch_steps_tma(const StepArgs& a, int xchunk, int it0, int nsteps, cudaStr
     return SW_OK;
   } else {
     // two steps per pass: two steps per launch where two remain (one step
-    // otherwise) unless the compensated sum is on.  A lone solve defaults to
-    // one step per launch: at full clock it runs faster that way (102
-    // against 90 Gcell-steps/s at 192^3).
+    // otherwise) unless the compensated sum is on (the default: 116 against
+    // 93 Gcell-steps/s at 192^3).
     const bool fuse = steps_per_pass_of(a.steps_per_pass, false) == 2 && !a.kahan && nsteps >= 2;
     TmaF32 t;
     rc = make_tma_f32(a, xchunk, &t, 0);

@@ -819,7 +819,7 @@ def shear_fdtd(
     "spectral" explicitly), ``kahan`` (False: compensated displacement sum), ``step_kernel`` ("tma" default, or "direct"), ``xchunk`` (planes
     per tile along x, 0 = automatic), ``steps_per_pass`` (mixed form: 2
     fuses two time steps per pass over HBM, except with ``kahan``; 1 one
-    step per launch; 0 (default) two in batches, one for a lone solve), ``cuda_graph`` (True: long step runs replay one instantiated CUDA
+    step per launch; 0 (default) two), ``cuda_graph`` (True: long step runs replay one instantiated CUDA
     graph of 32 steps), ``force_terms`` (extra separable terms:
     list of ``((bx, by, bz), env)``), ``force_stream_bytes`` (4-D forces: the
     non-zero slices are projected up front and streamed from the device

@@ -17,10 +17,8 @@ library set the cut (enum ``sw_tune_knob``):
   whichever of 64 x 8 and 32 x 16 covers the plane with fewer cells; 1 and
   2 force one;
 * ``steps_per_pass`` — time steps per launch of mixed solves that leave
-  ``opts["steps_per_pass"]`` at 0: 0 keeps the library's choice (two in
-  batched launches, one for a lone solve), 1 or 2 force it.  Which is
-  faster depends on whether the GPU runs at its power cap: the two-step
-  kernel moves 2.5 x fewer DRAM bytes but issues 1.6 x the instructions.
+  ``opts["steps_per_pass"]`` at 0: 0 keeps the library's choice (two),
+  1 or 2 force it.
 
 :func:`autotune` times a shortened copy of a workload (one problem through
 ``shear_fdtd``, or a batch through ``shear_fdtd_batch``) under each

@@ -180,6 +180,26 @@ struct PView {
   }
 };
 
+// A = -div_c grad_c (op 0) at interior cell i with p read through `pv` and
+// pc = p at i: the one expression both phases evaluate (the update phase
+// recomputes Ap from the stored p instead of reading an Ap vector the apply
+// phase wrote), so the two agree bit for bit.
+template <typename PV>
+__device__ __forceinline__ double op0_ap(const PV& pv, const CgInst& in, const Geom& g,
+                                         long long i, int x, int y, int z, double pc) {
+  double gp, gm, tx, ty, tz;
+  gp = (x + 1 <= g.nx - 2) ? (pv(i + 2 * g.sxy) - pc) * in.c2x : 0.0;
+  gm = (x - 1 >= 1) ? (pc - pv(i - 2 * g.sxy)) * in.c2x : 0.0;
+  tx = (gp - gm) * in.c2x;
+  gp = (y + 1 <= g.ny - 2) ? (pv(i + 2 * g.pz) - pc) * in.c2y : 0.0;
+  gm = (y - 1 >= 1) ? (pc - pv(i - 2 * g.pz)) * in.c2y : 0.0;
+  ty = (gp - gm) * in.c2y;
+  gp = (z + 1 <= g.nz - 2) ? (pv(i + 2) - pc) * in.c2z : 0.0;
+  gm = (z - 1 >= 1) ? (pc - pv(i - 2)) * in.c2z : 0.0;
+  tz = (gp - gm) * in.c2z;
+  return -((tx + ty) + tz);
+}
+
 // One tile of the apply phase (every thread of the block; uniform control).
 template <bool COH>
 __device__ __forceinline__ void apply_tile(const CgInst* __restrict__ tab, int ninst, int t,
@@ -214,18 +234,7 @@ __device__ __forceinline__ void apply_tile(const CgInst* __restrict__ tab, int n
       acc += pc * ap;
       continue;
     }
-    double gp, gm, tx, ty, tz;
-    gp = (x + 1 <= g.nx - 2) ? (pv(i + 2 * g.sxy) - pc) * in.c2x : 0.0;
-    gm = (x - 1 >= 1) ? (pc - pv(i - 2 * g.sxy)) * in.c2x : 0.0;
-    tx = (gp - gm) * in.c2x;
-    gp = (y + 1 <= g.ny - 2) ? (pv(i + 2 * g.pz) - pc) * in.c2y : 0.0;
-    gm = (y - 1 >= 1) ? (pc - pv(i - 2 * g.pz)) * in.c2y : 0.0;
-    ty = (gp - gm) * in.c2y;
-    gp = (z + 1 <= g.nz - 2) ? (pv(i + 2) - pc) * in.c2z : 0.0;
-    gm = (z - 1 >= 1) ? (pc - pv(i - 2)) * in.c2z : 0.0;
-    tz = (gp - gm) * in.c2z;
-    const double ap = -((tx + ty) + tz);
-    in.ap[i] = ap;
+    const double ap = op0_ap(pv, in, g, i, x, y, z, pc);  // not stored: the update recomputes it
     if (!pv.first) pnew[i] = pc;
     acc += pc * ap;
   }
@@ -283,13 +292,28 @@ __device__ __forceinline__ void update_tile(const CgInst* __restrict__ tab, int 
     const double* __restrict__ AP = in.ap;
     const double* __restrict__ PK = pk;
     const long long c0 = (long long)y * g.pz + z;
+    if (in.op == 0) {
+      // Ap from p_k (written before the barrier: plain loads, as in PView)
+      auto pkv = [PK](long long j) { return PK[j]; };
+#pragma unroll 1
+      for (int x = tc.x0; x < tc.x1; ++x) {
+        const long long i = (long long)x * g.sxy + c0;
+        const double pc = PK[i];
+        const double ap = op0_ap(pkv, in, g, i, x, y, z, pc);
+        X[i] = fma(alpha, pc, X[i]);
+        const double rn = fma(-alpha, ap, R[i]);
+        R[i] = rn;
+        acc += rn * rn;
+      }
+    } else {
 #pragma unroll 4
-    for (int x = tc.x0; x < tc.x1; ++x) {
-      const long long i = (long long)x * g.sxy + c0;
-      X[i] = fma(alpha, PK[i], X[i]);
-      const double rn = fma(-alpha, AP[i], R[i]);
-      R[i] = rn;
-      acc += rn * rn;
+      for (int x = tc.x0; x < tc.x1; ++x) {
+        const long long i = (long long)x * g.sxy + c0;
+        X[i] = fma(alpha, PK[i], X[i]);
+        const double rn = fma(-alpha, AP[i], R[i]);
+        R[i] = rn;
+        acc += rn * rn;
+      }
     }
   }
   double bs = block_sum(acc, red);
@@ -373,7 +397,7 @@ __device__ bool cg_grid_sync(CgGrid* b) {
   return ok_s != 0;
 }
 
-__global__ void __launch_bounds__(TILE_THREADS) cg_persist(const CgInst* __restrict__ tab,
+__global__ void __launch_bounds__(TILE_THREADS, 5) cg_persist(const CgInst* __restrict__ tab,
                                                            int ninst, int ntiles, CgGrid* bar) {
   __shared__ double red[32];
   __shared__ unsigned int lastflag;

@@ -200,6 +200,14 @@ __device__ __forceinline__ double op0_ap(const PV& pv, const CgInst& in, const G
   return -((tx + ty) + tz);
 }
 
+// Ask L2 for a line a few planes ahead of a column walk (the walk issues one
+// plane's loads at a time; the hint keeps more DRAM reads in flight).  Only
+// addresses inside the vector are passed.
+constexpr int kCgPrefetchPlanes = 4;
+__device__ __forceinline__ void prefetch_l2(const void* p) {
+  asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+
 // One tile of the apply phase (every thread of the block; uniform control).
 template <bool COH>
 __device__ __forceinline__ void apply_tile(const CgInst* __restrict__ tab, int ninst, int t,
@@ -223,6 +231,11 @@ __device__ __forceinline__ void apply_tile(const CgInst* __restrict__ tab, int n
   for (int x = tc.x0; x < tc.x1; ++x) {
     if (!interior(g, x, y, z)) continue;
     const long long i = (long long)x * g.sxy + (long long)y * g.pz + z;
+    if (x + kCgPrefetchPlanes <= g.nx - 1) {
+      const long long ia = i + kCgPrefetchPlanes * g.sxy;
+      prefetch_l2(pv.pold + ia);
+      if (!pv.first) prefetch_l2(pv.r + ia);
+    }
     const double pc = pv(i);
     if (in.op == 1) {  // -mu L7(p), laplacian_center's operation order
       const double lap = ((pv(i + g.sxy) - 2.0 * pc) + pv(i - g.sxy)) * in.ihx2 +
@@ -298,6 +311,12 @@ __device__ __forceinline__ void update_tile(const CgInst* __restrict__ tab, int 
 #pragma unroll 1
       for (int x = tc.x0; x < tc.x1; ++x) {
         const long long i = (long long)x * g.sxy + c0;
+        if (x + kCgPrefetchPlanes <= g.nx - 1) {
+          const long long ia = i + kCgPrefetchPlanes * g.sxy;
+          prefetch_l2(X + ia);
+          prefetch_l2(R + ia);
+          prefetch_l2(PK + ia);
+        }
         const double pc = PK[i];
         const double ap = op0_ap(pkv, in, g, i, x, y, z, pc);
         X[i] = fma(alpha, pc, X[i]);

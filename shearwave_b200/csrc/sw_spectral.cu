@@ -33,42 +33,50 @@ namespace sw {
 // basis of one axis (host, closed form)
 // ---------------------------------------------------------------------------
 // Q (m x m, row-major Q[i*m + k]: interior index i = grid index i+1, mode k)
-// and lam[k] (physical eigenvalues, 1/(4 h^2) included).
-void axis_basis(int n, double h, double* Q, double* lam) {
-  const int m = n - 2;
-  if (m <= 0) return;
-  std::fill(Q, Q + (size_t)m * m, 0.0);
-  const double scale = 1.0 / (4.0 * h * h);
-  int col = 0;
-  for (int par = 0; par < 2; ++par) {
-    // chain: grid indices g = first, first+2, ..., last within [1, n-2]
-    const int first = (par == 1) ? 1 : 2;
-    if (first > n - 2) continue;
-    const int last = first + 2 * ((n - 2 - first) / 2);
-    const int K = (last - first) / 2 + 1;
-    const bool nf = (first == 1), nl = (last == n - 2);  // Neumann-like ends
-    for (int k = 0; k < K; ++k, ++col) {
-      double lk;
-      for (int j = 0; j < K; ++j) {  // chain position j -> grid index first + 2j
-        double v;
-        if (nf && nl) {  // N-N: cosines, k = 0..K-1
-          const double c = (k == 0) ? sqrt(1.0 / K) : sqrt(2.0 / K);
-          v = c * cos((j + 0.5) * k * M_PI / K);
-        } else if (!nf && !nl) {  // D-D: sines, k = 1..K
-          v = sqrt(2.0 / (K + 1)) * sin((j + 1.0) * (k + 1.0) * M_PI / (K + 1));
-        } else {  // one Neumann end, one Dirichlet end
-          const int jj = nf ? j : (K - 1 - j);  // distance from the Neumann end
-          v = sqrt(2.0 / (K + 0.5)) * cos((jj + 0.5) * (k + 0.5) * M_PI / (K + 0.5));
-        }
-        const int gi = first + 2 * j;  // grid index
-        Q[(size_t)(gi - 1) * m + col] = v;
-      }
-      if (nf && nl) lk = 2.0 - 2.0 * cos(k * M_PI / K);
-      else if (!nf && !nl) lk = 2.0 - 2.0 * cos((k + 1.0) * M_PI / (K + 1));
-      else lk = 2.0 - 2.0 * cos((k + 0.5) * M_PI / (K + 0.5));
-      lam[col] = lk * scale;
-    }
+// and lam[k] (physical eigenvalues, 1/(4 h^2) included).  The interior
+// indices form two chains, the even grid indices (columns 0..K0-1) and the
+// odd ones (columns K0..); an entry is non-zero only where its row and
+// column lie on the same chain.  One entry at a time, so that the host entry
+// point and the device kernel share the formulas; `lam` (when not null)
+// receives the column's eigenvalue.
+__host__ __device__ inline double basis_entry(int n, double h, int row, int col, double* lam) {
+  const int first0 = 2, first1 = 1;
+  const int K0 = first0 > n - 2 ? 0 : (n - 2 - first0) / 2 + 1;
+  const int par = col < K0 ? 0 : 1;
+  const int first = par == 0 ? first0 : first1;
+  const int k = par == 0 ? col : col - K0;
+  const int last = first + 2 * ((n - 2 - first) / 2);
+  const int K = (last - first) / 2 + 1;
+  const bool nf = (first == 1), nl = (last == n - 2);  // Neumann-like ends
+  if (lam != nullptr) {
+    double lk;
+    if (nf && nl) lk = 2.0 - 2.0 * cos(k * M_PI / K);
+    else if (!nf && !nl) lk = 2.0 - 2.0 * cos((k + 1.0) * M_PI / (K + 1));
+    else lk = 2.0 - 2.0 * cos((k + 0.5) * M_PI / (K + 0.5));
+    *lam = lk * (1.0 / (4.0 * h * h));
   }
+  const int gi = row + 1;  // grid index of the row
+  if ((gi & 1) != (first & 1)) return 0.0;
+  const int j = (gi - first) / 2;  // chain position
+  if (nf && nl) {                  // N-N: cosines, k = 0..K-1
+    const double c = (k == 0) ? sqrt(1.0 / K) : sqrt(2.0 / K);
+    return c * cos((j + 0.5) * k * M_PI / K);
+  }
+  if (!nf && !nl)  // D-D: sines, k = 1..K
+    return sqrt(2.0 / (K + 1)) * sin((j + 1.0) * (k + 1.0) * M_PI / (K + 1));
+  const int jj = nf ? j : (K - 1 - j);  // one Neumann end: distance from it
+  return sqrt(2.0 / (K + 0.5)) * cos((jj + 0.5) * (k + 0.5) * M_PI / (K + 0.5));
+}
+
+// The solve builds its bases on the device, one thread per entry (the host
+// would spend ~1 ms per solve on the m^2 cosines, with the GPU waiting).
+__global__ void axis_basis_kernel(int n, double h, double* __restrict__ Q,
+                                  double* __restrict__ lam) {
+  const int m = n - 2;
+  const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (m <= 0 || e >= (long long)m * m) return;
+  const int row = (int)(e / m), col = (int)(e % m);
+  Q[e] = basis_entry(n, h, row, col, row == 0 ? lam + col : nullptr);
 }
 
 // ---------------------------------------------------------------------------
@@ -305,7 +313,6 @@ int spectral_one(const void* fx, const void* fy, const void* fz, InStride fs, co
   const double hs[3] = {dX, dY, dZ};
   double* Q[3];
   double* L[3];
-  std::vector<double> hq, hl;
   cudaError_t e = cudaSuccess;
   for (int a = 0; a < 3; ++a) {
     const int m = ns[a] > 2 ? ns[a] - 2 : 1;
@@ -313,15 +320,12 @@ int spectral_one(const void* fx, const void* fy, const void* fz, InStride fs, co
     p += align_up((size_t)m * m * sizeof(double), 256);
     L[a] = (double*)p;
     p += align_up((size_t)m * sizeof(double), 256);
-    hq.assign((size_t)m * m, 0.0);
-    hl.assign(m, 0.0);
-    axis_basis(ns[a], hs[a], hq.data(), hl.data());
-    if (e == cudaSuccess)
-      e = cudaMemcpyAsync(Q[a], hq.data(), hq.size() * sizeof(double), cudaMemcpyHostToDevice,
-                          s);
-    if (e == cudaSuccess)
-      e = cudaMemcpyAsync(L[a], hl.data(), hl.size() * sizeof(double), cudaMemcpyHostToDevice,
-                          s);
+    if (ns[a] > 2) {
+      const long long cnt = (long long)m * m;
+      axis_basis_kernel<<<(unsigned)((cnt + 255) / 256), 256, 0, s>>>(ns[a], hs[a], Q[a], L[a]);
+      count_launches(1);
+      SW_CHECK_LAUNCH("spectral basis");
+    }
   }
   double* d_max = (double*)p;
   if (e == cudaSuccess) e = cudaMemsetAsync(ws, 0, 3 * vec, s);
@@ -414,6 +418,9 @@ extern "C" int sw_spectral_basis(int n, double h, double* Q, double* lam) {
     set_error("sw_spectral_basis: need n >= 3, h > 0 and host buffers");
     return SW_EINVAL;
   }
-  axis_basis(n, h, Q, lam);
+  const int m = n - 2;
+  for (int row = 0; row < m; ++row)
+    for (int col = 0; col < m; ++col)
+      Q[(size_t)row * m + col] = basis_entry(n, h, row, col, row == 0 ? lam + col : nullptr);
   return SW_OK;
 }

@@ -148,7 +148,7 @@ __device__ __forceinline__ void tb_pair_step(const float* __restrict__ P,
                                              float2 E, float2 (&pu)[3], float2 (&pd)[3],
                                              bool act_a, bool act_b, const Lap7Pair& lk,
                                              float damp, const TbTermRef* __restrict__ terms,
-                                             int nterms, unsigned nc, long long i,
+                                             int nterms, unsigned nc, long long i, long long pf,
                                              float* __restrict__ out, unsigned ocs,
                                              float* __restrict__ snap) {
 #pragma unroll
@@ -169,8 +169,11 @@ __device__ __forceinline__ void tb_pair_step(const float* __restrict__ P,
     if (PUSH) {
       for (int j = 0; j < nterms; ++j) {
         const TbTermRef r = terms[j];
-        const float2 Pt =
-            __ldg(reinterpret_cast<const float2*>(r.base + (long long)c * nc + i));
+        const float* pp = r.base + (long long)c * nc + i;
+        // the pattern is read with plain loads, outside the TMA ring: ask L2
+        // for the next plane's now (pf: its offset, 0 when there is none)
+        if (pf != 0) asm volatile("prefetch.global.L2 [%0];" ::"l"(pp + pf));
+        const float2 Pt = __ldg(reinterpret_cast<const float2*>(pp));
         inc = ffma2(Pt, splat2(r.scale), inc);
       }
     }
@@ -319,7 +322,8 @@ __device__ __forceinline__ TbPos tb_tile(const TmaF32TB* __restrict__ in, int lo
         sp = in->snaps + ((((long long)slot1 * g.nx + q) * g.ny + y) * g.nz + zp) * 3;
       tb_pair_step<VISC, DAMP, PUSH, SNAP, W, H * W>(
           k.ringA + cur.s * AF, k.ringA + nxt.s * AF, o, Mc, Ec, pu, pd, aa, ab, lk, damp,
-          tbuf.t[0], nl, nc, i, Lw + ol, (unsigned)LP, sp);
+          tbuf.t[0], nl, nc, i, PUSH && q + 1 <= g.nx - 2 ? g.sxy : 0, Lw + ol, (unsigned)LP,
+          sp);
     }
     __syncwarp();
     if (lane == 0) {
@@ -349,8 +353,8 @@ __device__ __forceinline__ TbPos tb_tile(const TmaF32TB* __restrict__ in, int lo
           if (SNAP && snap2)
             sp = in->snaps + ((((long long)slot2 * g.nx + x) * g.ny + y) * g.nz + zp) * 3;
           tb_pair_step<VISC, DAMP, PUSH, SNAP, LZ, LP>(Lc, Lw, ol, Mp, Ep, qu, qd, zin_a, zin_b,
-                                                       lk, damp, tbuf.t[1], n2, nc, i, D + i, nc,
-                                                       sp);
+                                                       lk, damp, tbuf.t[1], n2, nc, i, 0, D + i,
+                                                       nc, sp);
         }
       }
       __syncwarp();

@@ -1,14 +1,16 @@
 // Mixed-form step kernel that advances two time steps per pass over HBM
-// (the default of batched launches, opts steps_per_pass=2 for a lone solve;
-// runs without the compensated sum).
+// (the default of every mixed solve, batched or alone; runs without the
+// compensated sum).
 //
 // Same per-cell update as the one-step kernels (src/shearwave/solver.py:
-// 195-226 in increment form), applied twice in one pass:
+// 195-226 in increment form), applied twice in one pass.  For the 64-wide
+// tile shape (TbShape<64>; the 32-wide shape has two rows of 16 pairs per
+// warp and a 28 x 28 output tile):
 //
 //   level 0  the state at step t, streamed by TMA: u and d of a plane around
 //            the 60 x 13 output tile (one 68 x 17 x 1 x 6 box per plane;
 //            4-stage ring: planes q and q+1 held, two in flight) and the
-//            material coefficients of the 64 x 15 level-1 region (3 stages);
+//            material coefficients of the 64 x 15 level-1 region (2 stages);
 //   level 1  step t+1 on the 64 x 15 region (the tile, one cell of halo, one
 //            more column each side in z so z pairs stay aligned), written to
 //            a 3-slot shared-memory ring of planes;
@@ -17,23 +19,25 @@
 //
 // The CTA marches along x: when level-0 plane q+1 lands, level 1 computes
 // plane q and level 2 plane q-1.  Fifteen consumer warps each own one
-// level-1 row of 32 z pairs (8-byte shared loads and stores for both cells)
-// and the same pairs at level 2, so the coefficients carry over in
-// registers; the x neighbours at x-1 of both levels come from registers too
-// (the centre values of the plane computed before), which frees a level-0
-// stage as soon as level 1 has used it.  The level-1 ring has a full and an
-// empty mbarrier per slot (one arrival per warp): level 2 of plane q-1 waits
-// until every warp has written plane q-1 (it reads the rows above and
-// below), and level 1 reuses a slot once every warp has read it, so warps
-// drift up to a plane apart instead of meeting at a barrier; every wait is
-// bounded and an abort stops each warp on its own.  Level-1 cells outside
-// the grid interior are the zero shell.  Both levels use lap7_pair, so
-// two steps here equal two one-step launches bit for bit.  A pass reads
-// buffer t mod 3 and writes buffer (t+2) mod 3.
+// level-1 row of 32 z pairs (8-byte shared loads and stores for both cells,
+// packed .f32x2 arithmetic) and the same pairs at level 2, so the
+// coefficients carry over in registers; the x neighbours at x-1 of both
+// levels come from registers too (the centre values of the plane computed
+// before), which frees a level-0 stage as soon as level 1 has used it.  The
+// level-1 ring has a full and an empty mbarrier per slot (one arrival per
+// warp): level 2 of plane q-1 waits until every warp has written plane q-1
+// (it reads the rows above and below), and level 1 reuses a slot once every
+// warp has read it, so warps drift up to a plane apart instead of meeting at
+// a barrier; every wait is bounded and an abort stops each warp on its own.
+// Level-1 cells outside the grid interior are the zero shell.  Both levels
+// use lap7_pair, so two steps here equal two one-step launches bit for bit.
+// A pass reads buffer t mod 3 and writes buffer (t+2) mod 3.  Batched
+// launches give each solve its own tile shape; the force terms of push
+// tiles come from a shared-memory term buffer the producer fills.
 //
-// It moves about 27 bytes of DRAM traffic per cell-step (u, d in and out
-// once per two steps, coefficients twice, halos), against 66 for one-step
-// launches, and executes about 1.6 times their instructions.
+// It moves about 30 bytes of DRAM traffic per cell-step (u, d in and out
+// once per two steps, coefficients once per two steps, halos), against 66
+// for one-step launches.
 #include <math.h>
 
 #include <algorithm>

@@ -160,3 +160,52 @@ def test_bench_traffic_table_covers_both_step_kernels():
     assert one is not None and two is not None
     assert 0 < two < one
     assert bench.ncu_bytes_per_cell_step("no_such_kernel") is None
+
+
+def _load_bench():
+    import importlib.util
+    from pathlib import Path
+
+    root = Path(__file__).resolve().parents[1]
+    spec = importlib.util.spec_from_file_location("bench_for_test", root / "bench.py")
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    return bench
+
+
+def test_serving_request_pool_is_seeded_and_bounded(monkeypatch):
+    """A long config-4 stream draws its arrivals from a small pool of
+    distinct seeded requests: the same order for the same seed, every entry
+    one of the pool's objects (nothing regenerated per arrival)."""
+    bench = _load_bench()
+    from shearwave_b200 import workloads as W
+
+    made = []
+
+    def fake_c4(rng):  # the generator's draws without building grids
+        made.append(int(rng.integers(0, 1 << 30)))
+        return {"id": made[-1]}
+
+    monkeypatch.setattr(W, "problem_c4", fake_c4)
+    a = bench.c4_requests(500, seed=3, pool=8)
+    b = bench.c4_requests(500, seed=3, pool=8)
+    assert len(a) == 500 and len({id(p) for p in a}) <= 8
+    assert [p["id"] for p in a] == [p["id"] for p in b]
+    assert len(made) == 16  # 8 per call
+    full = bench.c4_requests(20, seed=3, pool=0)
+    assert len({id(p) for p in full}) == 20
+
+
+def test_clock_sampler_without_nvidia_smi_reports_unavailable(monkeypatch):
+    """The bench's clock sampler starts before the timed region; with no
+    nvidia-smi (as on a CPU-only machine) it reports no samples instead of
+    failing the run."""
+    bench = _load_bench()
+
+    def no_smi(*a, **k):
+        raise FileNotFoundError("nvidia-smi")
+
+    monkeypatch.setattr(bench.subprocess, "Popen", no_smi)
+    with bench.ClockSampler(0) as c:
+        pass
+    assert c.summary()["samples"] == 0
